@@ -1,0 +1,311 @@
+"""Benchmark: short-read batch (1,000,000 pairs, 100-150 bp, 0-4% edits,
+2-bit packed), gap-affine (0,4,6,2), end-to-end, score + CIGAR.
+
+A step is one batched alignment of the whole pair set.  `value` is pairs/s
+with inputs resident in HBM (device-buffer API, CUDA events on the launching
+stream); `e2e` is the same metric through the host-buffer API, with the
+host->device input copies and device->host result/CIGAR copies inside every
+step.  Roofline: the HBM algorithmic bytes of the workload (packed inputs, an
+8-byte score/status record and one byte per CIGAR op per pair) over the
+alignment kernel's event-timed duration.  Between timed steps L2 is flushed
+by writing a 512 MiB buffer (outside the per-step events).
+
+`--impl reference` times the CPU restatement of the reference path (the
+oracle; no Rust toolchain exists on the box) with all host threads on the
+same pairs.  Multi-GPU: one process per GPU, each aligning its own seeded
+shard of the same size (weak scaling, no collective on the data path).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+PEN = [0, 4, 6, 2]
+METRIC = "pairs/sec + equiv GCUPS, batched vs plain GPU (bit-exact); served p50/p99 ms"
+WORKLOAD = "short-read batch: 1,000,000 pairs, n~U[100,150], p~U[0,0.04], 2-bit packed, gap-affine 0,4,6,2, end-to-end, score+CIGAR"
+
+
+def load_pkg():
+    from _pkg import load
+    return load()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def make_workload(num_pairs, rank):
+    pkg = load_pkg()
+    from wfa_b200 import synth
+    ps = synth.uniform_pairs(num_pairs, 100, 150, 0.0, 0.04, synth.SEED_BASE + 2 + 1000 * rank)
+    words, pwo, two = synth.pack2bits(ps)
+    words = np.concatenate([words, np.zeros(4, np.uint32)])
+    return pkg, synth, ps, words, pwo, two
+
+
+class ClockSampler:
+    """nvidia-smi clocks during the timed region."""
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def cpu_baseline(ps, threads, max_pairs=None):
+    """The oracle (C++ restatement) on the host cores; returns (pairs/s, pairs, secs)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    n = len(ps) if max_pairs is None else min(len(ps), max_pairs)
+    sub = ps.subset(np.arange(n))
+    secs, _, _, _ = O.batch(3, PEN, ps.buf.tobytes(), sub.p_off, sub.p_len, sub.t_off, sub.t_len,
+                            compute_alignment=True, mode=0, threads=threads, want_results=False)
+    return n / secs, n, secs
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    pkg, synth, ps, _, _, _ = make_workload(args.pairs, 0)
+    threads = os.cpu_count() or 1
+    sample = min(len(ps), args.cpu_sample)
+    for _ in range(args.warmup):
+        cpu_baseline(ps, threads, max_pairs=min(sample, 20_000))
+    tot_secs, tot_pairs = 0.0, 0
+    for _ in range(args.steps):
+        rate, n, secs = cpu_baseline(ps, threads, max_pairs=sample)
+        tot_secs += secs
+        tot_pairs += n
+    value = tot_pairs / tot_secs
+    cells = float(np.mean(ps.p_len.astype(np.float64) * ps.t_len))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "pairs/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000 * tot_secs / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)",
+            "config": {"workload": WORKLOAD, "sample_pairs_per_step": sample},
+            "gcups": value * cells / 1e9,
+            "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": threads, "kind": "port",
+                             "sample": f"{sample} pairs of the workload per step"},
+            "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_gpu(args):
+    import torch
+    rank, world, local = dist_env()
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pkg, synth, ps, words, pwo, two = make_workload(args.pairs, rank)
+    n = len(ps)
+    a = pkg.WavefrontAligner(pkg.GAP_AFFINE, PEN, device=local)
+    a.set_alignment_scope(True)
+
+    # Device-resident inputs and outputs.
+    t_words = torch.from_numpy(words.view(np.int32)).to(dev)
+    t_po, t_pl = torch.from_numpy(pwo).to(dev), torch.from_numpy(ps.p_len).to(dev)
+    t_to, t_tl = torch.from_numpy(two).to(dev), torch.from_numpy(ps.t_len).to(dev)
+    caps = 2 * (ps.p_len.astype(np.int64) + ps.t_len) + 1
+    coff = np.concatenate([[0], np.cumsum(caps)[:-1]]).astype(np.int64)
+    t_co = torch.from_numpy(coff).to(dev)
+    cig = torch.empty(int(caps.sum()) + 16, dtype=torch.uint8, device=dev)
+    res = torch.empty(n * 10, dtype=torch.int32, device=dev)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        a.align_batch_device(t_words.data_ptr(), t_words.numel() * 4, t_po.data_ptr(),
+                             t_pl.data_ptr(), t_to.data_ptr(), t_tl.data_ptr(), n, res.data_ptr(),
+                             cig.data_ptr(), t_co.data_ptr(), int(caps.sum()), packed=True,
+                             stream=stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    launches0 = a.kernel_launches()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    step_ms, kern_ms = [], []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            e1.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+            kern_ms.append(a.last_kernel_ms())
+    torch.cuda.synchronize()
+    launches = a.kernel_launches() - launches0
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * n * args.steps / (total_ms / 1000.0)
+
+    # Results of the last step (for the byte counts and a parity spot check).
+    rd = res.cpu().numpy().view(pkg.RESULT_DTYPE)
+    assert np.all(rd["status"] == 5), "not every pair completed"
+    cig_ops = int(rd["cigar_length"].astype(np.int64).sum())
+    in_bytes = int(((ps.p_len + 3) // 4).sum() + ((ps.t_len + 3) // 4).sum())
+    alg_bytes = in_bytes + 8 * n + cig_ops
+    kms = float(np.mean(kern_ms))
+    hbm_peak, peak_kind = peaks()
+    achieved = alg_bytes / (kms / 1000.0) / 1e9
+    cells = float(np.sum(ps.p_len.astype(np.float64) * ps.t_len))
+
+    # End to end: host (pinned) buffers through the host-buffer API.
+    pin = lambda x: torch.from_numpy(np.ascontiguousarray(x)).pin_memory().numpy()
+    h_words, h_po, h_pl, h_to, h_tl = pin(words), pin(pwo), pin(ps.p_len), pin(two), pin(ps.t_len)
+    h_res = torch.zeros(n * 10, dtype=torch.int32).pin_memory().numpy().view(pkg.RESULT_DTYPE)
+    h_cig = torch.zeros(int(caps.sum()) + 16, dtype=torch.uint8).pin_memory().numpy()
+    e2e_ms = []
+    for i in range(args.warmup + args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        hr, hc = a.align_batch(h_words, h_po, h_pl, h_to, h_tl, packed=True, out_results=h_res,
+                               out_cigars=h_cig)
+        t1 = time.perf_counter()
+        if i >= args.warmup:
+            e2e_ms.append((t1 - t0) * 1000)
+    e2e_total = sum(e2e_ms)
+    if world > 1:
+        t = torch.tensor([e2e_total], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_value = world * n * args.steps / (e2e_total / 1000.0)
+    assert np.array_equal(hr["score"], rd["score"])
+    h2d = int(h_words.nbytes + h_po.nbytes + h_pl.nbytes + h_to.nbytes + h_tl.nbytes)
+    d2h = int(hr.nbytes + int(hr["cigar_length"].astype(np.int64).sum()))
+
+    # Plain per-call form: one pair per call (host buffers), on a sample.
+    plain_n = min(args.plain_pairs, n)
+    raw = [ps.pair(i) for i in range(plain_n)]
+    for p, t in raw[:50]:
+        a.align_end2end(p, t)
+    t0 = time.perf_counter()
+    for p, t in raw:
+        a.align_end2end(p, t)
+    plain_secs = time.perf_counter() - t0
+    plain_value = plain_n / plain_secs
+
+    line = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic (seeded)",
+            "config": {"workload": WORKLOAD, "pairs_per_gpu": n, "l2": "flushed (512 MiB write) between steps",
+                       "form": "batched persistent kernel, device-resident inputs"},
+            "gcups": world * cells * args.steps / (total_ms / 1000.0) / 1e9,
+            "e2e": {"value": e2e_value, "unit": "pairs/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "api": "wfa_batch_align (pinned host buffers)"},
+            "plain": {"value": plain_value, "unit": "pairs/s", "pairs": plain_n,
+                      "api": "wfa_align_end2end, one pair per call"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": achieved / hbm_peak, "traffic": None, "peak_kind": peak_kind,
+                         "kernel_ms": kms, "algorithmic_bytes_per_launch": alg_bytes},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary()}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        rate, m, secs = cpu_baseline(ps, threads, max_pairs=args.cpu_sample)
+        line["cpu_baseline"] = {"value": rate, "unit": "pairs/s", "cores": threads, "kind": "port",
+                                "sample": f"first {m} pairs of the workload ({secs:.2f} s wall)"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    a.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--pairs", type=int, default=1_000_000)
+    ap.add_argument("--plain-pairs", type=int, default=2000)
+    ap.add_argument("--cpu-sample", type=int, default=1_000_000)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

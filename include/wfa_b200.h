@@ -1,0 +1,234 @@
+/*
+ * wfa_b200.h -- C ABI of the B200 wavefront-alignment library.
+ *
+ * The entry points replace the public aligner API of wfa2lib-rs
+ * (src/aligner.rs, `WavefrontAligner<N>`), one C function per Rust method,
+ * so that a Rust (or any FFI) caller binds them 1:1; INTEGRATION.md shows the
+ * binding.  Everything is plain pointers, sizes and integer codes.  Errors are
+ * negative return codes (never an abort): where the reference panics on
+ * invalid penalties (src/penalties.rs:157-167,198-209,253-265) the C ABI
+ * returns WFA_ERR_PENALTIES.
+ *
+ * Threading: a handle is used by one host thread at a time (the reference's
+ * aligner is Send, not Sync).  Different handles may run concurrently.
+ *
+ * Results are bit-identical to the reference's CPU path (score, CIGAR,
+ * tie-breaks, statuses) for every pair; each pair of a batch is aligned as a
+ * freshly created reference aligner with the handle's configuration would
+ * align it.
+ */
+#ifndef WFA_B200_H
+#define WFA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define WFA_API __attribute__((visibility("default")))
+#else
+#define WFA_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- enums (values match the reference's enum order) ------------------ */
+
+/* DistanceMetric, src/penalties.rs:12-23 */
+typedef enum {
+  WFA_METRIC_INDEL = 0,
+  WFA_METRIC_EDIT = 1,
+  WFA_METRIC_GAP_LINEAR = 2,
+  WFA_METRIC_GAP_AFFINE = 3,
+  WFA_METRIC_GAP_AFFINE_2P = 4
+} wfa_metric_t;
+
+/* AlignStatus, src/aligner.rs:120-135 */
+typedef enum {
+  WFA_STATUS_OK = 0,
+  WFA_STATUS_END_REACHED = 1,
+  WFA_STATUS_END_UNREACHABLE = 2,
+  WFA_STATUS_MAX_STEPS_REACHED = 3,
+  WFA_STATUS_OOM = 4,
+  WFA_STATUS_COMPLETED = 5,
+  WFA_STATUS_PARTIAL = 6
+} wfa_status_t;
+
+/* AlignmentScope, src/aligner.rs:26-31 */
+typedef enum { WFA_SCOPE_SCORE = 0, WFA_SCOPE_ALIGNMENT = 1 } wfa_scope_t;
+
+/* MemoryMode, src/aligner.rs:43-51 (BiWFA / "ultralow" is wfa_align_biwfa) */
+typedef enum { WFA_MEMORY_HIGH = 0, WFA_MEMORY_MED = 1, WFA_MEMORY_LOW = 2 } wfa_memory_t;
+
+/* Compat, src/aligner.rs:88-94 */
+typedef enum { WFA_COMPAT_C = 0, WFA_COMPAT_CORRECTED = 1 } wfa_compat_t;
+
+/* HeuristicStrategy, src/heuristic.rs:14-58 */
+typedef enum {
+  WFA_HEURISTIC_NONE = 0,
+  WFA_HEURISTIC_WFADAPTIVE = 1,   /* p0 min_wavefront_length, p1 max_distance_threshold, p2 steps */
+  WFA_HEURISTIC_XDROP = 2,        /* p0 xdrop, p1 steps_between_cutoffs */
+  WFA_HEURISTIC_ZDROP = 3,        /* p0 zdrop, p1 steps_between_cutoffs */
+  WFA_HEURISTIC_BANDED_STATIC = 4,   /* p0 min_k, p1 max_k */
+  WFA_HEURISTIC_BANDED_ADAPTIVE = 5  /* p0 min_k, p1 max_k, p2 steps */
+} wfa_heuristic_kind_t;
+
+/* Error codes (negative). */
+enum {
+  WFA_OK = 0,
+  WFA_ERR_PENALTIES = -1,   /* invalid penalties (the reference panics) */
+  WFA_ERR_ARGUMENT = -2,    /* NULL handle / bad size / bad enum */
+  WFA_ERR_UNSUPPORTED = -3, /* configuration this build does not run on the GPU */
+  WFA_ERR_CUDA = -4,        /* CUDA runtime error (see wfa_last_error_string) */
+  WFA_ERR_NO_DEVICE = -5,   /* no CUDA device */
+  WFA_ERR_OOM = -6          /* device memory exhausted */
+};
+
+/* ---- penalties ---------------------------------------------------------- */
+
+/* User penalties, as the reference's LinearPenalties / AffinePenalties /
+ * Affine2pPenalties (src/penalties.rs:26-65).  Gap-linear puts `indel` in
+ * gap_opening1.  Unused fields are ignored. */
+typedef struct {
+  int32_t match;
+  int32_t mismatch;
+  int32_t gap_opening1;
+  int32_t gap_extension1;
+  int32_t gap_opening2;
+  int32_t gap_extension2;
+} wfa_penalties_t;
+
+/* Replaces the validation asserts of WavefrontPenalties::new_linear/
+ * new_affine/new_affine2p (src/penalties.rs:157-296).  WFA_OK or
+ * WFA_ERR_PENALTIES. */
+WFA_API int wfa_penalties_check(wfa_metric_t metric, const wfa_penalties_t* penalties);
+
+/* ---- aligner handle ----------------------------------------------------- */
+
+typedef struct wfa_aligner wfa_aligner_t;
+
+/* WavefrontAligner::new (src/aligner.rs:409).  `device` is the CUDA device
+ * ordinal.  Returns NULL and sets *err (if err != NULL) on failure. */
+WFA_API wfa_aligner_t* wfa_aligner_create(wfa_metric_t metric, const wfa_penalties_t* penalties,
+                                  int device, int* err);
+WFA_API void wfa_aligner_destroy(wfa_aligner_t* h);
+
+/* Builder setters, src/aligner.rs:462-613.  Return WFA_OK or an error. */
+WFA_API int wfa_set_memory_mode(wfa_aligner_t* h, wfa_memory_t mode);               /* :462 */
+WFA_API int wfa_set_max_memory_compact(wfa_aligner_t* h, uint64_t bytes);           /* :469 */
+WFA_API int wfa_set_max_alignment_steps(wfa_aligner_t* h, int32_t max_steps);       /* :533 */
+WFA_API int wfa_set_alignment_scope(wfa_aligner_t* h, wfa_scope_t scope);           /* :542 */
+WFA_API int wfa_set_alignment_free_ends(wfa_aligner_t* h, int32_t pattern_begin_free,
+                                int32_t pattern_end_free, int32_t text_begin_free,
+                                int32_t text_end_free);                      /* :563 */
+WFA_API int wfa_set_alignment_extension(wfa_aligner_t* h);                          /* :582 */
+WFA_API int wfa_set_alignment_end_to_end(wfa_aligner_t* h);                         /* :595 */
+WFA_API int wfa_set_compat(wfa_aligner_t* h, wfa_compat_t compat);                  /* :606 */
+WFA_API int wfa_set_heuristic(wfa_aligner_t* h, wfa_heuristic_kind_t kind, int32_t p0, int32_t p1,
+                      int32_t p2);                                          /* :611 */
+
+/* ---- plain per-call aligners (host buffers) -------------------------------
+ * Each returns the alignment score (what the Rust method returns) or, when
+ * the call itself fails, a negative WFA_ERR_* code with wfa_status() ==
+ * WFA_STATUS_OOM and wfa_last_error() set.  Sequences are ASCII bytes. */
+WFA_API int32_t wfa_align_end2end(wfa_aligner_t* h, const uint8_t* pattern, int32_t pattern_length,
+                          const uint8_t* text, int32_t text_length);            /* :620 */
+WFA_API int32_t wfa_align_endsfree(wfa_aligner_t* h, const uint8_t* pattern, int32_t pattern_length,
+                           const uint8_t* text, int32_t text_length);           /* :707 */
+WFA_API int32_t wfa_align_biwfa(wfa_aligner_t* h, const uint8_t* pattern, int32_t pattern_length,
+                        const uint8_t* text, int32_t text_length);              /* :2563 */
+WFA_API int32_t wfa_align_biwfa_score(wfa_aligner_t* h, const uint8_t* pattern,
+                              int32_t pattern_length, const uint8_t* text,
+                              int32_t text_length);                              /* :2650 */
+/* 2-bit packed input, 4 bases per byte LSB-first (A0 C1 G2 T3), as
+ * align_packed2bits (src/aligner.rs:2755, src/sequences.rs:55-74). */
+WFA_API int32_t wfa_align_packed2bits(wfa_aligner_t* h, const uint8_t* pattern, int32_t pattern_length,
+                              const uint8_t* text, int32_t text_length);
+/* align_lambda (src/aligner.rs:2743) needs a host callback per base
+ * comparison; it cannot run on the device: always WFA_ERR_UNSUPPORTED. */
+WFA_API int32_t wfa_align_lambda(wfa_aligner_t* h, int (*match_fn)(int32_t, int32_t, void*), void* ctx,
+                         int32_t pattern_length, int32_t text_length);
+
+/* Accessors: status() (:834), cigar() (:839), alignment_end_pos (pub field).
+ * The CIGAR pointer stays valid until the next call on the handle. */
+WFA_API wfa_status_t wfa_status(const wfa_aligner_t* h);
+WFA_API int wfa_cigar(const wfa_aligner_t* h, const uint8_t** ops, int32_t* length, int32_t* score,
+              int32_t* end_v, int32_t* end_h);
+WFA_API int wfa_alignment_end_pos(const wfa_aligner_t* h, int32_t* score, int32_t* k, int32_t* offset);
+WFA_API int wfa_last_error(const wfa_aligner_t* h);
+WFA_API const char* wfa_last_error_string(const wfa_aligner_t* h);
+
+/* ---- batched form ---------------------------------------------------------
+ * Many pairs in one launch of the persistent kernel.  Sequences live in one
+ * buffer: pattern i is seq[p_off[i] .. p_off[i]+p_len[i]) and text i likewise
+ * (ASCII: byte offsets; WFA_SEQ_PACKED2: 32-bit-word offsets into a buffer of
+ * 2-bit codes, 16 bases per word LSB-first, every sequence word-aligned).
+ * Per pair the result goes to results[i]; CIGAR ops ('M','X','I','D') of pair
+ * i are written inside its slot cigars[cigar_off[i] .. + cigar_cap(i)) with
+ * cigar_cap(i) = 2*(p_len+t_len)+1 (wfa_batch_align_device: results[i].
+ * cigar_begin is relative to that slot; wfa_batch_align: the CIGARs are
+ * packed densely in input order and cigar_begin is the offset into `cigars`). */
+typedef enum { WFA_SEQ_ASCII = 0, WFA_SEQ_PACKED2 = 1 } wfa_seq_format_t;
+typedef enum { WFA_SPAN_END2END = 0, WFA_SPAN_ENDSFREE = 1 } wfa_span_mode_t;
+
+typedef struct {
+  int32_t score;        /* what align_* returns */
+  int32_t status;       /* wfa_status_t */
+  int32_t cigar_begin;  /* first op, relative to the pair's slot */
+  int32_t cigar_length; /* 0 in score-only mode */
+  int32_t cigar_score;  /* Cigar::score */
+  int32_t end_v;        /* Cigar::end_v */
+  int32_t end_h;        /* Cigar::end_h */
+  int32_t end_score;    /* alignment_end_pos.score */
+  int32_t end_k;        /* alignment_end_pos.k */
+  int32_t end_offset;   /* alignment_end_pos.offset */
+} wfa_result_t;
+
+typedef struct {
+  int32_t format;           /* wfa_seq_format_t */
+  int32_t span;             /* wfa_span_mode_t: align_end2end or align_endsfree semantics */
+  int64_t num_pairs;
+  const void* seq;          /* sequence buffer */
+  int64_t seq_bytes;        /* its size in bytes */
+  const int64_t* p_off;
+  const int32_t* p_len;
+  const int64_t* t_off;
+  const int32_t* t_len;
+  const int64_t* cigar_off; /* NULL in score-only mode */
+  int64_t cigar_bytes;      /* size of the CIGAR buffer */
+} wfa_batch_t;
+
+/* Host-buffer batch: copies inputs to the device, aligns every pair, copies
+ * results (and CIGARs) back.  cigars may be NULL in score-only mode.  Blocks
+ * until done.  Returns WFA_OK or an error code. */
+WFA_API int wfa_batch_align(wfa_aligner_t* h, const wfa_batch_t* batch, wfa_result_t* results,
+                    uint8_t* cigars);
+
+/* Device-buffer batch: every pointer of `batch`, `results` and `cigars` is
+ * device memory; the work is enqueued on `stream` (a cudaStream_t, 0 for the
+ * default stream) and the call returns without waiting.  Scratch memory is
+ * owned by the handle and reused across calls. */
+WFA_API int wfa_batch_align_device(wfa_aligner_t* h, const wfa_batch_t* batch, wfa_result_t* results,
+                           uint8_t* cigars, void* stream);
+
+/* Number of the library's own kernel launches issued so far by this handle. */
+WFA_API int64_t wfa_kernel_launches(const wfa_aligner_t* h);
+
+/* Device time (ms, CUDA events on the launching stream) of the alignment
+ * kernel launches of the handle's last call, retries included. */
+WFA_API double wfa_last_kernel_ms(const wfa_aligner_t* h);
+
+/* ---- helpers -------------------------------------------------------------- */
+
+/* Cigar::to_string_rle(true), src/cigar.rs:522-546.  Writes at most cap-1
+ * chars and a NUL; returns the full string length. */
+WFA_API int32_t wfa_cigar_rle(const uint8_t* ops, int32_t length, char* out, int32_t cap);
+
+/* Library version string. */
+WFA_API const char* wfa_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WFA_B200_H */

@@ -1573,7 +1573,9 @@ class Aligner {
     int64_t b = cigar.begin, e = cigar.end;
     if (span == SPAN_ENDSFREE) {
       int32_t trailing = (plen() - cigar.end_v) + (tlen() - cigar.end_h);
-      cigar.end = std::max<int64_t>(0, e - trailing);  // usize::saturating_sub
+      // end.saturating_sub(trailing as usize): a negative count wraps to a
+      // huge usize, so the view becomes empty.
+      cigar.end = trailing < 0 ? 0 : std::max<int64_t>(0, e - trailing);
       uint8_t op = b < (int64_t)cigar.ops.size() ? cigar.ops[(size_t)b] : 0;
       int32_t fr = op == 'I' ? t0 : op == 'D' ? p0 : 0;
       cigar_skip_gap(op, fr);

@@ -1,0 +1,106 @@
+// wfa_emu.cpp -- TEST-ONLY host builds of the device aligner (wfa_align.cuh).
+// Default build: a one-lane warp.  With -DWFA_EMU_THREADS: 32 host threads
+// per warp, __syncwarp and the reductions as barriers.  The CPU tests compare
+// them with the oracle so the kernel's logic is checked before it runs on a
+// GPU.  Not part of the product.
+#define WFA_EMU 1
+#include <cstdlib>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+#include "../../wfa2lib-rs_b200/csrc/wfa_align.cuh"
+#include "../../wfa2lib-rs_b200/csrc/wfa_params.h"
+
+using namespace wfab;
+
+#ifdef WFA_EMU_THREADS
+namespace wfab {
+thread_local int g_emu_lane = 0;
+EmuWarp* g_emu_warp = nullptr;
+}  // namespace wfab
+#endif
+
+template <int CLS>
+static bool run_lane(const AlignParams& P, const Workspace& ws, int64_t i) {
+  if (P.format == WFA_SEQ_PACKED2) {
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(P.seq);
+    SeqPacked sp{w + P.p_off[i], P.p_len[i], (P.p_len[i] + 15) >> 4};
+    SeqPacked st{w + P.t_off[i], P.t_len[i], (P.t_len[i] + 15) >> 4};
+    return align_one<CLS, SeqPacked>(P, ws, i, sp, st);
+  }
+  SeqAscii sp{P.seq + P.p_off[i], P.p_len[i]};
+  SeqAscii st{P.seq + P.t_off[i], P.t_len[i]};
+  return align_one<CLS, SeqAscii>(P, ws, i, sp, st);
+}
+
+template <int CLS>
+static bool run_pair(const AlignParams& P, int64_t i) {
+  constexpr int NC = CLS == kAffine2pClass ? 5 : CLS == kAffineClass ? 3 : 1;
+  std::vector<WfD> ring((size_t)P.scope * NC);
+  std::vector<int32_t> ringv((size_t)P.scope * NC * P.wmax, 0x5A5A5A5A);
+  std::vector<int4> hist((size_t)P.hist_scores, int4{0, -1, 0, 0});
+  std::vector<int32_t> harena((size_t)P.hist_words, 0x5A5A5A5A);
+  Workspace ws{ring.data(), ringv.data(), hist.data(), harena.data()};
+#ifdef WFA_EMU_THREADS
+  EmuWarp warp;
+  g_emu_warp = &warp;
+  bool retry[32];
+  std::vector<std::thread> lanes;
+  for (int l = 0; l < 32; ++l)
+    lanes.emplace_back([&, l]() {
+      g_emu_lane = l;
+      retry[l] = run_lane<CLS>(P, ws, i);
+    });
+  for (auto& t : lanes) t.join();
+  for (int l = 1; l < 32; ++l)
+    if (retry[l] != retry[0]) std::abort();  // lanes disagreed: not warp-uniform
+  return retry[0];
+#else
+  return run_lane<CLS>(P, ws, i);
+#endif
+}
+
+extern "C" int64_t wfa_emu_batch(int metric, const int32_t* pen6, int compute_alignment, int span,
+                                 int extension, const int32_t* free4, int hkind, const int32_t* hp3,
+                                 int32_t max_steps, int format, const uint8_t* seq, int64_t seq_bytes,
+                                 const int64_t* p_off, const int32_t* p_len, const int64_t* t_off,
+                                 const int32_t* t_len, int64_t num_pairs, const int64_t* cigar_off,
+                                 uint8_t* cigars, wfa_result_t* results, int32_t wmax,
+                                 int32_t hist_scores, int64_t hist_words) {
+  AlignParams P;
+  std::memset(&P, 0, sizeof P);
+  wfa_penalties_t u = {pen6[0], pen6[1], pen6[2], pen6[3], pen6[4], pen6[5]};
+  if (set_penalties(metric, &u, P) != WFA_OK) return -1;
+  P.span = span;
+  P.extension = extension;
+  if (free4) { P.p0 = free4[0]; P.pf = free4[1]; P.t0 = free4[2]; P.tf = free4[3]; }
+  P.hkind = hkind;
+  if (hp3) { P.hp0 = hp3[0]; P.hp1 = hp3[1]; P.hp2 = hp3[2]; }
+  P.compute_alignment = compute_alignment;
+  P.max_steps = max_steps;
+  P.format = format;
+  P.seq = seq;
+  P.seq_bytes = seq_bytes;
+  P.p_off = p_off; P.p_len = p_len; P.t_off = t_off; P.t_len = t_len;
+  P.cigar_off = cigar_off;
+  P.cigars = cigars;
+  P.results = results;
+  P.num_pairs = num_pairs;
+  P.wmax = wmax;
+  P.hist_scores = hist_scores;
+  P.hist_words = hist_words;
+  int64_t retries = 0;
+  int cls = metric_class(metric);
+  for (int64_t i = 0; i < num_pairs; ++i) {
+    bool r;
+    switch (cls) {
+      case kEditClass: r = run_pair<kEditClass>(P, i); break;
+      case kLinearClass: r = run_pair<kLinearClass>(P, i); break;
+      case kAffineClass: r = run_pair<kAffineClass>(P, i); break;
+      default: r = run_pair<kAffine2pClass>(P, i); break;
+    }
+    if (r) { results[i].status = kStatusRetry; ++retries; }
+  }
+  return retries;
+}

@@ -1,0 +1,35 @@
+"""The device aligner with a full 32-lane warp emulated by host threads.
+
+Lane partitioning of the diagonals, the warp reductions behind trims,
+termination and heuristics, and warp-uniform control flow (a lane that
+diverges at a barrier would hang or abort) are exercised here on CPU.
+Kept small: every emulated pair costs 32 host threads.
+"""
+import pytest
+
+import emu_lib
+from test_emu_vs_oracle import HEUR, oracle_run
+from test_oracle_unit import lcg_pairs
+
+CASES = [
+    (3, [0, 4, 6, 2], 0, None, 0, (0, 0, 0)),
+    (4, [0, 4, 6, 2, 24, 1], 0, None, 0, (0, 0, 0)),
+    (1, None, 0, None, 0, (0, 0, 0)),
+    (2, [-1, 3, 2], 1, [6, 6, 6, 6], 0, (0, 0, 0)),
+    (3, [-3, 5, 3, 2], 1, [4, 9, 4, 9], 0, (0, 0, 0)),
+    (3, [0, 4, 6, 2], 0, None, HEUR["wfa-adaptive"], (10, 50, 1)),
+    (3, [0, 4, 6, 2], 0, None, HEUR["xdrop"], (20, 1, 0)),
+    (3, [0, 4, 6, 2], 0, None, HEUR["zdrop"], (20, 1, 0)),
+    (4, [0, 4, 6, 2, 24, 1], 0, None, HEUR["banded-adaptive"], (-3, 3, 1)),
+    (0, None, 0, None, HEUR["banded-static"], (-5, 5, 0)),
+]
+
+
+@pytest.mark.parametrize("metric,pen,span,free,hk,hp", CASES)
+def test_32_lanes(metric, pen, span, free, hk, hp):
+    pairs = lcg_pairs(101 + metric + hk, 3, 260)
+    res, cig = emu_lib.run(metric, pen, pairs, span=span, free=free, heuristic=hk, hparams=hp,
+                           lanes=32, packed=metric == 3)
+    for i, (p, t) in enumerate(pairs):
+        s, st, ops, ep, _ = oracle_run(metric, pen, p, t, True, span, free, hk, list(hp))
+        assert (int(res["score"][i]), int(res["status"][i]), cig[i]) == (s, st, ops), i

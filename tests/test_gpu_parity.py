@@ -1,0 +1,252 @@
+"""GPU parity: the CUDA path through the C ABI against the oracle.
+
+Integer work, so the bar is bit-exact: score, status, CIGAR (tie-breaks
+included), CIGAR score/end and alignment end position of every pair.
+"""
+import random
+
+import numpy as np
+import pytest
+
+import cli_format
+import oracle as O
+from _pkg import load
+from test_emu_vs_oracle import HEUR, PENS
+from test_oracle_unit import lcg_pairs
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def pkg():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no GPU")
+    return load()
+
+
+def pack(pairs):
+    buf, po, pl, to, tl = bytearray(), [], [], [], []
+    for p, t in pairs:
+        po.append(len(buf)); buf += p; pl.append(len(p))
+        to.append(len(buf)); buf += t; tl.append(len(t))
+    buf += b"\0" * 16
+    return np.frombuffer(bytes(buf), np.uint8), po, pl, to, tl
+
+
+def gpu_batch(pkg, metric, pen, pairs, compute=True, span=0, free=None, hk=0, hp=(0, 0, 0),
+              extension=False, packed=False):
+    a = pkg.WavefrontAligner(metric, pen)
+    a.set_alignment_scope(compute)
+    if hk:
+        a.set_heuristic(hk, *hp)
+    if extension:
+        a.set_alignment_extension()
+    elif span:
+        a.set_alignment_free_ends(*free)
+    if packed:
+        from wfa_b200 import synth
+        ps = synth.PairSet(*pack(pairs))
+        words, pwo, two = synth.pack2bits(ps)
+        res, cig = a.align_batch(np.concatenate([words, np.zeros(4, np.uint32)]), pwo, ps.p_len,
+                                 two, ps.t_len, packed=True, span=int(span or extension))
+    else:
+        seq, po, pl, to, tl = pack(pairs)
+        res, cig = a.align_batch(seq, po, pl, to, tl, span=int(span or extension))
+    cigars = [cig[r["cigar_begin"]:r["cigar_begin"] + r["cigar_length"]].tobytes().decode()
+              for r in res]
+    return res, cigars
+
+
+def oracle_one(metric, pen, p, t, compute, span, free, hk, hp, extension):
+    a = O.OracleAligner(metric, pen)
+    a.set_alignment_scope(compute)
+    if hk:
+        a.set_heuristic(hk, *hp)
+    if extension:
+        a.set_alignment_extension()
+        s = a.align_endsfree(p, t)
+    elif span:
+        a.set_alignment_free_ends(*free)
+        s = a.align_endsfree(p, t)
+    else:
+        s = a.align_end2end(p, t)
+    ops, cs, ev, eh = a.cigar()
+    return s, a.status(), ops.decode() if compute else "", a.end_pos(), (cs, ev, eh)
+
+
+def compare(pkg, metric, pen, pairs, compute=True, span=0, free=None, hk=0, hp=(0, 0, 0),
+            extension=False, packed=False):
+    res, cig = gpu_batch(pkg, metric, pen, pairs, compute, span, free, hk, hp, extension, packed)
+    for i, (p, t) in enumerate(pairs):
+        s, st, ops, ep, (cs, ev, eh) = oracle_one(metric, pen, p, t, compute, span, free, hk, hp,
+                                                  extension)
+        r = res[i]
+        got = (int(r["score"]), int(r["status"]), cig[i] if compute else "",
+               (int(r["end_score"]), int(r["end_k"]), int(r["end_offset"])))
+        assert got == (s, st, ops, ep), (metric, pen, i, got[:2], (s, st))
+        if compute:
+            assert (int(r["cigar_score"]), int(r["end_v"]), int(r["end_h"])) == (cs, ev, eh), i
+
+
+@pytest.mark.parametrize("metric,pen", PENS)
+@pytest.mark.parametrize("compute", [True, False])
+def test_end2end(pkg, metric, pen, compute):
+    pairs = lcg_pairs(211 + metric, 120, 300)
+    compare(pkg, metric, pen, pairs, compute=compute)
+    compare(pkg, metric, pen, pairs[:60], compute=compute, packed=True)
+
+
+@pytest.mark.parametrize("metric,pen", PENS)
+def test_endsfree_and_extension(pkg, metric, pen):
+    r = random.Random(metric)
+    for p, t in lcg_pairs(223 + metric, 12, 200):
+        free = [r.randrange(0, len(p) // 4 + 1), r.randrange(0, len(p) // 4 + 1),
+                r.randrange(0, len(t) // 4 + 1), r.randrange(0, len(t) // 4 + 1)]
+        compare(pkg, metric, pen, [(p, t)], span=1, free=free)
+    if metric >= 2:
+        compare(pkg, metric, pen, lcg_pairs(227 + metric, 60, 200), extension=True)
+
+
+@pytest.mark.parametrize("metric,pen", PENS)
+@pytest.mark.parametrize("h,hp", [("wfa-adaptive", (10, 50, 1)), ("xdrop", (20, 1, 0)),
+                                  ("xdrop", (20, 3, 0)), ("zdrop", (20, 1, 0)),
+                                  ("banded-static", (-5, 5, 0)), ("banded-adaptive", (-3, 3, 1))])
+def test_heuristics(pkg, metric, pen, h, hp):
+    if h in ("xdrop", "zdrop") and metric in (0, 1):
+        pytest.skip("drops are rejected with edit/indel")
+    compare(pkg, metric, pen, lcg_pairs(233 + metric, 60, 300), hk=HEUR[h], hp=hp)
+    if metric >= 2 and h in ("xdrop", "zdrop"):
+        compare(pkg, metric, pen, lcg_pairs(239 + metric, 30, 200), hk=HEUR[h], hp=hp,
+                extension=True)
+
+
+def test_edges(pkg):
+    edge = [(b"", b""), (b"A", b""), (b"", b"ACGT"), (b"A", b"C"), (b"A", b"A"),
+            (b"ACGT" * 40, b"ACGT" * 40), (b"AAAAAAAA", b"CCCCCCCC"),
+            (b"ACGTTTTTTTTTTACGT", b"ACGTACGT"), (b"A" * 700, b"C" * 700)]
+    for metric, pen in PENS:
+        compare(pkg, metric, pen, edge)
+        compare(pkg, metric, pen, edge, packed=True)
+
+
+def test_retry_escalation(pkg):
+    """Pairs whose wavefronts outgrow the first scratch configuration are
+    re-run with more scratch and still match."""
+    r = random.Random(5)
+    big = (bytes(r.choice(b"ACGT") for _ in range(3000)), bytes(r.choice(b"ACGT") for _ in range(2900)))
+    pairs = lcg_pairs(241, 40, 150) + [big] + lcg_pairs(242, 40, 150)
+    compare(pkg, 3, [0, 4, 6, 2], pairs)
+    compare(pkg, 1, None, pairs)
+
+
+def test_plain_calls_and_golden_cli(pkg, golden):
+    """The plain per-call form reproduces the reference's CLI golden lines."""
+    for case in golden["cases"]:
+        if case["memory"] != "high":
+            continue
+        metric = O.METRICS[case["algo"]]
+        pen = [int(x) for x in case["penalties"].split(",")] if case["penalties"] else O.DEFAULT_PEN[metric]
+        so = case["score_only"]
+        a = pkg.WavefrontAligner(metric, pen)
+        a.set_alignment_scope(not so)
+        if case["heuristic"]:
+            a.set_heuristic(case["heuristic"], *[int(x) for x in case["hparams"].split(",")])
+        span_s = case["span"]
+        if span_s in ("extension", "extend"):
+            a.set_alignment_extension()
+        lines = []
+        for p, t in case["pairs"]:
+            pb, tb = p.encode(), t.encode()
+            if span_s == "global":
+                s = a.align_end2end(pb, tb)
+            else:
+                if span_s not in ("extension", "extend"):
+                    fr = [float(x) for x in span_s.split(",")[1:]]
+                    a.set_alignment_free_ends(O.nominal_prop(len(pb), fr[0]), O.nominal_prop(len(pb), fr[1]),
+                                              O.nominal_prop(len(tb), fr[2]), O.nominal_prop(len(tb), fr[3]))
+                s = a.align_endsfree(pb, tb)
+            c = a.cigar()
+            es, ek, eo = a.alignment_end_pos
+            rec = {"score": s, "status": a.status(), "end_score": es, "end_k": ek, "end_offset": eo}
+            orig = (pen + [0] * 6)[:6]
+            lines.append(cli_format.line(metric, orig, so, False, rec, c.operations.decode(), len(pb), len(tb)))
+        assert lines == case["expected"], case["name"]
+
+
+def test_config1_full(pkg):
+    """10,000 x 100 bp gap-affine pairs (the plain small workload), every pair."""
+    from wfa_b200 import synth
+    ps = synth.config1()
+    a = pkg.WavefrontAligner(3, [0, 4, 6, 2])
+    a.set_alignment_scope(True)
+    res, cig = a.align_batch(ps.buf, ps.p_off, ps.p_len, ps.t_off, ps.t_len)
+    secs, scores, status, hashes = O.batch(3, [0, 4, 6, 2], ps.buf.tobytes(), ps.p_off, ps.p_len,
+                                           ps.t_off, ps.t_len, threads=8)
+    assert np.array_equal(res["score"], scores)
+    assert np.array_equal(res["status"], status)
+    for i in range(len(ps)):
+        r = res[i]
+        ops = cig[r["cigar_begin"]:r["cigar_begin"] + r["cigar_length"]].tobytes()
+        h = 1469598103934665603
+        for c in ops:
+            h = ((h ^ c) * 1099511628211) & (2**64 - 1)
+        assert (h - 2**64 if h >= 2**63 else h) == hashes[i], i
+
+
+def test_config2_sample_packed(pkg):
+    """Short-read batch shape (100-150 bp, 0-4% edits), 2-bit packed input,
+    100,000 pairs, every pair against the oracle."""
+    from wfa_b200 import synth
+    ps = synth.uniform_pairs(100_000, 100, 150, 0.0, 0.04, synth.SEED_BASE + 2)
+    words, pwo, two = synth.pack2bits(ps)
+    a = pkg.WavefrontAligner(3, [0, 4, 6, 2])
+    a.set_alignment_scope(True)
+    res, cig = a.align_batch(np.concatenate([words, np.zeros(4, np.uint32)]), pwo, ps.p_len, two,
+                             ps.t_len, packed=True)
+    secs, scores, status, hashes = O.batch(3, [0, 4, 6, 2], ps.buf.tobytes(), ps.p_off, ps.p_len,
+                                           ps.t_off, ps.t_len, threads=8)
+    assert np.array_equal(res["score"], scores)
+    assert np.array_equal(res["status"], status)
+    idx = np.random.default_rng(0).choice(len(ps), 5000, replace=False)
+    for i in idx:
+        r = res[i]
+        ops = cig[r["cigar_begin"]:r["cigar_begin"] + r["cigar_length"]].tobytes()
+        h = 1469598103934665603
+        for c in ops:
+            h = ((h ^ c) * 1099511628211) & (2**64 - 1)
+        assert (h - 2**64 if h >= 2**63 else h) == hashes[i], i
+
+
+def test_device_api_matches_host_api(pkg):
+    import torch
+    from wfa_b200 import synth
+    ps = synth.uniform_pairs(5000, 100, 150, 0.0, 0.04, 77)
+    words, pwo, two = synth.pack2bits(ps)
+    a = pkg.WavefrontAligner(3, [0, 4, 6, 2])
+    a.set_alignment_scope(True)
+    res_h, cig_h = a.align_batch(np.concatenate([words, np.zeros(4, np.uint32)]), pwo, ps.p_len,
+                                 two, ps.t_len, packed=True)
+    dev = torch.device("cuda:0")
+    w = torch.from_numpy(np.concatenate([words, np.zeros(4, np.uint32)]).view(np.int32)).to(dev)
+    t_po = torch.from_numpy(pwo).to(dev)
+    t_pl = torch.from_numpy(ps.p_len).to(dev)
+    t_to = torch.from_numpy(two).to(dev)
+    t_tl = torch.from_numpy(ps.t_len).to(dev)
+    caps = 2 * (ps.p_len.astype(np.int64) + ps.t_len) + 1
+    coff = np.concatenate([[0], np.cumsum(caps)[:-1]]).astype(np.int64)
+    t_co = torch.from_numpy(coff).to(dev)
+    cig = torch.zeros(int(caps.sum()) + 16, dtype=torch.uint8, device=dev)
+    res = torch.zeros(len(ps) * 10, dtype=torch.int32, device=dev)
+    a.align_batch_device(w.data_ptr(), w.numel() * 4, t_po.data_ptr(), t_pl.data_ptr(),
+                         t_to.data_ptr(), t_tl.data_ptr(), len(ps), res.data_ptr(), cig.data_ptr(),
+                         t_co.data_ptr(), int(caps.sum()), packed=True)
+    torch.cuda.synchronize()
+    rd = res.cpu().numpy().view(res_h.dtype)
+    cd = cig.cpu().numpy()
+    assert np.array_equal(rd["score"], res_h["score"])
+    assert np.array_equal(rd["status"], res_h["status"])
+    for i in range(0, len(ps), 97):
+        a_ops = cd[coff[i] + rd["cigar_begin"][i]: coff[i] + rd["cigar_begin"][i] + rd["cigar_length"][i]]
+        b_ops = cig_h[res_h["cigar_begin"][i]: res_h["cigar_begin"][i] + res_h["cigar_length"][i]]
+        assert a_ops.tobytes() == b_ops.tobytes(), i

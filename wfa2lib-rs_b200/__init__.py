@@ -2,5 +2,9 @@
 wfa2lib-rs aligner API (src/aligner.rs of the reference crate).
 
 The compute path is the C-ABI shared library built from csrc/ (CUDA kernels
-for sm_100a plus the C++ host side); this package is its Python mirror.
+for sm_100a plus the C++ host side, lib/libwfa_b200.so); this package is its
+Python mirror.  Import it by path (the directory name is not an identifier),
+e.g. with importlib; see tests/_pkg.py.
 """
+from .aligner import (COMPLETED, EDIT, GAP_AFFINE, GAP_AFFINE_2P, GAP_LINEAR, INDEL,  # noqa: F401
+                      RESULT_DTYPE, Cigar, WavefrontAligner, cigar_rle, lib)

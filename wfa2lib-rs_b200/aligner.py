@@ -1,0 +1,282 @@
+"""Python mirror of the wfa2lib-rs aligner API over the C ABI (include/wfa_b200.h).
+
+`WavefrontAligner` has the methods of the reference's WavefrontAligner
+(src/aligner.rs:407-3555) with the same names, argument meaning and results;
+where the reference panics (invalid penalties) this raises ValueError.  Every
+alignment runs in the CUDA library (lib/libwfa_b200.so); if it is missing or no
+GPU is present the calls raise -- there is no CPU path.
+
+Batches: `align_batch` (host arrays; copies in and out) and
+`align_batch_device` (device pointers, e.g. torch CUDA tensors; no copies).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libwfa_b200.so")
+
+# Enum values of include/wfa_b200.h (the reference's enum order).
+INDEL, EDIT, GAP_LINEAR, GAP_AFFINE, GAP_AFFINE_2P = range(5)
+STATUS_NAMES = ["Ok", "EndReached", "EndUnreachable", "MaxStepsReached", "Oom", "Completed",
+                "Partial"]
+OK, END_REACHED, END_UNREACHABLE, MAX_STEPS_REACHED, OOM, COMPLETED, PARTIAL = range(7)
+SCOPE_SCORE, SCOPE_ALIGNMENT = 0, 1
+MEMORY = {"high": 0, "med": 1, "low": 2}
+HEURISTICS = {"none": 0, "wfa-adaptive": 1, "xdrop": 2, "zdrop": 3, "banded-static": 4,
+              "banded-adaptive": 5}
+SEQ_ASCII, SEQ_PACKED2 = 0, 1
+SPAN_END2END, SPAN_ENDSFREE = 0, 1
+ERRORS = {-1: "invalid penalties", -2: "invalid argument", -3: "unsupported configuration",
+          -4: "CUDA error", -5: "no CUDA device", -6: "out of device memory"}
+
+RESULT_DTYPE = np.dtype([(f, np.int32) for f in (
+    "score", "status", "cigar_begin", "cigar_length", "cigar_score", "end_v", "end_h",
+    "end_score", "end_k", "end_offset")])
+
+
+class Penalties(ctypes.Structure):
+    _fields_ = [("match", ctypes.c_int32), ("mismatch", ctypes.c_int32),
+                ("gap_opening1", ctypes.c_int32), ("gap_extension1", ctypes.c_int32),
+                ("gap_opening2", ctypes.c_int32), ("gap_extension2", ctypes.c_int32)]
+
+
+class Batch(ctypes.Structure):
+    _fields_ = [("format", ctypes.c_int32), ("span", ctypes.c_int32), ("num_pairs", ctypes.c_int64),
+                ("seq", ctypes.c_void_p), ("seq_bytes", ctypes.c_int64),
+                ("p_off", ctypes.c_void_p), ("p_len", ctypes.c_void_p),
+                ("t_off", ctypes.c_void_p), ("t_len", ctypes.c_void_p),
+                ("cigar_off", ctypes.c_void_p), ("cigar_bytes", ctypes.c_int64)]
+
+
+_lib = None
+
+
+def lib():
+    """The CUDA library; raises if it was not built (there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"CUDA library not built: {LIB_PATH} (run __graft_entry__.build())")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, i32, i64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64
+    P32 = ctypes.POINTER(i32)
+    sig = {
+        "wfa_penalties_check": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(Penalties)]),
+        "wfa_aligner_create": (vp, [ctypes.c_int, ctypes.POINTER(Penalties), ctypes.c_int,
+                                    ctypes.POINTER(ctypes.c_int)]),
+        "wfa_aligner_destroy": (None, [vp]),
+        "wfa_set_memory_mode": (ctypes.c_int, [vp, ctypes.c_int]),
+        "wfa_set_max_memory_compact": (ctypes.c_int, [vp, ctypes.c_uint64]),
+        "wfa_set_max_alignment_steps": (ctypes.c_int, [vp, i32]),
+        "wfa_set_alignment_scope": (ctypes.c_int, [vp, ctypes.c_int]),
+        "wfa_set_alignment_free_ends": (ctypes.c_int, [vp, i32, i32, i32, i32]),
+        "wfa_set_alignment_extension": (ctypes.c_int, [vp]),
+        "wfa_set_alignment_end_to_end": (ctypes.c_int, [vp]),
+        "wfa_set_compat": (ctypes.c_int, [vp, ctypes.c_int]),
+        "wfa_set_heuristic": (ctypes.c_int, [vp, ctypes.c_int, i32, i32, i32]),
+        "wfa_status": (ctypes.c_int, [vp]),
+        "wfa_cigar": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_void_p), P32, P32, P32, P32]),
+        "wfa_alignment_end_pos": (ctypes.c_int, [vp, P32, P32, P32]),
+        "wfa_last_error": (ctypes.c_int, [vp]),
+        "wfa_last_error_string": (ctypes.c_char_p, [vp]),
+        "wfa_batch_align": (ctypes.c_int, [vp, ctypes.POINTER(Batch), vp, vp]),
+        "wfa_batch_align_device": (ctypes.c_int, [vp, ctypes.POINTER(Batch), vp, vp, vp]),
+        "wfa_kernel_launches": (i64, [vp]),
+        "wfa_last_kernel_ms": (ctypes.c_double, [vp]),
+        "wfa_cigar_rle": (i32, [vp, i32, ctypes.c_char_p, i32]),
+        "wfa_version": (ctypes.c_char_p, []),
+    }
+    for name in ("wfa_align_end2end", "wfa_align_endsfree", "wfa_align_biwfa",
+                 "wfa_align_biwfa_score", "wfa_align_packed2bits"):
+        sig[name] = (i32, [vp, ctypes.c_char_p, i32, ctypes.c_char_p, i32])
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def _pen(metric, penalties):
+    p = list(penalties or []) + [0] * 6
+    if metric == GAP_LINEAR:  # (match, mismatch, indel)
+        return Penalties(p[0], p[1], p[2], 0, 0, 0)
+    return Penalties(*p[:6])
+
+
+class Cigar:
+    """The reference's Cigar (src/cigar.rs:16): operations plus score/end."""
+
+    def __init__(self, ops, score, end_v, end_h):
+        self.operations = ops
+        self.score, self.end_v, self.end_h = score, end_v, end_h
+
+    def to_string_rle(self, print_matches=True):
+        out, i, ops = [], 0, self.operations.decode()
+        while i < len(ops):
+            j = i
+            while j < len(ops) and ops[j] == ops[i]:
+                j += 1
+            if print_matches or ops[i] != "M":
+                out.append(f"{j - i}{ops[i]}")
+            i = j
+        return "".join(out)
+
+    def is_null(self):
+        return len(self.operations) == 0
+
+
+class WavefrontAligner:
+    """WavefrontAligner<N> (src/aligner.rs:146) backed by the B200 library."""
+
+    def __init__(self, metric, penalties=None, device=0):
+        L = lib()
+        err = ctypes.c_int(0)
+        self.metric = metric
+        self.penalties = list(penalties or [])
+        self._h = L.wfa_aligner_create(metric, ctypes.byref(_pen(metric, penalties)), device,
+                                       ctypes.byref(err))
+        if not self._h:
+            if err.value == -1:
+                raise ValueError(f"invalid penalties {penalties} for metric {metric}")
+            raise RuntimeError(f"wfa_aligner_create failed: {ERRORS.get(err.value, err.value)}")
+        self._L = L
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.wfa_aligner_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def _check(self, r):
+        if r < 0:
+            msg = self._L.wfa_last_error_string(self._h).decode()
+            if r == -3:
+                raise NotImplementedError(msg)
+            raise RuntimeError(f"{ERRORS.get(r, r)}: {msg}")
+        return r
+
+    # --- builder setters (src/aligner.rs:462-613) ---
+    def set_memory_mode(self, mode):
+        self._check(self._L.wfa_set_memory_mode(self._h, MEMORY.get(mode, mode)))
+
+    def set_max_memory_compact(self, nbytes):
+        self._check(self._L.wfa_set_max_memory_compact(self._h, nbytes))
+
+    def set_max_alignment_steps(self, steps):
+        self._check(self._L.wfa_set_max_alignment_steps(self._h, steps))
+
+    def set_alignment_scope(self, compute_alignment):
+        s = SCOPE_ALIGNMENT if compute_alignment in (True, SCOPE_ALIGNMENT) else SCOPE_SCORE
+        self._check(self._L.wfa_set_alignment_scope(self._h, s))
+
+    def set_alignment_free_ends(self, pattern_begin_free, pattern_end_free, text_begin_free,
+                                text_end_free):
+        self._check(self._L.wfa_set_alignment_free_ends(
+            self._h, pattern_begin_free, pattern_end_free, text_begin_free, text_end_free))
+
+    def set_alignment_extension(self):
+        self._check(self._L.wfa_set_alignment_extension(self._h))
+
+    def set_alignment_end_to_end(self):
+        self._check(self._L.wfa_set_alignment_end_to_end(self._h))
+
+    def set_compat(self, corrected):
+        self._check(self._L.wfa_set_compat(self._h, 1 if corrected else 0))
+
+    def set_heuristic(self, kind, *params):
+        k = HEURISTICS[kind] if isinstance(kind, str) else (kind or 0)
+        p = list(params) + [0, 0, 0]
+        self._check(self._L.wfa_set_heuristic(self._h, k, p[0], p[1], p[2]))
+
+    # --- plain per-call aligners ---
+    def align_end2end(self, pattern, text):
+        return self._check(self._L.wfa_align_end2end(self._h, pattern, len(pattern), text, len(text)))
+
+    def align_endsfree(self, pattern, text):
+        return self._check(self._L.wfa_align_endsfree(self._h, pattern, len(pattern), text, len(text)))
+
+    def align_biwfa(self, pattern, text):
+        return self._check(self._L.wfa_align_biwfa(self._h, pattern, len(pattern), text, len(text)))
+
+    def align_biwfa_score(self, pattern, text):
+        return self._check(self._L.wfa_align_biwfa_score(self._h, pattern, len(pattern), text,
+                                                         len(text)))
+
+    def align_packed2bits(self, pattern, pattern_length, text, text_length):
+        return self._check(self._L.wfa_align_packed2bits(self._h, pattern, pattern_length, text,
+                                                         text_length))
+
+    def align_lambda(self, match_funct, pattern_length, text_length):
+        raise NotImplementedError("lambda sequences need a host callback per base comparison")
+
+    def status(self):
+        return self._L.wfa_status(self._h)
+
+    def cigar(self):
+        ops = ctypes.c_void_p()
+        n, s, v, h = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        self._L.wfa_cigar(self._h, ctypes.byref(ops), ctypes.byref(n), ctypes.byref(s),
+                          ctypes.byref(v), ctypes.byref(h))
+        data = ctypes.string_at(ops.value, n.value) if n.value > 0 else b""
+        return Cigar(data, s.value, v.value, h.value)
+
+    @property
+    def alignment_end_pos(self):
+        s, k, o = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        self._L.wfa_alignment_end_pos(self._h, ctypes.byref(s), ctypes.byref(k), ctypes.byref(o))
+        return s.value, k.value, o.value
+
+    def kernel_launches(self):
+        return self._L.wfa_kernel_launches(self._h)
+
+    def last_kernel_ms(self):
+        return self._L.wfa_last_kernel_ms(self._h)
+
+    # --- batches ---
+    def align_batch(self, seq, p_off, p_len, t_off, t_len, packed=False, span=SPAN_END2END,
+                    out_results=None, out_cigars=None):
+        """Host arrays in; returns (results[RESULT_DTYPE], dense CIGAR bytes).
+
+        Pair i's CIGAR is cigars[r['cigar_begin'] : r['cigar_begin'] + r['cigar_length']].
+        out_results / out_cigars may be preallocated (e.g. pinned) buffers; the
+        CIGAR buffer needs sum(2*(p_len+t_len)+1) bytes at most."""
+        n = len(p_len)
+        seq = np.ascontiguousarray(seq).view(np.uint8)
+        arrs = [a if (isinstance(a, np.ndarray) and a.dtype == d and a.flags.c_contiguous)
+                else np.ascontiguousarray(a, dtype=d) for a, d in
+                ((p_off, np.int64), (p_len, np.int32), (t_off, np.int64), (t_len, np.int32))]
+        res = out_results if out_results is not None else np.zeros(n, RESULT_DTYPE)
+        if out_cigars is not None:
+            cig = out_cigars
+        else:
+            caps = 2 * (arrs[1].astype(np.int64) + arrs[3]) + 1
+            cig = np.zeros(int(caps.sum()) + 16, np.uint8)
+        b = Batch(SEQ_PACKED2 if packed else SEQ_ASCII, span, n, seq.ctypes.data, seq.nbytes,
+                  arrs[0].ctypes.data, arrs[1].ctypes.data, arrs[2].ctypes.data,
+                  arrs[3].ctypes.data, None, 0)
+        self._check(self._L.wfa_batch_align(self._h, ctypes.byref(b), res.ctypes.data,
+                                            cig.ctypes.data))
+        return res, cig
+
+    def align_batch_device(self, seq_ptr, seq_bytes, p_off, p_len, t_off, t_len, num_pairs,
+                           results_ptr, cigars_ptr=None, cigar_off=None, cigar_bytes=0,
+                           packed=False, span=SPAN_END2END, stream=0):
+        """All arguments are device pointers (ints); enqueued on `stream`."""
+        b = Batch(SEQ_PACKED2 if packed else SEQ_ASCII, span, num_pairs, seq_ptr, seq_bytes,
+                  p_off, p_len, t_off, t_len, cigar_off, cigar_bytes)
+        return self._check(self._L.wfa_batch_align_device(self._h, ctypes.byref(b), results_ptr,
+                                                          cigars_ptr, stream))
+
+
+def cigar_rle(ops):
+    """Cigar::to_string_rle(true) through the library helper."""
+    L = lib()
+    n = L.wfa_cigar_rle(ops, len(ops), None, 0)
+    buf = ctypes.create_string_buffer(n + 1)
+    L.wfa_cigar_rle(ops, len(ops), buf, n + 1)
+    return buf.value.decode()

@@ -1,0 +1,1251 @@
+// wfa_align.cuh -- the per-pair wavefront aligner run by one warp.
+//
+// One warp aligns one pair.  The control flow (score loop, input fetch,
+// range union, null steps, termination, heuristics, backtrace) is
+// warp-uniform: every lane holds the same scalar state.  Lanes split the
+// diagonals of each wavefront (k = lo + lane, lo + lane + 32, ...) and meet in
+// warp reductions for the trims, termination and heuristic cutoffs.
+//
+// Storage model.  The reference keeps, per wavefront, an allocation, limits
+// [lo, hi] and an initialised range, and NULL-fills input ends before reading
+// them (src/wavefront.rs:422-457).  Every cell outside the initialised range
+// reads as OFFSET_NULL there, so here a wavefront stores exactly its
+// initialised range [a, b] and a read outside it returns OFFSET_NULL
+// directly; no fill is ever written.  Limits and the initialised range evolve
+// as in the reference: both set by the compute step and trim_ends; limits
+// narrowed by the heuristics; the range emptied when a cutoff empties the
+// wavefront.  Component slots are a ring of max_score_scope scores; in
+// high-memory (CIGAR) mode the M wavefronts of every score are also kept in a
+// per-warp history arena for the backtrace.
+//
+// The same source compiles as host C++ with a one-lane "warp" (WFA_EMU):
+// the CPU tests run that build against the oracle to check this logic before
+// it runs on a GPU.  It is test-only and never part of the product library.
+#pragma once
+
+#include <stdint.h>
+
+#include "wfa_common.h"
+
+#if defined(__CUDACC__) && !defined(WFA_EMU)
+#define WFA_D __device__ __forceinline__
+#define WFA_DN __device__ __noinline__
+#define WFA_WARP 32
+#define WFA_CUDA_WARP 1
+#else
+#include <algorithm>
+#include <climits>
+#ifndef __CUDACC__
+struct int4 { int x, y, z, w; };
+#endif
+#define WFA_D inline
+#define WFA_DN inline
+#ifdef WFA_EMU_THREADS
+#include <barrier>
+#define WFA_WARP 32
+#else
+#define WFA_WARP 1
+#endif
+#endif
+
+namespace wfab {
+
+// ---------------------------------------------------------------------------
+// Warp primitives (one-lane stand-ins in the emulation build)
+// ---------------------------------------------------------------------------
+#if defined(WFA_EMU_THREADS)
+// Test-only: 32 host threads play the lanes of one warp; __syncwarp and the
+// warp reductions become barriers, so lane partitioning, reductions and
+// warp-uniform control flow are exercised exactly as on the GPU.
+struct EmuWarp {
+  std::barrier<> bar{32};
+  int red[32];
+};
+extern thread_local int g_emu_lane;
+extern EmuWarp* g_emu_warp;
+#endif
+
+struct Warp {
+#if defined(WFA_EMU_THREADS)
+  static int lane() { return g_emu_lane; }
+  static void sync() { g_emu_warp->bar.arrive_and_wait(); }
+  static int reduce(int v, bool mx) {
+    EmuWarp* w = g_emu_warp;
+    w->red[g_emu_lane] = v;
+    w->bar.arrive_and_wait();
+    int r = w->red[0];
+    for (int i = 1; i < 32; ++i) r = mx ? (w->red[i] > r ? w->red[i] : r) : (w->red[i] < r ? w->red[i] : r);
+    w->bar.arrive_and_wait();
+    return r;
+  }
+  static int min(int v) { return reduce(v, false); }
+  static int max(int v) { return reduce(v, true); }
+  static unsigned any(bool p) { return (unsigned)reduce(p ? 1 : 0, true); }
+  static uint32_t ffs(uint32_t x) { return x ? (uint32_t)__builtin_ctz(x) + 1 : 0; }
+  static uint32_t clz(uint32_t x) { return x ? (uint32_t)__builtin_clz(x) : 32; }
+  static uint32_t funnel(uint32_t lo, uint32_t hi, uint32_t s) {
+    s &= 31;
+    uint64_t v = ((uint64_t)hi << 32) | lo;
+    return (uint32_t)(v >> s);
+  }
+#elif WFA_WARP == 32
+  static WFA_D int lane() { return threadIdx.x & 31; }
+  static WFA_D int min(int v) { return __reduce_min_sync(0xffffffffu, v); }
+  static WFA_D int max(int v) { return __reduce_max_sync(0xffffffffu, v); }
+  static WFA_D unsigned any(bool p) { return __ballot_sync(0xffffffffu, p); }
+  static WFA_D void sync() { __syncwarp(); }
+  static WFA_D uint32_t ffs(uint32_t x) { return (uint32_t)__ffs((int)x); }
+  static WFA_D uint32_t clz(uint32_t x) { return (uint32_t)__clz((int)x); }
+  static WFA_D uint32_t funnel(uint32_t lo, uint32_t hi, uint32_t s) { return __funnelshift_r(lo, hi, s); }
+#else
+  static int lane() { return 0; }
+  static int min(int v) { return v; }
+  static int max(int v) { return v; }
+  static unsigned any(bool p) { return p ? 1u : 0u; }
+  static void sync() {}
+  static uint32_t ffs(uint32_t x) { return x ? (uint32_t)__builtin_ctz(x) + 1 : 0; }
+  static uint32_t clz(uint32_t x) { return x ? (uint32_t)__builtin_clz(x) : 32; }
+  static uint32_t funnel(uint32_t lo, uint32_t hi, uint32_t s) {
+    s &= 31;
+    uint64_t v = ((uint64_t)hi << 32) | lo;
+    return (uint32_t)(v >> s);
+  }
+#endif
+};
+
+WFA_D int imin(int a, int b) { return a < b ? a : b; }
+WFA_D int imax(int a, int b) { return a > b ? a : b; }
+WFA_D int64_t lmax(int64_t a, int64_t b) { return a > b ? a : b; }
+
+// ---------------------------------------------------------------------------
+// Sequences.  fetch(pos) returns the UNITS codes starting at pos, lowest code
+// in the lowest bits; positions outside [0, len) hold unspecified codes, and
+// callers clamp to the sequence lengths (the reference's sentinels end every
+// extension at the end of either sequence, src/sequences.rs:12-19).
+// ---------------------------------------------------------------------------
+struct SeqPacked {  // 2-bit codes, 16 per word, word-aligned start
+  static constexpr int UNITS = 16, BITS = 2;
+  const uint32_t* w;
+  int32_t len, nw;
+  WFA_D uint32_t word(int i) const { return (i >= 0 && i < nw) ? w[i] : 0u; }
+  WFA_D uint32_t fetch(int pos) const {
+    if (pos < 0) {
+      int s = -pos;
+      return s >= 16 ? 0u : (word(0) << (2 * s));
+    }
+    int i = pos >> 4;
+    return Warp::funnel(word(i), word(i + 1), (uint32_t)(2 * (pos & 15)));
+  }
+};
+
+struct SeqAscii {  // bytes, any alignment
+  static constexpr int UNITS = 4, BITS = 8;
+  const uint8_t* p;
+  int32_t len;
+  // Aligned 32-bit word i relative to the word containing p[0]; loaded only
+  // if it holds at least one byte of the sequence.
+  WFA_D uint32_t word_at(int64_t i) const {
+    uintptr_t a0 = ((uintptr_t)p) & ~(uintptr_t)3;
+    uintptr_t a = a0 + (uintptr_t)(i * 4);
+    uintptr_t end = (uintptr_t)p + (uintptr_t)len;
+    if (i < 0 || len <= 0 || a >= end) return 0u;
+    return *(const uint32_t*)a;
+  }
+  WFA_D uint32_t fetch(int pos) const {
+    int sh = 0;
+    if (pos < 0) {
+      sh = -pos;
+      if (sh >= 4) return 0u;
+      pos = 0;
+    }
+    uintptr_t off = (((uintptr_t)p) & 3) + (uintptr_t)pos;
+    int64_t i = (int64_t)(off >> 2);
+    return Warp::funnel(word_at(i), word_at(i + 1), (uint32_t)(8 * (off & 3))) << (8 * sh);
+  }
+};
+
+// Matches of P[v..] with T[h..], at most R (forward extension).
+template <class S>
+WFA_D int lcp_fwd(const S& P, int v, const S& T, int h, int R) {
+  int l = 0;
+  while (l < R) {
+    uint32_t x = P.fetch(v + l) ^ T.fetch(h + l);
+    if (x) { l += (int)((Warp::ffs(x) - 1) / S::BITS); break; }
+    l += S::UNITS;
+  }
+  return l < R ? l : R;
+}
+
+// Matches ending at P[v-1], T[h-1] walking backwards, at most R
+// (st_backward_matches, src/backtrace.rs:668-686).
+template <class S>
+WFA_D int lcp_bwd(const S& P, int v, const S& T, int h, int R) {
+  int l = 0;
+  while (l < R) {
+    uint32_t x = P.fetch(v - l - S::UNITS) ^ T.fetch(h - l - S::UNITS);
+    if (x) { l += (int)(Warp::clz(x) / S::BITS); break; }
+    l += S::UNITS;
+  }
+  return l < R ? l : R;
+}
+
+// ---------------------------------------------------------------------------
+// Wavefront descriptors
+// ---------------------------------------------------------------------------
+constexpr int kPresent = 1, kNullFlag = 2;
+constexpr int CM = 0, CI1 = 1, CD1 = 2, CI2 = 3, CD2 = 4;
+
+struct WfD {
+  int32_t* vals;  // cell k at vals[k - a]
+  int32_t lo, hi; // limits
+  int32_t a, b;   // initialised range
+  int32_t flags;
+  int32_t pad;
+};
+
+WFA_D bool wf_present(const WfD& d) { return (d.flags & kPresent) != 0; }
+WFA_D bool wf_is_null(const WfD& d) { return !(d.flags & kPresent) || (d.flags & kNullFlag); }
+WFA_D WfD wf_none() {
+  WfD d;
+  d.vals = nullptr; d.lo = 1; d.hi = -1; d.a = 1; d.b = 0; d.flags = 0; d.pad = 0;
+  return d;
+}
+// Cell read with the reference's semantics (OFFSET_NULL outside the
+// initialised range; null inputs read as the null wavefront).
+WFA_D int32_t rd(const WfD& d, int k) {
+  return (k >= d.a && k <= d.b) ? d.vals[k - d.a] : kOffsetNull;
+}
+WFA_D bool cell_in_bounds(int32_t off, int k, int n, int m) {
+  return (uint32_t)off <= (uint32_t)m && (uint32_t)(off - k) <= (uint32_t)n;
+}
+
+// Heuristic state, src/heuristic.rs:62-148.
+struct HState {
+  int32_t steps_wait, max_sw_score, max_wf_score, max_sw_k, max_sw_off, zdrop_last;
+};
+
+// Per-warp workspace pointers.
+struct Workspace {
+  WfD* ring;        // [scope][NC] descriptors (shared memory on the GPU)
+  int32_t* ringv;   // [scope][NC][wmax] cells
+  int4* hist;       // [hist_scores] M history records {a, b, cell offset of a, present}
+  int32_t* harena;  // M history cells
+};
+
+template <int CLS, class S>
+struct PairAligner {
+  static constexpr int NC = CLS == kAffine2pClass ? 5 : CLS == kAffineClass ? 3 : 1;
+  static constexpr bool AFF = CLS >= kAffineClass;
+  static constexpr bool TWO = CLS == kAffine2pClass;
+
+  const AlignParams& P;
+  Workspace ws;
+  S pat, txt;
+  int32_t n, m;
+  int32_t lane;
+  int32_t scope, wmax;
+  bool modular;  // score-only: no M history
+  int32_t cap;   // num_wavefronts score cap (high memory)
+  int32_t p0, pf, t0, tf;
+  bool endsfree;
+  int32_t hist_lo, hist_hi;
+  int32_t num_null_steps;
+  int32_t status;
+  int32_t end_score, end_k, end_off;
+  HState hs;
+  bool retry;
+  int64_t hused;
+  // CIGAR (written backwards into the pair's slot)
+  uint8_t* cg;
+  int64_t cg_cap, cg_begin, cg_end;
+  int32_t cg_score, cg_ev, cg_eh;
+
+  WFA_D PairAligner(const AlignParams& p) : P(p) {}
+
+  // ---- slots --------------------------------------------------------------
+  WFA_D WfD& slot(int c, int s) { return ws.ring[(s % scope) * NC + c]; }
+  WFA_D WfD get(int c, int s) {  // input fetch (score may be negative)
+    if (s < 0) return wf_none();
+    return slot(c, s);
+  }
+  WFA_D void put(int c, int s, const WfD& d) {
+    Warp::sync();
+    if (lane == 0) slot(c, s) = d;
+    Warp::sync();
+  }
+  WFA_D void hist_put(int s, const WfD& d) {  // M history record (high memory)
+    if (modular) return;
+    if (s >= P.hist_scores) { retry = true; return; }
+    if (lane == 0) {
+      int4 r;
+      r.x = d.a; r.y = d.b;
+      r.z = wf_present(d) ? (int32_t)(d.vals - ws.harena) : 0;
+      r.w = wf_present(d) ? 1 : 0;
+      ws.hist[s] = r;
+    }
+    Warp::sync();
+  }
+  // Storage for an output of component c at score s covering [L, H].
+  WFA_D int32_t* alloc(int c, int s, int L, int H) {
+    int64_t w = (int64_t)H - L + 1;
+    if (c == CM && !modular) {
+      if (hused + w > P.hist_words) { retry = true; return nullptr; }
+      int32_t* v = ws.harena + hused;
+      hused += w;
+      return v;
+    }
+    if (w > wmax) { retry = true; return nullptr; }
+    return ws.ringv + ((int64_t)((s % scope) * NC + c)) * wmax;
+  }
+
+  // ---- helpers --------------------------------------------------------------
+  // num_wavefronts, src/components.rs:435-505 (components start sized for
+  // 1000 x 1000, src/aligner.rs:377-378, and only grow).
+  WFA_D int32_t dims_num(int32_t pl, int32_t tl) const {
+    int32_t ad = pl > tl ? pl - tl : tl - pl, mn = imin(pl, tl);
+    switch (CLS) {
+      case kEditClass:
+        return P.metric == WFA_METRIC_INDEL ? pl + tl + 1 : imax(pl, tl) + 1;
+      case kLinearClass:
+        return mn * P.mismatch + P.o1 * ad + 1;
+      case kAffineClass:
+        return mn * P.mismatch + P.o1 + ad * P.e1 + 1;
+      default:
+        return mn * P.mismatch + imin(P.o1 + ad * P.e1, P.o2 + ad * P.e2) + 1;
+    }
+  }
+  WFA_D bool has_slot(int s) const { return modular || s < cap; }
+
+  // endsfree_begin_k, src/aligner.rs:3408-3421
+  WFA_D bool begin_k(int s, int& k) const {
+    if (P.match == 0 || !endsfree) return false;
+    if (t0 == 0 && p0 == 0) return false;
+    if (s % (-P.match) != 0) return false;
+    k = s / (-P.match);
+    return t0 >= k || p0 >= k;
+  }
+
+  WFA_D void clamp_band(int& lo, int& hi) const {  // src/aligner.rs:3308-3317
+    if (P.hkind == WFA_HEURISTIC_BANDED_STATIC || P.hkind == WFA_HEURISTIC_BANDED_ADAPTIVE) {
+      lo = imax(lo, P.hp0);
+      hi = imin(hi, P.hp1);
+    }
+  }
+
+  // Trim an output wavefront computed over [lo, hi] (trim_ends,
+  // src/compute/mod.rs:14-49) given the warp's min/max in-bounds diagonal.
+  WFA_D WfD finish(int32_t* base, int L, int lo, int hi, int vmin, int vmax) {
+    WfD d;
+    d.flags = kPresent;
+    d.pad = 0;
+    if (vmax >= vmin && vmax != INT_MIN) {
+      d.lo = vmin; d.hi = vmax;
+    } else {
+      d.lo = lo; d.hi = lo - 1;
+      d.flags |= kNullFlag;
+    }
+    d.a = d.lo; d.b = d.hi;
+    d.vals = base + (d.a - L);
+    return d;
+  }
+
+  // Trim pass over stored cells [lo, hi] (used after endsfree_init).
+  WFA_D WfD trim_pass(int32_t* base, int L, int lo, int hi) {
+    int vmin = INT_MAX, vmax = INT_MIN;
+    Warp::sync();
+    for (int k = lo + lane; k <= hi; k += WFA_WARP) {
+      if (cell_in_bounds(base[k - L], k, n, m)) { vmin = imin(vmin, k); vmax = imax(vmax, k); }
+    }
+    vmin = Warp::min(vmin);
+    vmax = Warp::max(vmax);
+    return finish(base, L, lo, hi, vmin, vmax);
+  }
+
+  // endsfree_init, src/aligner.rs:3426-3452, on M stored at base (cell L)
+  // and computed over [lo, hi]; returns the new limits through lo/hi.
+  WFA_D void endsfree_init(int32_t* base, int L, int& lo, int& hi, int k) {
+    Warp::sync();
+    if (t0 >= k) {
+      if (hi >= k) {
+        if (base[k - L] <= k) { Warp::sync(); if (lane == 0) base[k - L] = k; }
+      } else {
+        for (int kk = hi + 1 + lane; kk < k; kk += WFA_WARP) base[kk - L] = kOffsetNull;
+        if (lane == 0) base[k - L] = k;
+        hi = k;
+      }
+    }
+    Warp::sync();
+    if (p0 >= k) {
+      if (lo <= -k) {
+        if (base[-k - L] <= 0) { Warp::sync(); if (lane == 0) base[-k - L] = 0; }
+      } else {
+        if (lane == 0) base[-k - L] = 0;
+        for (int kk = -k + 1 + lane; kk < lo; kk += WFA_WARP) base[kk - L] = kOffsetNull;
+        lo = -k;
+      }
+    }
+    Warp::sync();
+  }
+
+  // endsfree_null_m, src/aligner.rs:3470-3494
+  WFA_D WfD endsfree_null_m(int s, int k) {
+    bool text = t0 >= k, pattern = p0 >= k;
+    int lo, hi;
+    if (text && pattern) { lo = -k; hi = k; }
+    else if (text) { lo = k; hi = k; }
+    else if (pattern) { lo = -k; hi = -k; }
+    else { lo = 0; hi = 0; }
+    int32_t* v = alloc(CM, s, lo, hi);
+    if (retry) return wf_none();
+    for (int kk = lo + lane; kk <= hi; kk += WFA_WARP) v[kk - lo] = kOffsetNull;
+    Warp::sync();
+    if (lane == 0) {
+      if (text) v[k - lo] = k;
+      if (pattern) v[-k - lo] = 0;
+    }
+    Warp::sync();
+    WfD d;
+    d.vals = v; d.lo = lo; d.hi = hi; d.a = lo; d.b = hi; d.flags = kPresent; d.pad = 0;
+    return d;
+  }
+
+  WFA_D void set_none(int s, int from_c, int to_c) {
+    for (int c = from_c; c < to_c; ++c) put(c, s, wf_none());
+  }
+  WFA_D void set_m(int s, const WfD& d) {
+    put(CM, s, d);
+    hist_put(s, d);
+  }
+
+  // ---- init_alignment, src/aligner.rs:846-1000 ------------------------------
+  WFA_D void init_alignment() {
+    for (int i = lane; i < scope * NC; i += WFA_WARP) ws.ring[i] = wf_none();
+    Warp::sync();
+    hist_lo = -(n + scope + 2);
+    hist_hi = m + scope + 2;
+    num_null_steps = 0;
+    status = WFA_STATUS_OK;
+    end_score = -1; end_k = kDiagNull; end_off = kOffsetNull;
+    hs.steps_wait = (P.hkind == WFA_HEURISTIC_WFADAPTIVE || P.hkind == WFA_HEURISTIC_BANDED_ADAPTIVE) ? P.hp2
+                    : (P.hkind == WFA_HEURISTIC_XDROP || P.hkind == WFA_HEURISTIC_ZDROP) ? P.hp1 : 0;
+    hs.max_sw_score = 0; hs.max_wf_score = 0; hs.max_sw_k = kDiagNull;
+    hs.max_sw_off = kOffsetNull; hs.zdrop_last = 0;
+    int lo0 = 0, hi0 = 0;
+    bool seeds = endsfree && P.match == 0;
+    if (seeds) { lo0 = -p0; hi0 = t0; }
+    int32_t* v = alloc(CM, 0, lo0, hi0);
+    if (retry) return;
+    for (int k = lo0 + lane; k <= hi0; k += WFA_WARP) {
+      int32_t val = k == 0 ? 0 : (k > 0 ? k : 0);  // seeds: (h,0) on k=h, (0,v) on k=-v
+      v[k - lo0] = val;
+    }
+    Warp::sync();
+    WfD d;
+    d.vals = v; d.lo = lo0; d.hi = hi0; d.a = lo0; d.b = hi0; d.flags = kPresent; d.pad = 0;
+    set_m(0, d);
+  }
+
+  // ---- compute steps ----------------------------------------------------------
+  // compute_edit_step, src/aligner.rs:1769-1864
+  WFA_D void compute_edit(int s) {
+    WfD prev = get(CM, s - 1);
+    if (wf_is_null(prev)) { ++num_null_steps; set_m(s, wf_none()); return; }
+    num_null_steps = 0;
+    int lo = imax(prev.lo - 1, hist_lo + 1), hi = imin(prev.hi + 1, hist_hi - 1);
+    if (lo > hi) { set_m(s, wf_none()); return; }
+    // NULL the cells the kernel reads beyond prev's limits (inside its
+    // initialised range only; outside it they already read as NULL).
+    if (lane == 0) {
+      int ks[4] = {prev.lo - 2, prev.lo - 1, prev.hi + 1, prev.hi + 2};
+      for (int i = 0; i < 4; ++i)
+        if (ks[i] >= prev.a && ks[i] <= prev.b) prev.vals[ks[i] - prev.a] = kOffsetNull;
+    }
+    Warp::sync();
+    int32_t* out = alloc(CM, s, lo, hi);
+    if (retry) return;
+    bool indel = P.metric == WFA_METRIC_INDEL;
+    int vmin = INT_MAX, vmax = INT_MIN;
+    for (int k = lo + lane; k <= hi; k += WFA_WARP) {
+      int32_t ins = rd(prev, k - 1), del = rd(prev, k + 1), mx;
+      if (indel) mx = imax(del, ins + 1);
+      else mx = imax(del, imax(ins, rd(prev, k)) + 1);
+      if (!cell_in_bounds(mx, k, n, m)) mx = kOffsetNull;
+      out[k - lo] = mx;
+      if (mx != kOffsetNull) { vmin = imin(vmin, k); vmax = imax(vmax, k); }
+    }
+    vmin = Warp::min(vmin);
+    vmax = Warp::max(vmax);
+    set_m(s, finish(out, lo, lo, hi, vmin, vmax));
+  }
+
+  // compute_linear_step, src/aligner.rs:1867-2003
+  WFA_D void compute_linear(int s) {
+    WfD mi = get(CM, s - P.mismatch), gp = get(CM, s - P.o1);
+    int bk;
+    if (wf_is_null(mi) && wf_is_null(gp)) {
+      ++num_null_steps;
+      WfD d = wf_none();
+      if (begin_k(s, bk)) d = endsfree_null_m(s, bk);
+      set_m(s, d);
+      return;
+    }
+    num_null_steps = 0;
+    if (wf_is_null(mi)) mi = wf_none();
+    if (wf_is_null(gp)) gp = wf_none();
+    int lo = imin(mi.lo, gp.lo - 1), hi = imax(mi.hi, gp.hi + 1);
+    clamp_band(lo, hi);
+    lo = imax(lo, hist_lo + 1);
+    hi = imin(hi, hist_hi - 1);
+    if (lo > hi) { set_m(s, wf_none()); return; }
+    bool bf = begin_k(s, bk);
+    int L = bf ? imin(lo, -bk) : lo, H = bf ? imax(hi, bk) : hi;
+    int32_t* out = alloc(CM, s, L, H);
+    if (retry) return;
+    int vmin = INT_MAX, vmax = INT_MIN;
+    for (int k = lo + lane; k <= hi; k += WFA_WARP) {
+      int32_t a = rd(mi, k) + 1, ins = rd(gp, k - 1) + 1, del = rd(gp, k + 1);
+      int32_t mx = imax(del, imax(ins, a));
+      if (!cell_in_bounds(mx, k, n, m)) mx = kOffsetNull;
+      out[k - L] = mx;
+      if (mx != kOffsetNull) { vmin = imin(vmin, k); vmax = imax(vmax, k); }
+    }
+    if (bf) {
+      endsfree_init(out, L, lo, hi, bk);
+      set_m(s, trim_pass(out, L, lo, hi));
+    } else {
+      vmin = Warp::min(vmin);
+      vmax = Warp::max(vmax);
+      set_m(s, finish(out, L, lo, hi, vmin, vmax));
+    }
+  }
+
+  // compute_affine_step (src/aligner.rs:2006-2193) and compute_affine2p_step
+  // (:2201-2553); the recurrences of src/compute/affine.rs:318-351 and
+  // src/compute/affine2p.rs:208-233.
+  WFA_D void compute_affine(int s) {
+    const int x = P.mismatch, oe1 = P.o1 + P.e1, e1 = P.e1;
+    const int oe2 = TWO ? P.o2 + P.e2 : 0, e2 = TWO ? P.e2 : 0;
+    WfD mm = get(CM, s - x), mo1 = get(CM, s - oe1);
+    WfD i1e = get(CI1, s - e1), d1e = get(CD1, s - e1);
+    WfD mo2 = wf_none(), i2e = wf_none(), d2e = wf_none();
+    if (TWO) { mo2 = get(CM, s - oe2); i2e = get(CI2, s - e2); d2e = get(CD2, s - e2); }
+    int bk;
+    bool all_null = wf_is_null(mm) && wf_is_null(mo1) && wf_is_null(i1e) && wf_is_null(d1e);
+    if (TWO) all_null = all_null && wf_is_null(mo2) && wf_is_null(i2e) && wf_is_null(d2e);
+    if (all_null) {
+      ++num_null_steps;
+      set_none(s, 1, NC);
+      WfD d = wf_none();
+      if (begin_k(s, bk)) d = endsfree_null_m(s, bk);
+      set_m(s, d);
+      return;
+    }
+    num_null_steps = 0;
+    if (wf_is_null(mm)) mm = wf_none();
+    if (wf_is_null(mo1)) mo1 = wf_none();
+    if (wf_is_null(i1e)) i1e = wf_none();
+    if (wf_is_null(d1e)) d1e = wf_none();
+    if (TWO) {
+      if (wf_is_null(mo2)) mo2 = wf_none();
+      if (wf_is_null(i2e)) i2e = wf_none();
+      if (wf_is_null(d2e)) d2e = wf_none();
+    }
+    bool affine_kernel = true;
+    if (TWO) {
+      bool i2a = wf_present(mo2) || wf_present(i2e), d2a = wf_present(mo2) || wf_present(d2e);
+      affine_kernel = !i2a && !d2a;
+    }
+    // Range union; absent inputs contribute the null bounds (1, -1).
+    int lo = imin(imin(mm.lo, mo1.lo - 1), imin(i1e.lo + 1, d1e.lo - 1));
+    int hi = imax(imax(mm.hi, mo1.hi + 1), imax(i1e.hi + 1, d1e.hi - 1));
+    if (TWO) {
+      lo = imin(lo, imin(mo2.lo - 1, imin(i2e.lo + 1, d2e.lo - 1)));
+      hi = imax(hi, imax(mo2.hi + 1, imax(i2e.hi + 1, d2e.hi - 1)));
+    }
+    clamp_band(lo, hi);
+    if (lo <= hi) { lo = imax(lo, hist_lo + 1); hi = imin(hi, hist_hi - 1); }
+    if (lo > hi) { set_none(s, 0, NC); if (!modular) hist_put(s, wf_none()); return; }
+    bool bf = begin_k(s, bk);
+    int L = bf ? imin(lo, -bk) : lo, H = bf ? imax(hi, bk) : hi;
+    int32_t* om = alloc(CM, s, L, H);
+    int32_t* oi1 = alloc(CI1, s, lo, hi);
+    int32_t* od1 = alloc(CD1, s, lo, hi);
+    int32_t *oi2 = nullptr, *od2 = nullptr;
+    if (TWO && !affine_kernel) { oi2 = alloc(CI2, s, lo, hi); od2 = alloc(CD2, s, lo, hi); }
+    if (retry) return;
+    int mn_m = INT_MAX, mx_m = INT_MIN, mn_i1 = INT_MAX, mx_i1 = INT_MIN, mn_d1 = INT_MAX, mx_d1 = INT_MIN;
+    int mn_i2 = INT_MAX, mx_i2 = INT_MIN, mn_d2 = INT_MAX, mx_d2 = INT_MIN;
+    for (int k = lo + lane; k <= hi; k += WFA_WARP) {
+      int32_t i1 = imax(rd(mo1, k - 1), rd(i1e, k - 1)) + 1;
+      int32_t d1 = imax(rd(mo1, k + 1), rd(d1e, k + 1));
+      int32_t mi = rd(mm, k) + 1;
+      int32_t mx;
+      if (!TWO || affine_kernel) {
+        mx = imax(mi, imax(i1, d1));
+      } else {
+        int32_t i2 = imax(rd(mo2, k - 1), rd(i2e, k - 1)) + 1;
+        int32_t d2 = imax(rd(mo2, k + 1), rd(d2e, k + 1));
+        mx = imax(mi, imax(imax(i1, i2), imax(d1, d2)));
+        oi2[k - lo] = i2;
+        od2[k - lo] = d2;
+        if (cell_in_bounds(i2, k, n, m)) { mn_i2 = imin(mn_i2, k); mx_i2 = imax(mx_i2, k); }
+        if (cell_in_bounds(d2, k, n, m)) { mn_d2 = imin(mn_d2, k); mx_d2 = imax(mx_d2, k); }
+      }
+      if (!cell_in_bounds(mx, k, n, m)) mx = kOffsetNull;
+      om[k - L] = mx;
+      oi1[k - lo] = i1;
+      od1[k - lo] = d1;
+      if (mx != kOffsetNull) { mn_m = imin(mn_m, k); mx_m = imax(mx_m, k); }
+      if (cell_in_bounds(i1, k, n, m)) { mn_i1 = imin(mn_i1, k); mx_i1 = imax(mx_i1, k); }
+      if (cell_in_bounds(d1, k, n, m)) { mn_d1 = imin(mn_d1, k); mx_d1 = imax(mx_d1, k); }
+    }
+    mn_i1 = Warp::min(mn_i1); mx_i1 = Warp::max(mx_i1);
+    mn_d1 = Warp::min(mn_d1); mx_d1 = Warp::max(mx_d1);
+    put(CI1, s, finish(oi1, lo, lo, hi, mn_i1, mx_i1));
+    put(CD1, s, finish(od1, lo, lo, hi, mn_d1, mx_d1));
+    if (TWO) {
+      if (affine_kernel) {
+        set_none(s, CI2, CD2 + 1);
+      } else {
+        mn_i2 = Warp::min(mn_i2); mx_i2 = Warp::max(mx_i2);
+        mn_d2 = Warp::min(mn_d2); mx_d2 = Warp::max(mx_d2);
+        put(CI2, s, finish(oi2, lo, lo, hi, mn_i2, mx_i2));
+        put(CD2, s, finish(od2, lo, lo, hi, mn_d2, mx_d2));
+      }
+    }
+    if (bf) {
+      int mlo = lo, mhi = hi;
+      endsfree_init(om, L, mlo, mhi, bk);
+      set_m(s, trim_pass(om, L, mlo, mhi));
+    } else {
+      mn_m = Warp::min(mn_m); mx_m = Warp::max(mx_m);
+      set_m(s, finish(om, L, lo, hi, mn_m, mx_m));
+    }
+  }
+
+  WFA_D void compute_step(int s) {
+    if (CLS == kEditClass) compute_edit(s);
+    else if (CLS == kLinearClass) compute_linear(s);
+    else compute_affine(s);
+  }
+
+  // ---- extend ----------------------------------------------------------------
+  // extend_matches_packed_end2end (src/extend.rs:47-70): extend every
+  // diagonal of [lo, hi] with offset >= 0.  Returns the lowest diagonal
+  // meeting the ends-free termination (termination_endsfree,
+  // src/termination.rs:31-58) when `endsfree_term`, else INT_MAX.
+  WFA_D int extend_wf(WfD& d, bool endsfree_term, int& term_off) {
+    int best = INT_MAX, best_off = 0;
+    for (int k = d.lo + lane; k <= d.hi; k += WFA_WARP) {
+      int32_t off = d.vals[k - d.a];
+      if (off >= 0) {
+        int v = off - k, h = off;
+        int R = imin(n - v, m - h);
+        if (R > 0) {
+          off += lcp_fwd(pat, v, txt, h, R);
+          d.vals[k - d.a] = off;
+        }
+        if (endsfree_term && k < best) {
+          int hh = off, vv = off - k;
+          if ((hh >= m && n - vv <= pf) || (vv >= n && m - hh <= tf)) { best = k; best_off = off; }
+        }
+      }
+    }
+    Warp::sync();
+    if (endsfree_term) {
+      int kb = Warp::min(best);
+      if (kb != INT_MAX) term_off = d.vals[kb - d.a];
+      (void)best_off;
+      return kb;
+    }
+    return INT_MAX;
+  }
+
+  // ---- heuristics: src/heuristic.rs:167-520, src/aligner.rs:1644-1766 ---------
+  WFA_D int32_t dist(const WfD& d, int k) const {  // wf_distance_end2end
+    int32_t off = d.vals[k - d.a];
+    if (off < 0) return INT_MAX;
+    return imax(n - (off - k), m - off);
+  }
+  // SW score of cell k (compute_sw_scores); `valid` false for offset < 0.
+  WFA_D int32_t sw_score(const WfD& d, int k, int score, bool& valid) const {
+    int32_t off = d.vals[k - d.a];
+    valid = off >= 0;
+    if (!valid) return 0;
+    int swg = P.match != 0 ? -P.match : 1;
+    bool bfree = P.match == 0 && endsfree;
+    int fv = k < 0 ? imin(-k, bfree ? p0 : 0) : 0;
+    int fh = k > 0 ? imin(k, bfree ? t0 : 0) : 0;
+    int v = off - k - fv, h = off - fh;
+    return (swg * (v + h) - score) / 2;
+  }
+  // Warp max of the SW scores with the lowest diagonal among the maxima.
+  WFA_D void sw_max(const WfD& d, int score, int& cmax, int& ck, int& coff) {
+    int best = INT_MIN, bk = INT_MAX;
+    for (int k = d.lo + lane; k <= d.hi; k += WFA_WARP) {
+      bool ok;
+      int sw = sw_score(d, k, score, ok);
+      if (ok && (sw > best || (sw == best && k < bk))) { best = sw; bk = k; }
+    }
+    cmax = Warp::max(best);
+    int cand = (best == cmax) ? bk : INT_MAX;
+    ck = Warp::min(cand);
+    if (cmax == INT_MIN) { ck = 0; coff = 0; }
+    else coff = d.vals[ck - d.a];
+  }
+
+  // heuristic_cutoff; returns true on a Z-drop.  d is M at `score`.
+  WFA_D bool heuristic_cutoff(WfD& d, int score) {
+    if (d.lo > d.hi) return false;
+    hs.steps_wait -= 1;
+    switch (P.hkind) {
+      case WFA_HEURISTIC_WFADAPTIVE: {
+        if (hs.steps_wait > 0) return false;
+        int blo = d.lo, bhi = d.hi;
+        if (bhi - blo + 1 < P.hp0) return false;
+        int mn = INT_MAX;
+        for (int k = blo + lane; k <= bhi; k += WFA_WARP) mn = imin(mn, dist(d, k));
+        int min_d = imin(Warp::min(mn), imax(n, m));
+        int ak = m - n, thr = P.hp1;
+        auto ok = [&](int k) { return (int32_t)((uint32_t)dist(d, k) - (uint32_t)min_d) <= thr; };
+        int top = imin(ak, d.hi), nlo = d.lo;
+        if (top > d.lo) {
+          int f = INT_MAX;
+          for (int k = d.lo + lane; k < top; k += WFA_WARP) if (ok(k)) { f = k; break; }
+          f = Warp::min(f);
+          nlo = imin(f, top);
+        }
+        int bottom = imax(ak, nlo), nhi = d.hi;
+        if (d.hi > bottom) {
+          int l = INT_MIN;
+          for (int k = d.hi - lane; k > bottom; k -= WFA_WARP) if (ok(k)) { l = k; break; }
+          l = Warp::max(l);
+          nhi = imax(l, bottom);
+        }
+        d.lo = nlo;
+        d.hi = nhi;
+        hs.steps_wait = P.hp2;
+        return false;
+      }
+      case WFA_HEURISTIC_BANDED_STATIC:
+        if (d.lo < P.hp0) d.lo = P.hp0;
+        if (d.hi > P.hp1) d.hi = P.hp1;
+        return false;
+      case WFA_HEURISTIC_BANDED_ADAPTIVE: {
+        if (hs.steps_wait > 0) return false;
+        int lo = d.lo, hi = d.hi, len = hi - lo + 1;
+        if (len < 4) return false;
+        int maxlen = P.hp1 - P.hp0 + 1;
+        if (len > maxlen) {
+          int leeway = (len - maxlen) / 2, q = len / 4;
+          int d0 = dist(d, lo), d1 = dist(d, lo + q), d2 = dist(d, lo + 2 * q), d3 = dist(d, hi);
+          int nl = lo;
+          if (d0 > d3) nl += leeway;
+          if (d1 > d2) nl += leeway;
+          d.lo = imax(nl, lo);
+          d.hi = imin(nl + maxlen - 1, hi);
+        }
+        hs.steps_wait = P.hp2;
+        return false;
+      }
+      case WFA_HEURISTIC_XDROP: {
+        if (hs.steps_wait > 0) return false;
+        int cmax, ck, co;
+        sw_max(d, score, cmax, ck, co);
+        if (hs.max_sw_k != kDiagNull) {
+          int mx = hs.max_sw_score, xd = P.hp0;
+          auto keep = [&](int k) {
+            bool ok;
+            int sw = sw_score(d, k, score, ok);
+            return ok && !(mx - sw >= xd);
+          };
+          int f = INT_MAX;
+          for (int k = d.lo + lane; k <= d.hi; k += WFA_WARP) if (keep(k)) { f = k; break; }
+          int nlo = imin(Warp::min(f), d.hi + 1);
+          int l = INT_MIN;
+          for (int k = d.hi - lane; k >= nlo; k -= WFA_WARP) if (keep(k)) { l = k; break; }
+          int nhi = imax(Warp::max(l), nlo - 1);
+          d.lo = nlo;
+          d.hi = nhi;
+          if (cmax > hs.max_sw_score) { hs.max_sw_score = cmax; hs.max_sw_k = ck; }
+        } else {
+          hs.max_sw_score = cmax;
+          hs.max_sw_k = ck;
+        }
+        hs.steps_wait = P.hp1;
+        return false;
+      }
+      case WFA_HEURISTIC_ZDROP: {
+        if (hs.steps_wait > 0) return false;
+        int cmax, ck, co;
+        sw_max(d, score, cmax, ck, co);
+        if (hs.max_sw_k == kDiagNull || cmax > hs.max_sw_score) {
+          hs.max_sw_score = cmax; hs.max_wf_score = score; hs.max_sw_k = ck;
+          hs.max_sw_off = co; hs.zdrop_last = score;
+        } else if (hs.max_sw_score - cmax <= P.hp0) {
+          hs.zdrop_last = score;
+        } else if (score - hs.zdrop_last >= scope - 1) {
+          return true;
+        }
+        hs.steps_wait = P.hp1;
+        return false;
+      }
+      default:
+        return false;
+    }
+  }
+
+  // apply_heuristic_cutoff, src/aligner.rs:1644-1766.  True on a Z-drop.
+  WFA_D bool apply_heuristic(int score) {
+    WfD d = slot(CM, score);
+    if (P.hkind == WFA_HEURISTIC_BANDED_STATIC && d.lo >= P.hp0 && d.hi <= P.hp1) return false;
+    int lo_base = d.lo, hi_base = d.hi;
+    bool z = heuristic_cutoff(d, score);
+    if (z) {
+      end_score = hs.max_wf_score; end_k = hs.max_sw_k; end_off = hs.max_sw_off;
+      return true;
+    }
+    if (lo_base > hi_base || (d.lo == lo_base && d.hi == hi_base)) return false;
+    if (d.lo > d.hi) { d.flags |= kNullFlag; d.a = d.lo; d.b = d.hi; }
+    put(CM, score, d);
+    hist_put(score, d);
+    if (AFF) {
+      for (int c = 1; c < NC; ++c) {
+        WfD w = slot(c, score);
+        if (!wf_present(w)) continue;
+        if (d.lo > w.lo) w.lo = d.lo;
+        if (d.hi < w.hi) w.hi = d.hi;
+        if (w.lo > w.hi) { w.flags |= kNullFlag; w.a = w.lo; w.b = w.hi; }
+        put(c, score, w);
+      }
+    }
+    return false;
+  }
+
+  // extend_end2end (src/aligner.rs:1004-1050) / extend_endsfree (:1053-1101).
+  WFA_D bool extend_step(int score) {
+    WfD d = slot(CM, score);
+    if (!wf_present(d)) {
+      if (num_null_steps > scope) { status = WFA_STATUS_END_UNREACHABLE; return true; }
+      return false;
+    }
+    int toff = 0;
+    int tk = extend_wf(d, endsfree, toff);
+    if (endsfree) {
+      if (tk != INT_MAX) {
+        end_score = score; end_k = tk; end_off = toff;
+        status = WFA_STATUS_END_REACHED;
+        return true;
+      }
+    } else {
+      int ak = m - n;
+      if (d.lo <= ak && ak <= d.hi && d.vals[ak - d.a] >= m) {
+        end_score = score; end_k = ak; end_off = m;
+        status = WFA_STATUS_END_REACHED;
+        return true;
+      }
+    }
+    if (P.hkind != WFA_HEURISTIC_NONE && apply_heuristic(score)) {
+      status = WFA_STATUS_END_UNREACHABLE;
+      return true;
+    }
+    return false;
+  }
+
+  // ---- CIGAR output ------------------------------------------------------------
+  WFA_D void run(uint8_t op, int cnt) {  // write_ops, src/backtrace.rs:689-698
+    if (cnt <= 0) return;
+    if (cg_begin - cnt + 1 < 0) { status = WFA_STATUS_OOM; cg_begin = -1; return; }
+    for (int i = lane; i < cnt; i += WFA_WARP) cg[cg_begin - i] = op;
+    cg_begin -= cnt;
+  }
+  WFA_D void matches(int cnt) {  // write_matches, src/backtrace.rs:111-128
+    if (cnt < 0) { cg_begin += -(int64_t)cnt; return; }
+    run('M', cnt);
+  }
+  WFA_D void push(uint8_t op) { run(op, 1); }
+  WFA_D uint8_t op_at(int64_t i) const { return cg[i]; }
+
+  // M history lookup (st_m_offset, src/backtrace.rs:645-663; NULL cells ->
+  // false, as outside the initialised range).
+  WFA_D bool m_cell(int score, int k, int32_t& out) const {
+    if (score < 0 || !has_slot(score)) return false;
+    int4 r = ws.hist[score];
+    if (!r.w || k < r.x || k > r.y) return false;
+    out = ws.harena[r.z + (k - r.x)];
+    return true;
+  }
+  WFA_D bool st_m_offset(int score, int k, int32_t& out) const {
+    int32_t o;
+    if (!m_cell(score, k, o) || o == kOffsetNull) return false;
+    out = o;
+    return true;
+  }
+
+  // backtrace_affine_singletrack, src/backtrace.rs:751-858
+  WFA_D bool st_gap(int gscore, int l, int off_orig, int& k, int& offset) {
+    int32_t mo;
+    if (st_m_offset(gscore, k - l, mo) && mo + l >= off_orig && mo + l <= offset) {
+      run('M', offset - (mo + l));
+      run('I', l);
+      k -= l;
+      offset = mo;
+      return true;
+    }
+    if (st_m_offset(gscore, k + l, mo) && mo >= off_orig && mo <= offset) {
+      run('M', offset - mo);
+      run('D', l);
+      k += l;
+      offset = mo;
+      return true;
+    }
+    return false;
+  }
+  WFA_D void backtrace_singletrack(int ascore, int k, int offset) {
+    int score = ascore, off_orig = offset;
+    run('D', n - (offset - k));
+    run('I', m - offset);
+    bool in_m = true;
+    int l = 0;
+    while (score != 0 && status != WFA_STATUS_OOM) {
+      if (in_m) {
+        int v = offset - k, h = offset;
+        int nm = lcp_bwd(pat, v, txt, h, imin(v, h));
+        off_orig = offset - nm;
+        int mis = score - P.mismatch;
+        int32_t mo;
+        if (st_m_offset(mis, k, mo) && mo == off_orig - 1) {
+          run('M', nm);
+          run('X', 1);
+          offset = off_orig - 1;
+          score = mis;
+        } else {
+          in_m = false;
+          l = 0;
+        }
+      } else {
+        ++l;
+        int ind1 = score - P.o1 - l * P.e1;
+        int ind2 = TWO ? score - P.o2 - l * P.e2 : -1;
+        if (st_gap(ind1, l, off_orig, k, offset)) { score = ind1; in_m = true; }
+        else if (st_gap(ind2, l, off_orig, k, offset)) { score = ind2; in_m = true; }
+        else if (ind1 < 0 && ind2 < 0) break;
+      }
+    }
+    int v = offset - k, h = offset;
+    int nm = imin(v, h);
+    v -= nm;
+    h -= nm;
+    run('M', nm);
+    run('D', v);
+    run('I', h);
+  }
+
+  // backtrace_linear, src/backtrace.rs:132-258
+  WFA_D int64_t bt_pack(int score, int k, int dk, int add, int64_t type, bool ins) const {
+    // bt_misms (dk 0), bt_ins1_open (dk -1, cell k-1), bt_del1_open (dk +1)
+    if (score < 0) return kOffsetNull;
+    int4 r = ws.hist[score];
+    if (!r.w) return kOffsetNull;
+    bool inside;
+    if (dk == 0) inside = r.x <= k && k <= r.y;
+    else if (ins) inside = r.x < k && k - 1 <= r.y;
+    else inside = r.x <= k + 1 && k < r.y;
+    if (!inside) return kOffsetNull;
+    int32_t o = ws.harena[r.z + (k + dk - r.x)];
+    return ((int64_t)(o + add) << 4) | type;
+  }
+  WFA_D void backtrace_linear(int ascore, int k, int offset) {
+    int score = ascore, v = offset - k, h = offset;
+    if (v < n) run('D', n - v);
+    if (h < m) run('I', m - h);
+    const bool indel = P.metric == WFA_METRIC_INDEL;
+    while (v > 0 && h > 0 && score > 0 && status != WFA_STATUS_OOM) {
+      int ms = score - P.mismatch, gs = score - P.o1;
+      int64_t misms = indel ? (int64_t)kOffsetNull : bt_pack(ms, k, 0, 1, 9, false);
+      int64_t ins = bt_pack(gs, k, -1, 1, 1, true);
+      int64_t del = bt_pack(gs, k, 1, 0, 5, false);
+      int64_t mx = lmax(misms, lmax(ins, del));
+      if (mx < 0) break;
+      int moff = (int)(mx >> 4);
+      matches(offset - moff);
+      offset = moff;
+      v = offset - k; h = offset;
+      if (v <= 0 || h <= 0) break;
+      int t = (int)(mx & 0xF);
+      if (t == 9) { score = ms; push('X'); offset -= 1; }
+      else if (t == 1) { score = gs; push('I'); k -= 1; offset -= 1; }
+      else { score = gs; push('D'); k += 1; }
+      v = offset - k; h = offset;
+    }
+    if (v > 0 && h > 0) {
+      int nm = imin(v, h);
+      matches(nm);
+      v -= nm; h -= nm;
+    }
+    run('D', v);
+    run('I', h);
+  }
+
+  WFA_D void backtrace_from(int score, int k, int offset) {  // src/aligner.rs:1414-1436
+    cg_end = cg_cap;
+    cg_begin = cg_cap - 1;
+    if (AFF) backtrace_singletrack(score, k, offset);
+    else backtrace_linear(score, k, offset);
+    cg_begin += 1;
+    cg_score = score;
+    Warp::sync();
+  }
+
+  // ---- CIGAR post-processing: src/cigar.rs, src/aligner.rs:1545-1640 ----------
+  WFA_D int32_t score_classic(int64_t b, int64_t e) const {  // score_gap_* with user penalties
+    const int32_t* p = P.orig;
+    int32_t s = 0;
+    if (CLS == kEditClass) {
+      for (int64_t i = b; i < e; ++i) s += op_at(i) != 'M';
+      return s;
+    }
+    if (CLS == kLinearClass) {
+      for (int64_t i = b; i < e; ++i) {
+        uint8_t op = op_at(i);
+        s -= op == 'M' ? p[0] : op == 'X' ? p[1] : p[2];
+      }
+      return s;
+    }
+    if (CLS == kAffineClass) {
+      uint8_t last = 0;
+      for (int64_t i = b; i < e; ++i) {
+        uint8_t op = op_at(i);
+        if (op == 'M') s -= p[0];
+        else if (op == 'X') s -= p[1];
+        else s -= p[3] + (last == op ? 0 : p[2]);
+        last = op;
+      }
+      return s;
+    }
+    int64_t i = b;
+    while (i < e) {
+      uint8_t op = op_at(i);
+      int64_t j = i;
+      while (j < e && op_at(j) == op) ++j;
+      int32_t len = (int32_t)(j - i);
+      if (op == 'M') s -= p[0] * len;
+      else if (op == 'X') s -= p[1] * len;
+      else s -= imin(p[2] + p[3] * len, p[4] + p[5] * len);
+      i = j;
+    }
+    return s;
+  }
+  WFA_D int32_t cigar_wfa_score(int64_t b, int64_t e, int v, int h) const {  // :2700-2719
+    int32_t c = score_classic(b, e);
+    if (CLS == kEditClass) return c;
+    if (P.match < 0) return -P.match * (v + h) - 2 * c;
+    return -c;
+  }
+  WFA_D int cigar_skip_gap(uint8_t op, int maxlen) {  // :1580-1592
+    int len = 0;
+    while (len < maxlen && cg_begin < cg_end && op_at(cg_begin) == op) { ++cg_begin; ++len; }
+    return len;
+  }
+  // maxtrim_gap_linear / _affine / _affine2p (src/cigar.rs:207-444); returns trimmed.
+  WFA_D bool maxtrim_ops() {
+    int64_t b = cg_begin, e = cg_end;
+    if (b >= e) return false;
+    const int32_t* p = P.orig;
+    int32_t max_score = 0, mv = 0, mh = 0, s = 0, v = 0, h = 0;
+    int64_t max_off = b;
+    if (CLS != kAffine2pClass) {
+      int32_t match_score = p[0] != 0 ? p[0] : -1;
+      uint8_t last = 0;
+      for (int64_t i = b; i < e; ++i) {
+        uint8_t op = op_at(i);
+        if (op == 'M') { s -= match_score; ++v; ++h; }
+        else if (op == 'X') { s -= p[1]; ++v; ++h; }
+        else if (op == 'I') { s -= CLS == kLinearClass ? p[2] : p[3] + (last == 'I' ? 0 : p[2]); ++h; }
+        else if (op == 'D') { s -= CLS == kLinearClass ? p[2] : p[3] + (last == 'D' ? 0 : p[2]); ++v; }
+        last = op;
+        if (max_score < s) { max_score = s; max_off = i; mv = v; mh = h; }
+      }
+    } else {
+      uint8_t last = 0;
+      int32_t len = 0;
+      auto opsc = [&](uint8_t op, int32_t L) -> int32_t {
+        if (op == 'M') { v += L; h += L; return (p[0] != 0 ? p[0] : -1) * L; }
+        if (op == 'X') { v += L; h += L; return p[1] * L; }
+        if (op == 'D') { v += L; return imin(p[2] + p[3] * L, p[4] + p[5] * L); }
+        if (op == 'I') { h += L; return imin(p[2] + p[3] * L, p[4] + p[5] * L); }
+        return 0;
+      };
+      for (int64_t i = b; i < e; ++i) {
+        uint8_t op = op_at(i);
+        if (op != last && last != 0) {
+          s -= opsc(last, len);
+          len = 0;
+          if (max_score < s) { max_score = s; max_off = i - 1; mv = v; mh = h; }
+        }
+        last = op;
+        ++len;
+      }
+      s -= opsc(last, len);
+      if (max_score < s) { max_score = s; max_off = e - 1; mv = v; mh = h; }
+    }
+    bool trimmed = max_off != e - 1;
+    if (max_score == 0) {
+      cg_begin = 0; cg_end = 0; cg_score = INT_MIN; cg_ev = -1; cg_eh = -1;
+    } else {
+      cg_end = max_off + 1; cg_score = max_score; cg_ev = mv; cg_eh = mh;
+    }
+    return trimmed;
+  }
+  WFA_D bool maxtrim_cigar() {  // src/aligner.rs:1545-1577
+    if (CLS == kEditClass) return false;
+    int bv = 0, bh = 0;
+    if (endsfree) {
+      bh = cigar_skip_gap('I', t0);
+      if (bh == 0) bv = cigar_skip_gap('D', p0);
+    }
+    if (cg_begin >= cg_end) {
+      cg_begin = 0; cg_end = 0; cg_score = INT_MIN; cg_ev = -1; cg_eh = -1;
+      return true;
+    }
+    bool trimmed = maxtrim_ops();
+    if (cg_score != INT_MIN) {
+      cg_score = cigar_wfa_score(cg_begin, cg_end, cg_ev, cg_eh);
+      cg_begin -= bv + bh;
+      cg_ev += bv;
+      cg_eh += bh;
+    }
+    return trimmed;
+  }
+  WFA_D int32_t rescore_heuristic(int score) {  // src/aligner.rs:1605-1640
+    if (P.hkind == WFA_HEURISTIC_NONE || !AFF) return score;
+    int64_t b = cg_begin, e = cg_end;
+    if (endsfree) {
+      int trailing = (n - cg_ev) + (m - cg_eh);
+      // end.saturating_sub(trailing as usize): negative wraps, view empty.
+      cg_end = (trailing < 0 || e - trailing < 0) ? 0 : e - trailing;
+      uint8_t op = b < cg_cap ? op_at(b) : 0;
+      int fr = op == 'I' ? t0 : op == 'D' ? p0 : 0;
+      cigar_skip_gap(op, fr);
+    }
+    int64_t vb = cg_begin, ve = cg_end > vb ? cg_end : vb;
+    int32_t r = 0;
+    if (ve > vb) {
+      int v = 0, h = 0;
+      for (int64_t i = vb; i < ve; ++i) { v += op_at(i) != 'I'; h += op_at(i) != 'D'; }
+      r = cigar_wfa_score(vb, ve, v, h);
+    }
+    cg_begin = b;
+    cg_end = e;
+    cg_score = r;
+    return r;
+  }
+
+  // ---- one pair: align_end2end_span (src/aligner.rs:638-698) and
+  // align_endsfree (:707-831), C compatibility ----------------------------------
+  WFA_D int32_t align() {
+    retry = false;
+    hused = 0;
+    cg_begin = 0; cg_end = 0; cg_score = INT_MIN; cg_ev = -1; cg_eh = -1;
+    init_alignment();
+    int score = 0;
+    const int hard_limit = 1 << 26;  // no reference alignment runs this long
+    if (!retry) {
+      for (;;) {
+        if (extend_step(score)) break;
+        if (retry) break;
+        ++score;
+        if (!has_slot(score)) { status = WFA_STATUS_MAX_STEPS_REACHED; break; }
+        compute_step(score);
+        if (retry) break;
+        if (score >= P.max_steps || score >= hard_limit) { status = WFA_STATUS_MAX_STEPS_REACHED; break; }
+      }
+    }
+    if (retry) { status = kStatusRetry; return 0; }
+    int32_t result = score;
+    const bool cigar = P.compute_alignment != 0;
+    if (!endsfree) {
+      if (status == WFA_STATUS_END_REACHED) {
+        if (cigar) {
+          backtrace_from(score, end_k, end_off);
+          cg_ev = end_off - end_k;
+          cg_eh = end_off;
+          result = rescore_heuristic(score);
+        }
+        if (status != WFA_STATUS_OOM) status = WFA_STATUS_COMPLETED;
+      } else if (status == WFA_STATUS_END_UNREACHABLE && end_off != kOffsetNull) {
+        if (cigar) {
+          backtrace_from(end_score >= 0 ? end_score : score, end_k, end_off);
+          maxtrim_cigar();
+        }
+        if (status != WFA_STATUS_OOM) status = WFA_STATUS_PARTIAL;
+      }
+    } else if (status == WFA_STATUS_END_REACHED || status == WFA_STATUS_END_UNREACHABLE) {
+      bool unreachable = status == WFA_STATUS_END_UNREACHABLE;
+      if (cigar && (status == WFA_STATUS_END_REACHED || end_off != kOffsetNull)) {
+        if (unreachable) backtrace_from(end_score >= 0 ? end_score : score, end_k, end_off);
+        else backtrace_from(score, end_k, end_off);
+        if (status == WFA_STATUS_OOM) return result;
+        if (P.extension || unreachable) {
+          bool trimmed = maxtrim_cigar();
+          status = (trimmed || unreachable) ? WFA_STATUS_PARTIAL : WFA_STATUS_COMPLETED;
+        } else {
+          cg_ev = end_off - end_k;
+          cg_eh = end_off;
+          result = rescore_heuristic(score);
+          status = WFA_STATUS_COMPLETED;
+        }
+      } else {
+        status = unreachable ? WFA_STATUS_PARTIAL : WFA_STATUS_COMPLETED;
+      }
+    }
+    return result;
+  }
+};
+
+// Set up and align pair `pair` of the launch with workspace `ws`, writing
+// its result.  Returns true if the pair must be retried with more scratch.
+template <int CLS, class S>
+WFA_D bool align_one(const AlignParams& P, const Workspace& ws, int64_t pair, S pat, S txt) {
+  PairAligner<CLS, S> A(P);
+  A.ws = ws;
+  A.lane = Warp::lane();
+  A.pat = pat;
+  A.txt = txt;
+  A.n = P.p_len[pair];
+  A.m = P.t_len[pair];
+  A.scope = P.scope;
+  A.wmax = P.wmax;
+  A.modular = P.compute_alignment == 0;
+  A.cap = A.modular ? INT_MAX : imax(A.dims_num(1000, 1000), A.dims_num(A.n, A.m));
+  A.endsfree = P.span == WFA_SPAN_ENDSFREE;
+  if (P.extension) { A.p0 = 0; A.pf = A.n; A.t0 = 0; A.tf = A.m; }
+  else if (A.endsfree) { A.p0 = P.p0; A.pf = P.pf; A.t0 = P.t0; A.tf = P.tf; }
+  else { A.p0 = A.pf = A.t0 = A.tf = 0; }
+  A.cg = nullptr;
+  A.cg_cap = 0;
+  if (!A.modular && P.cigars) {
+    A.cg = P.cigars + P.cigar_off[pair];
+    A.cg_cap = 2 * ((int64_t)A.n + A.m) + 1;
+  }
+  int32_t score = A.align();
+  if (A.status == kStatusRetry) return true;
+  if (A.lane == 0) {
+    wfa_result_t r;
+    r.score = score;
+    r.status = A.status;
+    bool has = A.cg_end > A.cg_begin && !A.modular;
+    r.cigar_begin = has ? (int32_t)A.cg_begin : 0;
+    r.cigar_length = has ? (int32_t)(A.cg_end - A.cg_begin) : 0;
+    r.cigar_score = A.cg_score;
+    r.end_v = A.cg_ev;
+    r.end_h = A.cg_eh;
+    r.end_score = A.end_score;
+    r.end_k = A.end_k;
+    r.end_offset = A.end_off;
+    P.results[pair] = r;
+  }
+  return false;
+}
+
+}  // namespace wfab

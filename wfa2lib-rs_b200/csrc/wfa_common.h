@@ -1,0 +1,58 @@
+// wfa_common.h -- types shared by the host side and the kernels.
+#pragma once
+#include <stdint.h>
+
+#include "../../include/wfa_b200.h"
+
+namespace wfab {
+
+// OFFSET_NULL (src/offset.rs:15) and DPMATRIX_DIAGONAL_NULL (:46).
+constexpr int32_t kOffsetNull = INT32_MIN / 2;
+constexpr int32_t kDiagNull = INT32_MAX;
+
+// Internal pair status: the pair needs more scratch than this launch gave it
+// and is re-run by the host with a larger configuration.
+constexpr int32_t kStatusRetry = 100;
+
+// Metric classes compiled as separate kernel instantiations.
+enum MetricClass { kEditClass = 0, kLinearClass = 1, kAffineClass = 2, kAffine2pClass = 3 };
+
+// Everything a launch needs; passed by value (kernel parameter space).
+struct AlignParams {
+  // Metric and internal penalties (after the Eizenga transform,
+  // src/penalties.rs:157-296); orig = user penalties for CIGAR scoring.
+  int32_t metric;
+  int32_t match, mismatch, o1, e1, o2, e2;
+  int32_t orig[6];
+  int32_t scope;  // max_score_scope (src/components.rs:435-505)
+  // Span: 0 end-to-end, 1 ends-free.  extension: free ends = whole lengths.
+  int32_t span, extension;
+  int32_t p0, pf, t0, tf;
+  // Heuristic (wfa_heuristic_kind_t and its three parameters).
+  int32_t hkind, hp0, hp1, hp2;
+  int32_t compute_alignment;
+  int32_t max_steps;
+  // Input.
+  int32_t format;  // wfa_seq_format_t
+  const uint8_t* seq;
+  int64_t seq_bytes;
+  const int64_t* p_off;
+  const int32_t* p_len;
+  const int64_t* t_off;
+  const int32_t* t_len;
+  const int64_t* cigar_off;
+  uint8_t* cigars;
+  wfa_result_t* results;
+  const int64_t* pair_list;  // NULL: pairs 0..num_pairs-1
+  int64_t num_pairs;
+  // Scratch (one slice per resident warp).
+  int32_t* scratch;
+  int64_t warp_words;  // ints per warp slice
+  int32_t wmax;        // ring slot width (cells)
+  int32_t hist_scores; // M history capacity (scores)
+  int64_t hist_words;  // M history arena capacity (cells)
+  unsigned long long* work_counter;
+  int32_t* retry_count;
+};
+
+}  // namespace wfab
