@@ -21,17 +21,25 @@ EmuWarp* g_emu_warp = nullptr;
 }  // namespace wfab
 #endif
 
-template <int CLS>
-static bool run_lane(const AlignParams& P, const Workspace& ws, int64_t i) {
+template <int CLS, bool GEN>
+static bool run_lane_g(const AlignParams& P, const Workspace& ws, int64_t i) {
   if (P.format == WFA_SEQ_PACKED2) {
     const uint32_t* w = reinterpret_cast<const uint32_t*>(P.seq);
     SeqPacked sp{w + P.p_off[i], P.p_len[i], (P.p_len[i] + 15) >> 4};
     SeqPacked st{w + P.t_off[i], P.t_len[i], (P.t_len[i] + 15) >> 4};
-    return align_one<CLS, SeqPacked>(P, ws, i, sp, st);
+    return align_one<CLS, SeqPacked, GEN>(P, ws, i, sp, st);
   }
   SeqAscii sp{P.seq + P.p_off[i], P.p_len[i]};
   SeqAscii st{P.seq + P.t_off[i], P.t_len[i]};
-  return align_one<CLS, SeqAscii>(P, ws, i, sp, st);
+  return align_one<CLS, SeqAscii, GEN>(P, ws, i, sp, st);
+}
+
+// Same dispatch as the kernel launcher: the lean instantiation for
+// end-to-end alignments without a heuristic, the general one otherwise.
+template <int CLS>
+static bool run_lane(const AlignParams& P, const Workspace& ws, int64_t i) {
+  if (P.span == WFA_SPAN_END2END && P.hkind == WFA_HEURISTIC_NONE) return run_lane_g<CLS, false>(P, ws, i);
+  return run_lane_g<CLS, true>(P, ws, i);
 }
 
 template <int CLS>

@@ -232,7 +232,10 @@ struct Workspace {
   int32_t* harena;  // M history cells
 };
 
-template <int CLS, class S>
+// GEN = false compiles the common configuration only (end-to-end, no
+// heuristic): the ends-free and heuristic code paths drop out, which keeps
+// the kernel body small.
+template <int CLS, class S, bool GEN = true>
 struct PairAligner {
   static constexpr int NC = CLS == kAffine2pClass ? 5 : CLS == kAffineClass ? 3 : 1;
   static constexpr bool AFF = CLS >= kAffineClass;
@@ -261,41 +264,52 @@ struct PairAligner {
   int32_t cg_score, cg_ev, cg_eh;
 
   WFA_D PairAligner(const AlignParams& p) : P(p) {}
+  WFA_D int hk() const { return GEN ? P.hkind : (int)WFA_HEURISTIC_NONE; }
+  WFA_D bool ef() const { return GEN && endsfree; }
 
   // ---- slots --------------------------------------------------------------
   WFA_D WfD& slot(int c, int s) { return ws.ring[(s % scope) * NC + c]; }
+  // Slot (c, s) holds a live wavefront: present and not null (flags are
+  // 0 none, kPresent, or kPresent|kNullFlag).
+  WFA_D bool live(int c, int s) { return s >= 0 && slot(c, s).flags == kPresent; }
   WFA_D WfD get(int c, int s) {  // input fetch (score may be negative)
     if (s < 0) return wf_none();
     return slot(c, s);
   }
-  WFA_D void put(int c, int s, const WfD& d) {
-    Warp::sync();
+  // Descriptor stores are made by lane 0; callers reach a warp-collective
+  // operation (or an explicit sync) between reading a slot and storing into
+  // it, and sync() makes the stores visible before the next step reads them.
+  WFA_D void put_ns(int c, int s, const WfD& d) {
     if (lane == 0) slot(c, s) = d;
-    Warp::sync();
   }
-  WFA_D void hist_put(int s, const WfD& d) {  // M history record (high memory)
-    if (modular) return;
-    if (s >= P.hist_scores) { retry = true; return; }
-    if (lane == 0) {
-      int4 r;
-      r.x = d.a; r.y = d.b;
-      r.z = wf_present(d) ? (int32_t)(d.vals - ws.harena) : 0;
-      r.w = wf_present(d) ? 1 : 0;
-      ws.hist[s] = r;
-    }
+  WFA_D void put(int c, int s, const WfD& d) {
+    put_ns(c, s, d);
     Warp::sync();
   }
   // Storage for an output of component c at score s covering [L, H].
   WFA_D int32_t* alloc(int c, int s, int L, int H) {
     int64_t w = (int64_t)H - L + 1;
-    if (c == CM && !modular) {
-      if (hused + w > P.hist_words) { retry = true; return nullptr; }
-      int32_t* v = ws.harena + hused;
-      hused += w;
-      return v;
-    }
     if (w > wmax) { retry = true; return nullptr; }
     return ws.ringv + ((int64_t)((s % scope) * NC + c)) * wmax;
+  }
+  // High memory: once M at score s is final (after its extend step), copy its
+  // initialised range to the history arena for the backtrace.
+  WFA_D void hist_commit(int s) {
+    if (modular) return;
+    if (s >= P.hist_scores) { retry = true; return; }
+    WfD d = slot(CM, s);
+    int4 r;
+    r.x = d.a; r.y = d.b; r.z = 0; r.w = 0;
+    if (wf_present(d)) {
+      int64_t w = d.b >= d.a ? (int64_t)d.b - d.a + 1 : 0;
+      if (hused + w > P.hist_words) { retry = true; return; }
+      for (int64_t i = lane; i < w; i += WFA_WARP) ws.harena[hused + i] = d.vals[i];
+      r.z = (int32_t)hused;
+      r.w = 1;
+      hused += w;
+    }
+    if (lane == 0) ws.hist[s] = r;
+    Warp::sync();
   }
 
   // ---- helpers --------------------------------------------------------------
@@ -318,7 +332,7 @@ struct PairAligner {
 
   // endsfree_begin_k, src/aligner.rs:3408-3421
   WFA_D bool begin_k(int s, int& k) const {
-    if (P.match == 0 || !endsfree) return false;
+    if (P.match == 0 || !ef()) return false;
     if (t0 == 0 && p0 == 0) return false;
     if (s % (-P.match) != 0) return false;
     k = s / (-P.match);
@@ -326,7 +340,7 @@ struct PairAligner {
   }
 
   WFA_D void clamp_band(int& lo, int& hi) const {  // src/aligner.rs:3308-3317
-    if (P.hkind == WFA_HEURISTIC_BANDED_STATIC || P.hkind == WFA_HEURISTIC_BANDED_ADAPTIVE) {
+    if (hk() == WFA_HEURISTIC_BANDED_STATIC || hk() == WFA_HEURISTIC_BANDED_ADAPTIVE) {
       lo = imax(lo, P.hp0);
       hi = imin(hi, P.hp1);
     }
@@ -410,11 +424,12 @@ struct PairAligner {
   }
 
   WFA_D void set_none(int s, int from_c, int to_c) {
-    for (int c = from_c; c < to_c; ++c) put(c, s, wf_none());
+    for (int c = from_c; c < to_c; ++c) put_ns(c, s, wf_none());
+    Warp::sync();
   }
   WFA_D void set_m(int s, const WfD& d) {
-    put(CM, s, d);
-    hist_put(s, d);
+    put_ns(CM, s, d);
+    Warp::sync();
   }
 
   // ---- init_alignment, src/aligner.rs:846-1000 ------------------------------
@@ -426,12 +441,12 @@ struct PairAligner {
     num_null_steps = 0;
     status = WFA_STATUS_OK;
     end_score = -1; end_k = kDiagNull; end_off = kOffsetNull;
-    hs.steps_wait = (P.hkind == WFA_HEURISTIC_WFADAPTIVE || P.hkind == WFA_HEURISTIC_BANDED_ADAPTIVE) ? P.hp2
-                    : (P.hkind == WFA_HEURISTIC_XDROP || P.hkind == WFA_HEURISTIC_ZDROP) ? P.hp1 : 0;
+    hs.steps_wait = (hk() == WFA_HEURISTIC_WFADAPTIVE || hk() == WFA_HEURISTIC_BANDED_ADAPTIVE) ? P.hp2
+                    : (hk() == WFA_HEURISTIC_XDROP || hk() == WFA_HEURISTIC_ZDROP) ? P.hp1 : 0;
     hs.max_sw_score = 0; hs.max_wf_score = 0; hs.max_sw_k = kDiagNull;
     hs.max_sw_off = kOffsetNull; hs.zdrop_last = 0;
     int lo0 = 0, hi0 = 0;
-    bool seeds = endsfree && P.match == 0;
+    bool seeds = ef() && P.match == 0;
     if (seeds) { lo0 = -p0; hi0 = t0; }
     int32_t* v = alloc(CM, 0, lo0, hi0);
     if (retry) return;
@@ -457,8 +472,11 @@ struct PairAligner {
     // initialised range only; outside it they already read as NULL).
     if (lane == 0) {
       int ks[4] = {prev.lo - 2, prev.lo - 1, prev.hi + 1, prev.hi + 2};
-      for (int i = 0; i < 4; ++i)
+      int4 hr = modular ? int4{0, -1, 0, 0} : ws.hist[s - 1];
+      for (int i = 0; i < 4; ++i) {
         if (ks[i] >= prev.a && ks[i] <= prev.b) prev.vals[ks[i] - prev.a] = kOffsetNull;
+        if (hr.w && ks[i] >= hr.x && ks[i] <= hr.y) ws.harena[hr.z + ks[i] - hr.x] = kOffsetNull;
+      }
     }
     Warp::sync();
     int32_t* out = alloc(CM, s, lo, hi);
@@ -525,21 +543,22 @@ struct PairAligner {
   WFA_D void compute_affine(int s) {
     const int x = P.mismatch, oe1 = P.o1 + P.e1, e1 = P.e1;
     const int oe2 = TWO ? P.o2 + P.e2 : 0, e2 = TWO ? P.e2 : 0;
-    WfD mm = get(CM, s - x), mo1 = get(CM, s - oe1);
-    WfD i1e = get(CI1, s - e1), d1e = get(CD1, s - e1);
-    WfD mo2 = wf_none(), i2e = wf_none(), d2e = wf_none();
-    if (TWO) { mo2 = get(CM, s - oe2); i2e = get(CI2, s - e2); d2e = get(CD2, s - e2); }
     int bk;
-    bool all_null = wf_is_null(mm) && wf_is_null(mo1) && wf_is_null(i1e) && wf_is_null(d1e);
-    if (TWO) all_null = all_null && wf_is_null(mo2) && wf_is_null(i2e) && wf_is_null(d2e);
-    if (all_null) {
+    // Null step (every input missing or empty), decided on the flags alone.
+    bool any_live = live(CM, s - x) || live(CM, s - oe1) || live(CI1, s - e1) || live(CD1, s - e1);
+    if (TWO) any_live = any_live || live(CM, s - oe2) || live(CI2, s - e2) || live(CD2, s - e2);
+    if (!any_live) {
       ++num_null_steps;
-      set_none(s, 1, NC);
+      for (int c = 1; c < NC; ++c) put_ns(c, s, wf_none());
       WfD d = wf_none();
       if (begin_k(s, bk)) d = endsfree_null_m(s, bk);
       set_m(s, d);
       return;
     }
+    WfD mm = get(CM, s - x), mo1 = get(CM, s - oe1);
+    WfD i1e = get(CI1, s - e1), d1e = get(CD1, s - e1);
+    WfD mo2 = wf_none(), i2e = wf_none(), d2e = wf_none();
+    if (TWO) { mo2 = get(CM, s - oe2); i2e = get(CI2, s - e2); d2e = get(CD2, s - e2); }
     num_null_steps = 0;
     if (wf_is_null(mm)) mm = wf_none();
     if (wf_is_null(mo1)) mo1 = wf_none();
@@ -564,7 +583,11 @@ struct PairAligner {
     }
     clamp_band(lo, hi);
     if (lo <= hi) { lo = imax(lo, hist_lo + 1); hi = imin(hi, hist_hi - 1); }
-    if (lo > hi) { set_none(s, 0, NC); if (!modular) hist_put(s, wf_none()); return; }
+    if (lo > hi) {
+      for (int c = 1; c < NC; ++c) put_ns(c, s, wf_none());
+      set_m(s, wf_none());
+      return;
+    }
     bool bf = begin_k(s, bk);
     int L = bf ? imin(lo, -bk) : lo, H = bf ? imax(hi, bk) : hi;
     int32_t* om = alloc(CM, s, L, H);
@@ -601,16 +624,17 @@ struct PairAligner {
     }
     mn_i1 = Warp::min(mn_i1); mx_i1 = Warp::max(mx_i1);
     mn_d1 = Warp::min(mn_d1); mx_d1 = Warp::max(mx_d1);
-    put(CI1, s, finish(oi1, lo, lo, hi, mn_i1, mx_i1));
-    put(CD1, s, finish(od1, lo, lo, hi, mn_d1, mx_d1));
+    put_ns(CI1, s, finish(oi1, lo, lo, hi, mn_i1, mx_i1));
+    put_ns(CD1, s, finish(od1, lo, lo, hi, mn_d1, mx_d1));
     if (TWO) {
       if (affine_kernel) {
-        set_none(s, CI2, CD2 + 1);
+        put_ns(CI2, s, wf_none());
+        put_ns(CD2, s, wf_none());
       } else {
         mn_i2 = Warp::min(mn_i2); mx_i2 = Warp::max(mx_i2);
         mn_d2 = Warp::min(mn_d2); mx_d2 = Warp::max(mx_d2);
-        put(CI2, s, finish(oi2, lo, lo, hi, mn_i2, mx_i2));
-        put(CD2, s, finish(od2, lo, lo, hi, mn_d2, mx_d2));
+        put_ns(CI2, s, finish(oi2, lo, lo, hi, mn_i2, mx_i2));
+        put_ns(CD2, s, finish(od2, lo, lo, hi, mn_d2, mx_d2));
       }
     }
     if (bf) {
@@ -673,7 +697,7 @@ struct PairAligner {
     valid = off >= 0;
     if (!valid) return 0;
     int swg = P.match != 0 ? -P.match : 1;
-    bool bfree = P.match == 0 && endsfree;
+    bool bfree = P.match == 0 && ef();
     int fv = k < 0 ? imin(-k, bfree ? p0 : 0) : 0;
     int fh = k > 0 ? imin(k, bfree ? t0 : 0) : 0;
     int v = off - k - fv, h = off - fh;
@@ -698,7 +722,7 @@ struct PairAligner {
   WFA_D bool heuristic_cutoff(WfD& d, int score) {
     if (d.lo > d.hi) return false;
     hs.steps_wait -= 1;
-    switch (P.hkind) {
+    switch (hk()) {
       case WFA_HEURISTIC_WFADAPTIVE: {
         if (hs.steps_wait > 0) return false;
         int blo = d.lo, bhi = d.hi;
@@ -798,7 +822,7 @@ struct PairAligner {
   // apply_heuristic_cutoff, src/aligner.rs:1644-1766.  True on a Z-drop.
   WFA_D bool apply_heuristic(int score) {
     WfD d = slot(CM, score);
-    if (P.hkind == WFA_HEURISTIC_BANDED_STATIC && d.lo >= P.hp0 && d.hi <= P.hp1) return false;
+    if (hk() == WFA_HEURISTIC_BANDED_STATIC && d.lo >= P.hp0 && d.hi <= P.hp1) return false;
     int lo_base = d.lo, hi_base = d.hi;
     bool z = heuristic_cutoff(d, score);
     if (z) {
@@ -807,18 +831,21 @@ struct PairAligner {
     }
     if (lo_base > hi_base || (d.lo == lo_base && d.hi == hi_base)) return false;
     if (d.lo > d.hi) { d.flags |= kNullFlag; d.a = d.lo; d.b = d.hi; }
-    put(CM, score, d);
-    hist_put(score, d);
+    WfD eq[NC];
+    for (int c = 1; c < NC; ++c) eq[c] = slot(c, score);
+    Warp::sync();
+    put_ns(CM, score, d);
     if (AFF) {
       for (int c = 1; c < NC; ++c) {
-        WfD w = slot(c, score);
+        WfD w = eq[c];
         if (!wf_present(w)) continue;
         if (d.lo > w.lo) w.lo = d.lo;
         if (d.hi < w.hi) w.hi = d.hi;
         if (w.lo > w.hi) { w.flags |= kNullFlag; w.a = w.lo; w.b = w.hi; }
-        put(c, score, w);
+        put_ns(c, score, w);
       }
     }
+    Warp::sync();
     return false;
   }
 
@@ -830,8 +857,8 @@ struct PairAligner {
       return false;
     }
     int toff = 0;
-    int tk = extend_wf(d, endsfree, toff);
-    if (endsfree) {
+    int tk = extend_wf(d, ef(), toff);
+    if (ef()) {
       if (tk != INT_MAX) {
         end_score = score; end_k = tk; end_off = toff;
         status = WFA_STATUS_END_REACHED;
@@ -845,7 +872,7 @@ struct PairAligner {
         return true;
       }
     }
-    if (P.hkind != WFA_HEURISTIC_NONE && apply_heuristic(score)) {
+    if (hk() != WFA_HEURISTIC_NONE && apply_heuristic(score)) {
       status = WFA_STATUS_END_UNREACHABLE;
       return true;
     }
@@ -1100,7 +1127,7 @@ struct PairAligner {
   WFA_D bool maxtrim_cigar() {  // src/aligner.rs:1545-1577
     if (CLS == kEditClass) return false;
     int bv = 0, bh = 0;
-    if (endsfree) {
+    if (ef()) {
       bh = cigar_skip_gap('I', t0);
       if (bh == 0) bv = cigar_skip_gap('D', p0);
     }
@@ -1118,9 +1145,9 @@ struct PairAligner {
     return trimmed;
   }
   WFA_D int32_t rescore_heuristic(int score) {  // src/aligner.rs:1605-1640
-    if (P.hkind == WFA_HEURISTIC_NONE || !AFF) return score;
+    if (hk() == WFA_HEURISTIC_NONE || !AFF) return score;
     int64_t b = cg_begin, e = cg_end;
-    if (endsfree) {
+    if (ef()) {
       int trailing = (n - cg_ev) + (m - cg_eh);
       // end.saturating_sub(trailing as usize): negative wraps, view empty.
       cg_end = (trailing < 0 || e - trailing < 0) ? 0 : e - trailing;
@@ -1152,8 +1179,9 @@ struct PairAligner {
     const int hard_limit = 1 << 26;  // no reference alignment runs this long
     if (!retry) {
       for (;;) {
-        if (extend_step(score)) break;
-        if (retry) break;
+        bool done = extend_step(score);
+        hist_commit(score);
+        if (done || retry) break;
         ++score;
         if (!has_slot(score)) { status = WFA_STATUS_MAX_STEPS_REACHED; break; }
         compute_step(score);
@@ -1164,7 +1192,7 @@ struct PairAligner {
     if (retry) { status = kStatusRetry; return 0; }
     int32_t result = score;
     const bool cigar = P.compute_alignment != 0;
-    if (!endsfree) {
+    if (!ef()) {
       if (status == WFA_STATUS_END_REACHED) {
         if (cigar) {
           backtrace_from(score, end_k, end_off);
@@ -1205,9 +1233,9 @@ struct PairAligner {
 
 // Set up and align pair `pair` of the launch with workspace `ws`, writing
 // its result.  Returns true if the pair must be retried with more scratch.
-template <int CLS, class S>
+template <int CLS, class S, bool GEN = true>
 WFA_D bool align_one(const AlignParams& P, const Workspace& ws, int64_t pair, S pat, S txt) {
-  PairAligner<CLS, S> A(P);
+  PairAligner<CLS, S, GEN> A(P);
   A.ws = ws;
   A.lane = Warp::lane();
   A.pat = pat;

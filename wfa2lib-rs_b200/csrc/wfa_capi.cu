@@ -73,10 +73,17 @@ struct wfa_aligner {
   int last_err = WFA_OK;
   std::string err_str;
   // device resources
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;    // compute (every kernel of the handle)
+  cudaStream_t s_in = nullptr;      // host->device copies
+  cudaStream_t s_out = nullptr;     // device->host copies
   int num_sms = 148;
   DevBuf seq, poff, plen, toff, tlen, coff, results, cigars, dense, scratch, counters, pairlist;
   int64_t launches = 0;
+  uint8_t* pinned = nullptr;  // host staging for the plain per-call form
+  size_t pinned_cap = 0;
+  int occ_key = -1;
+  size_t occ_smem = 0;
+  int occ_val = 1;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_kernel_ms = 0.0;
 };
@@ -122,7 +129,7 @@ __global__ void compact_cigars(const wfa_result_t* res, const int64_t* slot_off,
                                int64_t n) {
   int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
-  if (w >= n) return;
+  if (w >= n || res[w].status == kStatusRetry) return;  // retried pairs are copied later
   int32_t len = res[w].cigar_length;
   const uint8_t* src = slots + slot_off[w] + res[w].cigar_begin;
   uint8_t* dst = dense + dst_off[w];
@@ -168,6 +175,87 @@ static void fill_params(const wfa_aligner_t* h, const wfa_batch_t* b, AlignParam
   P.pair_list = nullptr;
 }
 
+// Initial scratch configuration for a batch whose longest pair has
+// n + m = max_len_sum.  First pass: ring cells in shared memory when a slot
+// of kRingSmemWidth cells per (score, component) fits the budget, and
+// sequences of up to kSeqSmemWords words staged in shared memory.  Pairs that
+// outgrow a configuration are re-run with a larger one (next_cfg).
+static constexpr int kRingSmemWidth = 64, kSeqSmemWords = 64;
+static constexpr size_t kRingSmemBudget = 8 * 1024;  // bytes per warp
+static constexpr size_t kScratchBudget = (size_t)6 << 30;
+
+struct Round {
+  ScratchCfg cfg;
+  bool ring_smem;
+};
+
+static Round first_round(const AlignParams& P, int nc, int32_t max_len_sum) {
+  Round r;
+  r.cfg.wmax = std::max(8, std::min(max_len_sum + 3, 8192));
+  r.cfg.hist_scores = P.compute_alignment ? 1024 : 0;
+  r.cfg.hist_words = P.compute_alignment ? (int64_t)std::max(32768, 16 * (max_len_sum + 3)) : 0;
+  r.ring_smem = (size_t)P.scope * nc * kRingSmemWidth * 4 <= kRingSmemBudget;
+  if (r.ring_smem) r.cfg.wmax = std::min(r.cfg.wmax, kRingSmemWidth);
+  return r;
+}
+
+static void next_round(Round& r, const AlignParams& P, int32_t max_len_sum) {
+  if (r.ring_smem) {
+    r.ring_smem = false;  // retries use the scratch ring at full width
+    r.cfg.wmax = std::max(8, std::min(max_len_sum + 3, 8192));
+  } else {
+    r.cfg.wmax = std::min(max_len_sum + 3, std::max(r.cfg.wmax, 1) * 4);
+  }
+  if (P.compute_alignment) {
+    r.cfg.hist_scores *= 4;
+    r.cfg.hist_words *= 4;
+  }
+}
+
+// Sizes the scratch for round r and launches the alignment kernel over
+// `todo` pairs (`list`: their indices, or NULL for 0..todo-1).  No sync.
+static int launch_round(wfa_aligner_t* h, AlignParams& P, const Round& r, int64_t todo,
+                        const int64_t* list, cudaStream_t st) {
+  const int cls = metric_class(P.metric);
+  const int nc = metric_components(P.metric);
+  P.seq_smem_words = kSeqSmemWords;
+  P.ring_smem = r.ring_smem ? 1 : 0;
+  P.wmax = r.cfg.wmax;
+  const SmemLayout L = smem_layout(P.scope, nc, r.ring_smem ? r.cfg.wmax : 0, P.seq_smem_words);
+  const size_t smem = L.total;
+  if (smem > 200 * 1024) return fail(h, WFA_ERR_UNSUPPORTED, "wavefront ring too large");
+  const int key = cls * 4 + (P.format == WFA_SEQ_PACKED2) * 2 + (needs_general(P) ? 1 : 0);
+  if (key != h->occ_key || smem != h->occ_smem) {
+    h->occ_val = occupancy_blocks_per_sm(P, cls, smem);
+    h->occ_key = key;
+    h->occ_smem = smem;
+  }
+  int64_t ring_words = r.ring_smem ? 0 : (((int64_t)P.scope * nc * r.cfg.wmax + 3) & ~(int64_t)3);
+  int64_t warp_words = ring_words + (int64_t)r.cfg.hist_scores * 4 + r.cfg.hist_words;
+  warp_words = std::max<int64_t>((warp_words + 63) & ~(int64_t)63, 64);
+  int64_t max_warps = (int64_t)h->num_sms * h->occ_val * kWarpsPerBlock;
+  int64_t warps = std::max<int64_t>(std::min<int64_t>(max_warps, todo), 1);
+  while (warps > kWarpsPerBlock && (size_t)warps * warp_words * 4 > kScratchBudget) warps /= 2;
+  int blocks = (int)((warps + kWarpsPerBlock - 1) / kWarpsPerBlock);
+  size_t scratch_bytes = (size_t)blocks * kWarpsPerBlock * warp_words * 4;
+  CUDA_TRY(h, h->scratch.ensure(scratch_bytes), "scratch");
+  CUDA_TRY(h, h->counters.ensure(64), "counters");
+  P.scratch = h->scratch.as<int32_t>();
+  P.warp_words = warp_words;
+  P.hist_scores = r.cfg.hist_scores;
+  P.hist_words = r.cfg.hist_words;
+  P.work_counter = h->counters.as<unsigned long long>();
+  P.retry_count = reinterpret_cast<int32_t*>(P.work_counter + 1);
+  P.pair_list = list;
+  P.num_pairs = todo;
+  CUDA_TRY(h, cudaMemsetAsync(P.work_counter, 0, 16, st), "memset");
+  CUDA_TRY(h, cudaEventRecord(h->ev0, st), "event");
+  CUDA_TRY(h, launch_unialign(P, cls, blocks, smem, st), "kernel launch");
+  CUDA_TRY(h, cudaEventRecord(h->ev1, st), "event");
+  h->launches++;
+  return WFA_OK;
+}
+
 // Runs every pair of a device-resident batch, escalating scratch for pairs
 // that need more.  Synchronises `st` to read the retry count.
 static int run_device_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* d_results,
@@ -178,80 +266,39 @@ static int run_device_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t
   P.cigars = d_cigars;
   if (P.compute_alignment && (!d_cigars || !b->cigar_off))
     return fail(h, WFA_ERR_ARGUMENT, "CIGAR output buffers are required in alignment scope");
-  const int cls = metric_class(P.metric);
   const int nc = metric_components(P.metric);
-  const bool packed = P.format == WFA_SEQ_PACKED2;
-  const size_t smem = (size_t)kWarpsPerBlock * ring_desc_bytes(P.scope, nc);
-  if (smem > 200 * 1024) return fail(h, WFA_ERR_UNSUPPORTED, "wavefront ring too large");
-  const int occ = occupancy_blocks_per_sm(cls, packed, smem);
-
-  ScratchCfg cfg;
-  cfg.wmax = std::max(8, std::min(max_len_sum + 3, 8192));
-  cfg.hist_scores = P.compute_alignment ? 1024 : 0;
-  cfg.hist_words = P.compute_alignment ? (int64_t)std::max(32768, 16 * (max_len_sum + 3)) : 0;
-
-  CUDA_TRY(h, h->counters.ensure(64), "counters");
-  unsigned long long* d_work = h->counters.as<unsigned long long>();
-  int32_t* d_retry = reinterpret_cast<int32_t*>(d_work + 1);
-
+  Round r = first_round(P, nc, max_len_sum);
   int64_t todo = b->num_pairs;
   const int64_t* list = nullptr;
   h->last_kernel_ms = 0.0;
-  const size_t budget = (size_t)6 << 30;  // scratch bytes per handle
   for (int round = 0; todo > 0; ++round) {
     if (round > 8) return fail(h, WFA_ERR_OOM, "alignment needs more scratch than available");
-    int64_t ring_words = ((int64_t)P.scope * nc * cfg.wmax + 3) & ~(int64_t)3;
-    int64_t warp_words = ring_words + (int64_t)cfg.hist_scores * 4 + cfg.hist_words;
-    warp_words = (warp_words + 63) & ~(int64_t)63;
-    int64_t max_warps = (int64_t)h->num_sms * occ * kWarpsPerBlock;
-    int64_t warps = std::min<int64_t>(max_warps, (todo + 0) * 1);
-    warps = std::max<int64_t>(warps, 1);
-    while (warps > kWarpsPerBlock && (size_t)warps * warp_words * 4 > budget) warps /= 2;
-    int blocks = (int)((warps + kWarpsPerBlock - 1) / kWarpsPerBlock);
-    size_t scratch_bytes = (size_t)blocks * kWarpsPerBlock * warp_words * 4;
-    CUDA_TRY(h, h->scratch.ensure(scratch_bytes), "scratch");
-    P.scratch = h->scratch.as<int32_t>();
-    P.warp_words = warp_words;
-    P.wmax = cfg.wmax;
-    P.hist_scores = cfg.hist_scores;
-    P.hist_words = cfg.hist_words;
-    P.work_counter = d_work;
-    P.retry_count = d_retry;
-    P.pair_list = list;
-    P.num_pairs = todo;
-    CUDA_TRY(h, cudaMemsetAsync(d_work, 0, 16, st), "memset");
-    CUDA_TRY(h, cudaEventRecord(h->ev0, st), "event");
-    CUDA_TRY(h, launch_unialign(P, cls, blocks, smem, st), "kernel launch");
-    CUDA_TRY(h, cudaEventRecord(h->ev1, st), "event");
-    h->launches++;
+    int e = launch_round(h, P, r, todo, list, st);
+    if (e != WFA_OK) return e;
     int32_t retries = 0;
-    CUDA_TRY(h, cudaMemcpyAsync(&retries, d_retry, 4, cudaMemcpyDeviceToHost, st), "retry count");
+    CUDA_TRY(h, cudaMemcpyAsync(&retries, P.retry_count, 4, cudaMemcpyDeviceToHost, st), "retry count");
     CUDA_TRY(h, cudaStreamSynchronize(st), "kernel");
     float ms = 0.f;
     CUDA_TRY(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1), "event");
     h->last_kernel_ms += ms;
     if (retries == 0) break;
     // Gather the pairs to re-run into a list (double-buffered in pairlist).
-    size_t lbytes = (size_t)retries * 8;
-    CUDA_TRY(h, h->pairlist.ensure(2 * std::max(lbytes, (size_t)b->num_pairs * 8)), "pair list");
+    CUDA_TRY(h, h->pairlist.ensure(2 * (size_t)std::max<int64_t>(b->num_pairs, 1) * 8), "pair list");
     int64_t* half0 = h->pairlist.as<int64_t>();
     int64_t* half1 = half0 + b->num_pairs;
     int64_t* out = (list == half0) ? half1 : half0;
-    CUDA_TRY(h, cudaMemsetAsync(d_retry, 0, 4, st), "memset");
+    CUDA_TRY(h, cudaMemsetAsync(P.retry_count, 0, 4, st), "memset");
     int tb = 256;
-    collect_retries<<<(unsigned)((todo + tb - 1) / tb), tb, 0, st>>>(d_results, list, todo, out, d_retry);
+    collect_retries<<<(unsigned)((todo + tb - 1) / tb), tb, 0, st>>>(d_results, list, todo, out,
+                                                                     P.retry_count);
     h->launches++;
     CUDA_TRY(h, cudaGetLastError(), "collect retries");
     int32_t got = 0;
-    CUDA_TRY(h, cudaMemcpyAsync(&got, d_retry, 4, cudaMemcpyDeviceToHost, st), "retry count");
+    CUDA_TRY(h, cudaMemcpyAsync(&got, P.retry_count, 4, cudaMemcpyDeviceToHost, st), "retry count");
     CUDA_TRY(h, cudaStreamSynchronize(st), "collect retries");
     list = out;
     todo = got;
-    cfg.wmax = std::min(max_len_sum + 3, std::max(cfg.wmax, 1) * 4);
-    if (P.compute_alignment) {
-      cfg.hist_scores *= 4;
-      cfg.hist_words *= 4;
-    }
+    next_round(r, P, max_len_sum);
   }
   return WFA_OK;
 }
@@ -288,6 +335,8 @@ wfa_aligner_t* wfa_aligner_create(wfa_metric_t metric, const wfa_penalties_t* pe
   h->pen = P;
   cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device);
   if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&h->s_in, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&h->s_out, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess) {
     delete h;
     if (err) *err = WFA_ERR_CUDA;
@@ -304,9 +353,12 @@ void wfa_aligner_destroy(wfa_aligner_t* h) {
   for (DevBuf* b : {&h->seq, &h->poff, &h->plen, &h->toff, &h->tlen, &h->coff, &h->results,
                     &h->cigars, &h->dense, &h->scratch, &h->counters, &h->pairlist})
     b->release();
+  if (h->pinned) cudaFreeHost(h->pinned);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->stream) cudaStreamDestroy(h->stream);
+  if (h->s_in) cudaStreamDestroy(h->s_in);
+  if (h->s_out) cudaStreamDestroy(h->s_out);
   delete h;
 }
 
@@ -363,7 +415,11 @@ int wfa_set_heuristic(wfa_aligner_t* h, wfa_heuristic_kind_t kind, int32_t p0, i
   return WFA_OK;
 }
 
-// One pair through the batch path (plain per-call form).
+// One pair through the batch kernel (plain per-call form): one host->device
+// copy (sequences and metadata in one pinned staging buffer), one launch, the
+// result record and CIGAR slot copied back, one synchronisation.  A pair that
+// needs more scratch than the first configuration is re-run by the batch
+// driver.
 static int32_t align_plain(wfa_aligner_t* h, const uint8_t* p, int32_t n, const uint8_t* t,
                            int32_t m, int span, bool packed) {
   if (!h || n < 0 || m < 0 || (n > 0 && !p) || (m > 0 && !t)) return WFA_ERR_ARGUMENT;
@@ -377,49 +433,89 @@ static int32_t align_plain(wfa_aligner_t* h, const uint8_t* p, int32_t n, const 
   if (r != WFA_OK) return r;
   cudaSetDevice(h->device);
   cudaStream_t st = h->stream;
-  // Layout: pattern then text, each starting on a 16-byte boundary.
-  size_t pbytes = packed ? ((size_t)n + 3) / 4 : (size_t)n;
-  size_t tbytes = packed ? ((size_t)m + 3) / 4 : (size_t)m;
-  size_t toff_b = (pbytes + 15) & ~(size_t)15;
-  size_t total = toff_b + ((tbytes + 15) & ~(size_t)15) + 16;
-  int64_t cap = 2 * ((int64_t)n + m) + 1;
-  struct Meta { int64_t poff, toff, coff; int32_t plen, tlen; } meta;
+  // Staging layout: [meta 64 B][pattern, 16-aligned][text, 16-aligned][pad].
+  struct Meta { int64_t poff, toff, coff; int32_t plen, tlen; };
+  const size_t pbytes = packed ? ((size_t)n + 3) / 4 : (size_t)n;
+  const size_t tbytes = packed ? ((size_t)m + 3) / 4 : (size_t)m;
+  const size_t seq0 = 64;
+  const size_t toff_b = (pbytes + 15) & ~(size_t)15;
+  const size_t total = seq0 + toff_b + ((tbytes + 15) & ~(size_t)15) + 16;
+  const int64_t cap = 2 * ((int64_t)n + m) + 1;
+  if (total > h->pinned_cap) {
+    if (h->pinned) cudaFreeHost(h->pinned);
+    h->pinned = nullptr;
+    h->pinned_cap = 0;
+    size_t want = std::max(total, (size_t)1 << 16);
+    CUDA_TRY(h, cudaMallocHost(&h->pinned, want), "pinned staging");
+    h->pinned_cap = want;
+  }
+  std::memset(h->pinned, 0, total);
+  Meta meta;
   meta.poff = 0;
   meta.toff = packed ? (int64_t)(toff_b / 4) : (int64_t)toff_b;
   meta.coff = 0;
   meta.plen = n;
   meta.tlen = m;
+  std::memcpy(h->pinned, &meta, sizeof meta);
+  if (pbytes) std::memcpy(h->pinned + seq0, p, pbytes);
+  if (tbytes) std::memcpy(h->pinned + seq0 + toff_b, t, tbytes);
   CUDA_TRY(h, h->seq.ensure(total), "seq");
-  CUDA_TRY(h, h->poff.ensure(64), "meta");
   CUDA_TRY(h, h->results.ensure(sizeof(wfa_result_t)), "results");
   CUDA_TRY(h, h->cigars.ensure((size_t)cap), "cigars");
-  std::vector<uint8_t> staging(total, 0);
-  if (pbytes) std::memcpy(staging.data(), p, pbytes);
-  if (tbytes) std::memcpy(staging.data() + toff_b, t, tbytes);
-  CUDA_TRY(h, cudaMemcpyAsync(h->seq.p, staging.data(), total, cudaMemcpyHostToDevice, st), "H2D");
-  CUDA_TRY(h, cudaMemcpyAsync(h->poff.p, &meta, sizeof meta, cudaMemcpyHostToDevice, st), "H2D");
-  const char* mb = h->poff.as<char>();
+  CUDA_TRY(h, cudaMemcpyAsync(h->seq.p, h->pinned, total, cudaMemcpyHostToDevice, st), "H2D");
+  const char* mb = h->seq.as<char>();
   wfa_batch_t b;
   b.format = packed ? WFA_SEQ_PACKED2 : WFA_SEQ_ASCII;
   b.span = span;
   b.num_pairs = 1;
-  b.seq = h->seq.p;
-  b.seq_bytes = (int64_t)total;
+  b.seq = mb + seq0;
+  b.seq_bytes = (int64_t)(total - seq0);
   b.p_off = reinterpret_cast<const int64_t*>(mb + offsetof(Meta, poff));
   b.t_off = reinterpret_cast<const int64_t*>(mb + offsetof(Meta, toff));
   b.cigar_off = reinterpret_cast<const int64_t*>(mb + offsetof(Meta, coff));
   b.p_len = reinterpret_cast<const int32_t*>(mb + offsetof(Meta, plen));
   b.t_len = reinterpret_cast<const int32_t*>(mb + offsetof(Meta, tlen));
   b.cigar_bytes = cap;
-  r = run_device_batch(h, &b, h->results.as<wfa_result_t>(), h->cigars.as<uint8_t>(), st, n + m);
+  AlignParams P;
+  fill_params(h, &b, P);
+  P.results = h->results.as<wfa_result_t>();
+  P.cigars = h->cigars.as<uint8_t>();
+  const bool aln = P.compute_alignment != 0;
+  Round rd = first_round(P, metric_components(P.metric), n + m);
+  r = launch_round(h, P, rd, 1, nullptr, st);
   if (r != WFA_OK) return r;
   wfa_result_t res;
-  CUDA_TRY(h, cudaMemcpyAsync(&res, h->results.p, sizeof res, cudaMemcpyDeviceToHost, st), "D2H");
+  uint8_t* hbuf = h->pinned;  // reuse staging for the way back
+  const size_t back = sizeof(wfa_result_t) + (aln ? (size_t)cap : 0);
+  if (back > h->pinned_cap) {
+    CUDA_TRY(h, cudaStreamSynchronize(st), "sync");
+    cudaFreeHost(h->pinned);
+    h->pinned = nullptr;
+    h->pinned_cap = 0;
+    CUDA_TRY(h, cudaMallocHost(&h->pinned, back), "pinned staging");
+    h->pinned_cap = back;
+    hbuf = h->pinned;
+  }
+  CUDA_TRY(h, cudaMemcpyAsync(hbuf, h->results.p, sizeof res, cudaMemcpyDeviceToHost, st), "D2H");
+  if (aln)
+    CUDA_TRY(h, cudaMemcpyAsync(hbuf + sizeof res, h->cigars.p, (size_t)cap, cudaMemcpyDeviceToHost, st), "D2H");
   CUDA_TRY(h, cudaStreamSynchronize(st), "D2H");
+  std::memcpy(&res, hbuf, sizeof res);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+  h->last_kernel_ms = ms;
+  if (res.status == kStatusRetry) {
+    r = run_device_batch(h, &b, h->results.as<wfa_result_t>(), h->cigars.as<uint8_t>(), st, n + m);
+    if (r != WFA_OK) return r;
+    CUDA_TRY(h, cudaMemcpyAsync(hbuf, h->results.p, sizeof res, cudaMemcpyDeviceToHost, st), "D2H");
+    if (aln)
+      CUDA_TRY(h, cudaMemcpyAsync(hbuf + sizeof res, h->cigars.p, (size_t)cap, cudaMemcpyDeviceToHost, st), "D2H");
+    CUDA_TRY(h, cudaStreamSynchronize(st), "D2H");
+    std::memcpy(&res, hbuf, sizeof res);
+  }
   if (res.cigar_length > 0) {
-    h->cigar.resize((size_t)res.cigar_length);
-    CUDA_TRY(h, cudaMemcpy(h->cigar.data(), h->cigars.as<uint8_t>() + res.cigar_begin,
-                           (size_t)res.cigar_length, cudaMemcpyDeviceToHost), "D2H");
+    const uint8_t* ops = hbuf + sizeof res + res.cigar_begin;
+    h->cigar.assign(ops, ops + res.cigar_length);
   }
   h->status = res.status;
   h->cigar_score = res.cigar_score;
@@ -510,6 +606,12 @@ int wfa_batch_align_device(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t*
   return run_device_batch(h, b, results, cigars, st, mx);
 }
 
+// Host-buffer batch, pipelined in chunks of pairs: while chunk c aligns on
+// the compute stream, chunk c+1's inputs are copied in and chunk c-1's results
+// and CIGARs are copied out.  CIGARs are packed densely per chunk, in input
+// order; results[i].cigar_begin is the offset of pair i's ops in `cigars`.
+// Pairs that need more scratch than the first configuration are re-run at
+// the end by the batch driver.
 int wfa_batch_align(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* results, uint8_t* cigars) {
   int r = batch_common(h, b);
   if (r != WFA_OK) return r;
@@ -519,19 +621,40 @@ int wfa_batch_align(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* result
   const bool aln = h->scope == WFA_SCOPE_ALIGNMENT;
   if (aln && !cigars) return WFA_ERR_ARGUMENT;
   cudaSetDevice(h->device);
-  cudaStream_t st = h->stream;
-  int32_t mx = 0;
+  cudaStream_t sc = h->stream, si = h->s_in, so = h->s_out;
+  const int64_t chunk = std::max<int64_t>(65536, std::min<int64_t>(262144, (n + 3) / 4));
+  const int64_t nchunks = (n + chunk - 1) / chunk;
+  const bool packed = b->format == WFA_SEQ_PACKED2;
+  const int64_t unit = packed ? 4 : 1;  // bytes per offset unit
+
+  // Per chunk: sequence byte range, longest pair, CIGAR slot range.
+  std::vector<int64_t> slot_off(aln ? (size_t)n : 0);
+  std::vector<int64_t> c_lo((size_t)nchunks), c_hi((size_t)nchunks), c_slot0((size_t)nchunks + 1);
+  std::vector<int32_t> c_max((size_t)nchunks);
   int64_t slot_total = 0;
-  std::vector<int64_t> slot_off;
-  if (aln) slot_off.resize((size_t)n);
-  for (int64_t i = 0; i < n; ++i) {
-    int32_t s = b->p_len[i] + b->t_len[i];
-    mx = std::max(mx, s);
-    if (aln) {
-      slot_off[(size_t)i] = slot_total;
-      slot_total += 2 * (int64_t)s + 1;
+  for (int64_t ci = 0; ci < nchunks; ++ci) {
+    int64_t a = ci * chunk, e = std::min(n, a + chunk);
+    int64_t lo = INT64_MAX, hi = 0;
+    int32_t mx = 0;
+    c_slot0[(size_t)ci] = slot_total;
+    for (int64_t i = a; i < e; ++i) {
+      int64_t pl = b->p_len[i], tl = b->t_len[i];
+      int64_t pe = packed ? b->p_off[i] * 4 + (pl + 15) / 16 * 4 : b->p_off[i] + pl;
+      int64_t te = packed ? b->t_off[i] * 4 + (tl + 15) / 16 * 4 : b->t_off[i] + tl;
+      lo = std::min(lo, std::min(b->p_off[i], b->t_off[i]) * unit);
+      hi = std::max(hi, std::max(pe, te));
+      mx = std::max<int32_t>(mx, (int32_t)(pl + tl));
+      if (aln) {
+        slot_off[(size_t)i] = slot_total;
+        slot_total += 2 * (pl + tl) + 1;
+      }
     }
+    c_lo[(size_t)ci] = lo == INT64_MAX ? 0 : (lo & ~(int64_t)15);
+    c_hi[(size_t)ci] = std::min<int64_t>(b->seq_bytes, (hi + 15) & ~(int64_t)15);
+    c_max[(size_t)ci] = mx;
   }
+  c_slot0[(size_t)nchunks] = slot_total;
+
   size_t seq_bytes = ((size_t)b->seq_bytes + 15) & ~(size_t)15;
   CUDA_TRY(h, h->seq.ensure(seq_bytes + 16), "seq");
   CUDA_TRY(h, h->poff.ensure((size_t)n * 8), "p_off");
@@ -539,52 +662,175 @@ int wfa_batch_align(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* result
   CUDA_TRY(h, h->plen.ensure((size_t)n * 4), "p_len");
   CUDA_TRY(h, h->tlen.ensure((size_t)n * 4), "t_len");
   CUDA_TRY(h, h->results.ensure((size_t)n * sizeof(wfa_result_t)), "results");
-  CUDA_TRY(h, cudaMemcpyAsync(h->seq.p, b->seq, (size_t)b->seq_bytes, cudaMemcpyHostToDevice, st), "H2D");
-  CUDA_TRY(h, cudaMemcpyAsync(h->poff.p, b->p_off, (size_t)n * 8, cudaMemcpyHostToDevice, st), "H2D");
-  CUDA_TRY(h, cudaMemcpyAsync(h->toff.p, b->t_off, (size_t)n * 8, cudaMemcpyHostToDevice, st), "H2D");
-  CUDA_TRY(h, cudaMemcpyAsync(h->plen.p, b->p_len, (size_t)n * 4, cudaMemcpyHostToDevice, st), "H2D");
-  CUDA_TRY(h, cudaMemcpyAsync(h->tlen.p, b->t_len, (size_t)n * 4, cudaMemcpyHostToDevice, st), "H2D");
-  wfa_batch_t d = *b;
-  d.seq = h->seq.p;
-  d.seq_bytes = (int64_t)seq_bytes;
-  d.p_off = h->poff.as<int64_t>();
-  d.t_off = h->toff.as<int64_t>();
-  d.p_len = h->plen.as<int32_t>();
-  d.t_len = h->tlen.as<int32_t>();
-  d.cigar_off = nullptr;
   if (aln) {
     CUDA_TRY(h, h->coff.ensure((size_t)n * 8), "cigar_off");
     CUDA_TRY(h, h->cigars.ensure((size_t)slot_total + 16), "cigar slots");
-    CUDA_TRY(h, cudaMemcpyAsync(h->coff.p, slot_off.data(), (size_t)n * 8, cudaMemcpyHostToDevice, st), "H2D");
-    d.cigar_off = h->coff.as<int64_t>();
-    d.cigar_bytes = slot_total;
+    CUDA_TRY(h, h->dense.ensure((size_t)slot_total + 16), "dense cigars");
+    CUDA_TRY(h, h->pairlist.ensure((size_t)n * 8), "dense offsets");
   }
-  r = run_device_batch(h, &d, h->results.as<wfa_result_t>(), aln ? h->cigars.as<uint8_t>() : nullptr, st, mx);
-  if (r != WFA_OK) return r;
-  CUDA_TRY(h, cudaMemcpyAsync(results, h->results.p, (size_t)n * sizeof(wfa_result_t),
-                              cudaMemcpyDeviceToHost, st), "D2H");
-  CUDA_TRY(h, cudaStreamSynchronize(st), "D2H");
-  if (!aln) return WFA_OK;
-  // Dense CIGAR packing in input order: results[i].cigar_begin becomes the
-  // offset of pair i's ops in `cigars`.
-  std::vector<int64_t> dst((size_t)n);
-  int64_t total = 0;
-  for (int64_t i = 0; i < n; ++i) {
-    dst[(size_t)i] = total;
-    total += results[i].cigar_length;
+  std::vector<cudaEvent_t> ev_in((size_t)nchunks), ev_k((size_t)nchunks), ev_res((size_t)nchunks),
+      ev_off((size_t)nchunks);
+  auto destroy = [&]() {
+    for (auto* v : {&ev_in, &ev_k, &ev_res, &ev_off})
+      for (auto& e : *v)
+        if (e) cudaEventDestroy(e);
+  };
+  for (int64_t ci = 0; ci < nchunks; ++ci) {
+    for (auto* v : {&ev_in, &ev_k, &ev_res, &ev_off}) {
+      cudaEvent_t e = nullptr;
+      if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+        destroy();
+        return fail(h, WFA_ERR_CUDA, "event");
+      }
+      (*v)[(size_t)ci] = e;
+    }
   }
-  CUDA_TRY(h, h->dense.ensure((size_t)total + 16), "dense cigars");
-  CUDA_TRY(h, h->pairlist.ensure((size_t)n * 8), "offsets");
-  CUDA_TRY(h, cudaMemcpyAsync(h->pairlist.p, dst.data(), (size_t)n * 8, cudaMemcpyHostToDevice, st), "H2D");
-  int64_t threads = n * 32;
-  compact_cigars<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(
-      h->results.as<wfa_result_t>(), d.cigar_off, h->cigars.as<uint8_t>(), h->pairlist.as<int64_t>(),
-      h->dense.as<uint8_t>(), n);
-  h->launches++;
-  CUDA_TRY(h, cudaGetLastError(), "compact cigars");
-  CUDA_TRY(h, cudaMemcpyAsync(cigars, h->dense.p, (size_t)total, cudaMemcpyDeviceToHost, st), "D2H");
-  CUDA_TRY(h, cudaStreamSynchronize(st), "D2H");
-  for (int64_t i = 0; i < n; ++i) results[i].cigar_begin = (int32_t)dst[(size_t)i];
+  uint8_t* dseq = h->seq.as<uint8_t>();
+  int64_t *dpo = h->poff.as<int64_t>(), *dto = h->toff.as<int64_t>();
+  int32_t *dpl = h->plen.as<int32_t>(), *dtl = h->tlen.as<int32_t>();
+  wfa_result_t* dres = h->results.as<wfa_result_t>();
+  int64_t* dco = aln ? h->coff.as<int64_t>() : nullptr;
+  int64_t* ddst = aln ? h->pairlist.as<int64_t>() : nullptr;
+  h->last_kernel_ms = 0.0;
+
+#define PIPE_TRY(expr, what)                                                         \
+  do {                                                                               \
+    cudaError_t _e = (expr);                                                         \
+    if (_e != cudaSuccess) {                                                         \
+      destroy();                                                                     \
+      return fail(h, _e == cudaErrorMemoryAllocation ? WFA_ERR_OOM : WFA_ERR_CUDA, what, _e); \
+    }                                                                                \
+  } while (0)
+
+  // Phase 1, every chunk: inputs in (s_in), align (compute), results out (s_out).
+  for (int64_t ci = 0; ci < nchunks; ++ci) {
+    const int64_t a = ci * chunk, e = std::min(n, a + chunk), cn = e - a;
+    const size_t lo = (size_t)c_lo[(size_t)ci], hi = (size_t)c_hi[(size_t)ci];
+    if (hi > lo) PIPE_TRY(cudaMemcpyAsync(dseq + lo, (const uint8_t*)b->seq + lo, hi - lo, cudaMemcpyHostToDevice, si), "H2D");
+    PIPE_TRY(cudaMemcpyAsync(dpo + a, b->p_off + a, (size_t)cn * 8, cudaMemcpyHostToDevice, si), "H2D");
+    PIPE_TRY(cudaMemcpyAsync(dto + a, b->t_off + a, (size_t)cn * 8, cudaMemcpyHostToDevice, si), "H2D");
+    PIPE_TRY(cudaMemcpyAsync(dpl + a, b->p_len + a, (size_t)cn * 4, cudaMemcpyHostToDevice, si), "H2D");
+    PIPE_TRY(cudaMemcpyAsync(dtl + a, b->t_len + a, (size_t)cn * 4, cudaMemcpyHostToDevice, si), "H2D");
+    if (aln) PIPE_TRY(cudaMemcpyAsync(dco + a, slot_off.data() + a, (size_t)cn * 8, cudaMemcpyHostToDevice, si), "H2D");
+    PIPE_TRY(cudaEventRecord(ev_in[(size_t)ci], si), "event");
+    PIPE_TRY(cudaStreamWaitEvent(sc, ev_in[(size_t)ci], 0), "wait");
+    wfa_batch_t cb = *b;
+    cb.num_pairs = cn;
+    cb.seq = dseq;
+    cb.seq_bytes = (int64_t)seq_bytes;
+    cb.p_off = dpo + a; cb.t_off = dto + a; cb.p_len = dpl + a; cb.t_len = dtl + a;
+    cb.cigar_off = aln ? dco + a : nullptr;
+    cb.cigar_bytes = slot_total;
+    AlignParams P;
+    fill_params(h, &cb, P);
+    P.results = dres + a;
+    P.cigars = aln ? h->cigars.as<uint8_t>() : nullptr;
+    Round rd = first_round(P, metric_components(P.metric), c_max[(size_t)ci]);
+    int e2 = launch_round(h, P, rd, cn, nullptr, sc);
+    if (e2 != WFA_OK) { destroy(); return e2; }
+    PIPE_TRY(cudaEventRecord(ev_k[(size_t)ci], sc), "event");
+    PIPE_TRY(cudaStreamWaitEvent(so, ev_k[(size_t)ci], 0), "wait");
+    PIPE_TRY(cudaMemcpyAsync(results + a, dres + a, (size_t)cn * sizeof(wfa_result_t), cudaMemcpyDeviceToHost, so), "D2H");
+    PIPE_TRY(cudaEventRecord(ev_res[(size_t)ci], so), "event");
+  }
+
+  // Phase 2, as each chunk's results arrive: dense CIGAR offsets (host), then
+  // compaction (compute stream) and the dense copy out (s_out).
+  std::vector<int64_t> dst(aln ? (size_t)n : 0);
+  std::vector<int64_t> retry;
+  int64_t dense_total = 0;
+  for (int64_t ci = 0; ci < nchunks; ++ci) {
+    const int64_t a = ci * chunk, e = std::min(n, a + chunk), cn = e - a;
+    PIPE_TRY(cudaEventSynchronize(ev_res[(size_t)ci]), "results");
+    const int64_t d0 = dense_total;
+    for (int64_t i = a; i < e; ++i) {
+      if (results[i].status == kStatusRetry) { retry.push_back(i); results[i].cigar_length = 0; }
+      if (aln) {
+        dst[(size_t)i] = dense_total;
+        dense_total += results[i].cigar_length;
+      }
+    }
+    if (!aln || dense_total == d0) continue;
+    PIPE_TRY(cudaMemcpyAsync(ddst + a, dst.data() + a, (size_t)cn * 8, cudaMemcpyHostToDevice, si), "H2D");
+    PIPE_TRY(cudaEventRecord(ev_off[(size_t)ci], si), "event");
+    PIPE_TRY(cudaStreamWaitEvent(sc, ev_off[(size_t)ci], 0), "wait");
+    compact_cigars<<<(unsigned)((cn * 32 + 255) / 256), 256, 0, sc>>>(
+        dres + a, dco + a, h->cigars.as<uint8_t>(), ddst + a, h->dense.as<uint8_t>(), cn);
+    h->launches++;
+    PIPE_TRY(cudaGetLastError(), "compact cigars");
+    PIPE_TRY(cudaEventRecord(ev_k[(size_t)ci], sc), "event");
+    PIPE_TRY(cudaStreamWaitEvent(so, ev_k[(size_t)ci], 0), "wait");
+    PIPE_TRY(cudaMemcpyAsync(cigars + d0, h->dense.as<uint8_t>() + d0, (size_t)(dense_total - d0),
+                             cudaMemcpyDeviceToHost, so), "D2H");
+  }
+  PIPE_TRY(cudaStreamSynchronize(so), "D2H");
+  PIPE_TRY(cudaStreamSynchronize(sc), "compute");
+  destroy();
+#undef PIPE_TRY
+  for (int64_t i = 0; i < n; ++i)
+    if (aln) results[i].cigar_begin = (int32_t)dst[(size_t)i];
+
+  // Pairs that outgrew the first configuration: re-run with the batch driver.
+  if (!retry.empty()) {
+    const int64_t rn = (int64_t)retry.size();
+    std::vector<int64_t> po(rn), to(rn), co(rn);
+    std::vector<int32_t> pl(rn), tl(rn);
+    int32_t mx = 0;
+    int64_t rslot = 0;
+    for (int64_t j = 0; j < rn; ++j) {
+      int64_t i = retry[(size_t)j];
+      po[j] = b->p_off[i]; to[j] = b->t_off[i]; pl[j] = b->p_len[i]; tl[j] = b->t_len[i];
+      mx = std::max<int32_t>(mx, pl[j] + tl[j]);
+      co[j] = rslot;
+      rslot += 2 * ((int64_t)pl[j] + tl[j]) + 1;
+    }
+    DevBuf rbuf;
+    size_t need = (size_t)rn * (8 * 3 + 4 * 2 + sizeof(wfa_result_t)) + (size_t)rslot + 64;
+    CUDA_TRY(h, rbuf.ensure(need), "retry buffers");
+    char* base = rbuf.as<char>();
+    int64_t* rpo = reinterpret_cast<int64_t*>(base);
+    int64_t* rto = rpo + rn;
+    int64_t* rco = rto + rn;
+    int32_t* rpl = reinterpret_cast<int32_t*>(rco + rn);
+    int32_t* rtl = rpl + rn;
+    wfa_result_t* rres = reinterpret_cast<wfa_result_t*>(reinterpret_cast<char*>(rtl + rn) + ((rn & 1) ? 4 : 0));
+    uint8_t* rcig = reinterpret_cast<uint8_t*>(rres + rn);
+    cudaMemcpyAsync(rpo, po.data(), rn * 8, cudaMemcpyHostToDevice, sc);
+    cudaMemcpyAsync(rto, to.data(), rn * 8, cudaMemcpyHostToDevice, sc);
+    cudaMemcpyAsync(rco, co.data(), rn * 8, cudaMemcpyHostToDevice, sc);
+    cudaMemcpyAsync(rpl, pl.data(), rn * 4, cudaMemcpyHostToDevice, sc);
+    cudaMemcpyAsync(rtl, tl.data(), rn * 4, cudaMemcpyHostToDevice, sc);
+    wfa_batch_t rb = *b;
+    rb.num_pairs = rn;
+    rb.seq = dseq;
+    rb.seq_bytes = (int64_t)seq_bytes;
+    rb.p_off = rpo; rb.t_off = rto; rb.p_len = rpl; rb.t_len = rtl;
+    rb.cigar_off = aln ? rco : nullptr;
+    rb.cigar_bytes = rslot;
+    double kms = h->last_kernel_ms;
+    int e3 = run_device_batch(h, &rb, rres, aln ? rcig : nullptr, sc, mx);
+    h->last_kernel_ms += kms;
+    if (e3 != WFA_OK) { rbuf.release(); return e3; }
+    std::vector<wfa_result_t> rr((size_t)rn);
+    std::vector<uint8_t> rc(aln ? (size_t)rslot : 0);
+    cudaMemcpyAsync(rr.data(), rres, rn * sizeof(wfa_result_t), cudaMemcpyDeviceToHost, sc);
+    if (aln) cudaMemcpyAsync(rc.data(), rcig, (size_t)rslot, cudaMemcpyDeviceToHost, sc);
+    cudaError_t es = cudaStreamSynchronize(sc);
+    rbuf.release();
+    if (es != cudaSuccess) return fail(h, WFA_ERR_CUDA, "retry D2H", es);
+    for (int64_t j = 0; j < rn; ++j) {
+      int64_t i = retry[(size_t)j];
+      wfa_result_t x = rr[(size_t)j];
+      if (aln && x.cigar_length > 0) {
+        std::memcpy(cigars + dense_total, rc.data() + co[j] + x.cigar_begin, (size_t)x.cigar_length);
+        x.cigar_begin = (int32_t)dense_total;
+        dense_total += x.cigar_length;
+      } else {
+        x.cigar_begin = 0;
+      }
+      results[i] = x;
+    }
+  }
   return WFA_OK;
 }
 

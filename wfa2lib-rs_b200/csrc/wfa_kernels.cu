@@ -3,9 +3,10 @@
 // Launch shape: blocks of kWarpsPerBlock warps, grid sized to the SM count
 // times the resident blocks per SM.  Each warp pulls pair indices from a
 // device counter (work queue), so pairs of uneven length and score balance
-// across the machine; its wavefront descriptors live in shared memory and its
-// wavefront cells in a private slice of the scratch buffer (ring slots, plus
-// the M history in CIGAR mode).
+// across the machine.  Per warp, shared memory holds the wavefront
+// descriptor ring, the pair's sequences (when short enough) and, when the
+// ring is narrow enough, its cells; otherwise cells live in the warp's slice
+// of the scratch buffer, as does the M history of CIGAR mode.
 #include <cuda_runtime.h>
 
 #include "wfa_align.cuh"
@@ -13,22 +14,31 @@
 
 namespace wfab {
 
-template <int CLS, int ENC>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+// Register budget: the lean instantiations of the smaller metrics fit 80
+// registers (6 blocks = 24 warps per SM); the general and two-piece ones keep
+// 128 (4 blocks) rather than spill.
+template <int CLS, bool GEN>
+constexpr int min_blocks() { return (GEN || CLS == kAffine2pClass) ? 4 : kMinBlocksPerSM; }
+
+template <int CLS, int ENC, bool GEN>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, (min_blocks<CLS, GEN>()))
     unialign_kernel(const AlignParams P) {
   extern __shared__ __align__(16) uint8_t smem[];
   const int wib = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   const int64_t gwarp = (int64_t)blockIdx.x * kWarpsPerBlock + wib;
   constexpr int NC = CLS == kAffine2pClass ? 5 : CLS == kAffineClass ? 3 : 1;
+  const SmemLayout L = smem_layout(P.scope, NC, P.ring_smem ? P.wmax : 0, P.seq_smem_words);
   Workspace ws;
-  ws.ring = reinterpret_cast<WfD*>(smem) + (int64_t)wib * P.scope * NC;
+  ws.ring = reinterpret_cast<WfD*>(smem + L.desc_off + (size_t)wib * L.desc_bytes);
+  uint32_t* sseq = reinterpret_cast<uint32_t*>(smem + L.seq_off + (size_t)wib * L.seq_bytes);
   int32_t* slice = P.scratch + gwarp * P.warp_words;
-  ws.ringv = slice;
-  int64_t ring_words = (int64_t)P.scope * NC * P.wmax;
-  ring_words = (ring_words + 3) & ~(int64_t)3;
+  int64_t ring_words = P.ring_smem ? 0 : (((int64_t)P.scope * NC * P.wmax + 3) & ~(int64_t)3);
+  ws.ringv = P.ring_smem ? reinterpret_cast<int32_t*>(smem + L.ring_off + (size_t)wib * L.ring_bytes)
+                         : slice;
   ws.hist = reinterpret_cast<int4*>(slice + ring_words);
   ws.harena = slice + ring_words + (int64_t)P.hist_scores * 4;
+  const int sw = P.seq_smem_words;
   for (;;) {
     unsigned long long idx = 0;
     if (lane == 0) idx = atomicAdd(P.work_counter, 1ull);
@@ -40,11 +50,31 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
       const uint32_t* w = reinterpret_cast<const uint32_t*>(P.seq);
       SeqPacked sp{w + P.p_off[pair], P.p_len[pair], (P.p_len[pair] + 15) >> 4};
       SeqPacked st{w + P.t_off[pair], P.t_len[pair], (P.t_len[pair] + 15) >> 4};
-      retry = align_one<CLS, SeqPacked>(P, ws, pair, sp, st);
+      // Stage both sequences in shared memory when they fit.
+      if (sp.nw <= sw && st.nw <= sw) {
+        for (int i = lane; i < sp.nw; i += 32) sseq[i] = sp.w[i];
+        for (int i = lane; i < st.nw; i += 32) sseq[sw + i] = st.w[i];
+        __syncwarp();
+        sp.w = sseq;
+        st.w = sseq + sw;
+      }
+      retry = align_one<CLS, SeqPacked, GEN>(P, ws, pair, sp, st);
     } else {
       SeqAscii sp{P.seq + P.p_off[pair], P.p_len[pair]};
       SeqAscii st{P.seq + P.t_off[pair], P.t_len[pair]};
-      retry = align_one<CLS, SeqAscii>(P, ws, pair, sp, st);
+      const uintptr_t pa = (uintptr_t)sp.p, ta = (uintptr_t)st.p;
+      const int pw = sp.len > 0 ? (int)(((pa + sp.len + 3) & ~(uintptr_t)3) - (pa & ~(uintptr_t)3)) / 4 : 0;
+      const int tw = st.len > 0 ? (int)(((ta + st.len + 3) & ~(uintptr_t)3) - (ta & ~(uintptr_t)3)) / 4 : 0;
+      if (pw <= sw && tw <= sw) {
+        const uint32_t* pg = reinterpret_cast<const uint32_t*>(pa & ~(uintptr_t)3);
+        const uint32_t* tg = reinterpret_cast<const uint32_t*>(ta & ~(uintptr_t)3);
+        for (int i = lane; i < pw; i += 32) sseq[i] = pg[i];
+        for (int i = lane; i < tw; i += 32) sseq[sw + i] = tg[i];
+        __syncwarp();
+        sp.p = reinterpret_cast<const uint8_t*>(sseq) + (pa & 3);
+        st.p = reinterpret_cast<const uint8_t*>(sseq + sw) + (ta & 3);
+      }
+      retry = align_one<CLS, SeqAscii, GEN>(P, ws, pair, sp, st);
     }
     if (retry && lane == 0) {
       P.results[pair].status = kStatusRetry;
@@ -54,44 +84,69 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
   }
 }
 
-template <int CLS, int ENC>
+template <int CLS, int ENC, bool GEN>
 static cudaError_t launch_t(const AlignParams& P, int blocks, size_t smem, cudaStream_t st) {
-  auto k = unialign_kernel<CLS, ENC>;
-  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
+  auto k = unialign_kernel<CLS, ENC, GEN>;
+  static size_t configured = 0;  // dynamic shared memory already allowed for k
+  if (smem > configured) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    configured = smem;
+  }
   k<<<blocks, kWarpsPerBlock * 32, smem, st>>>(P);
   return cudaGetLastError();
 }
 
-cudaError_t launch_unialign(const AlignParams& P, int metric_class, int blocks, size_t smem,
-                            cudaStream_t st) {
-  const bool packed = P.format == WFA_SEQ_PACKED2;
-  switch (metric_class) {
-    case kEditClass:
-      return packed ? launch_t<kEditClass, 1>(P, blocks, smem, st) : launch_t<kEditClass, 0>(P, blocks, smem, st);
-    case kLinearClass:
-      return packed ? launch_t<kLinearClass, 1>(P, blocks, smem, st) : launch_t<kLinearClass, 0>(P, blocks, smem, st);
-    case kAffineClass:
-      return packed ? launch_t<kAffineClass, 1>(P, blocks, smem, st) : launch_t<kAffineClass, 0>(P, blocks, smem, st);
-    default:
-      return packed ? launch_t<kAffine2pClass, 1>(P, blocks, smem, st)
-                    : launch_t<kAffine2pClass, 0>(P, blocks, smem, st);
+template <int CLS, bool GEN>
+static cudaError_t launch_c(const AlignParams& P, int blocks, size_t smem, cudaStream_t st) {
+  return P.format == WFA_SEQ_PACKED2 ? launch_t<CLS, 1, GEN>(P, blocks, smem, st)
+                                     : launch_t<CLS, 0, GEN>(P, blocks, smem, st);
+}
+
+template <bool GEN>
+static cudaError_t launch_g(const AlignParams& P, int cls, int blocks, size_t smem, cudaStream_t st) {
+  switch (cls) {
+    case kEditClass: return launch_c<kEditClass, GEN>(P, blocks, smem, st);
+    case kLinearClass: return launch_c<kLinearClass, GEN>(P, blocks, smem, st);
+    case kAffineClass: return launch_c<kAffineClass, GEN>(P, blocks, smem, st);
+    default: return launch_c<kAffine2pClass, GEN>(P, blocks, smem, st);
   }
 }
 
-int occupancy_blocks_per_sm(int metric_class, bool packed, size_t smem) {
+bool needs_general(const AlignParams& P) {
+  return P.span != WFA_SPAN_END2END || P.hkind != WFA_HEURISTIC_NONE;
+}
+
+cudaError_t launch_unialign(const AlignParams& P, int metric_class, int blocks, size_t smem,
+                            cudaStream_t st) {
+  return needs_general(P) ? launch_g<true>(P, metric_class, blocks, smem, st)
+                          : launch_g<false>(P, metric_class, blocks, smem, st);
+}
+
+template <int CLS, int ENC, bool GEN>
+static int occ_t(size_t smem) {
   int nb = 0;
-  cudaError_t e = cudaSuccess;
-#define OCC(C, E) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, unialign_kernel<C, E>, kWarpsPerBlock * 32, smem)
-  switch (metric_class) {
-    case kEditClass: if (packed) OCC(kEditClass, 1); else OCC(kEditClass, 0); break;
-    case kLinearClass: if (packed) OCC(kLinearClass, 1); else OCC(kLinearClass, 0); break;
-    case kAffineClass: if (packed) OCC(kAffineClass, 1); else OCC(kAffineClass, 0); break;
-    default: if (packed) OCC(kAffine2pClass, 1); else OCC(kAffine2pClass, 0); break;
+  auto k = unialign_kernel<CLS, ENC, GEN>;
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, kWarpsPerBlock * 32, smem) != cudaSuccess)
+    nb = 1;
+  return nb < 1 ? 1 : nb;
+}
+
+template <bool GEN>
+static int occ_g(int cls, bool packed, size_t smem) {
+  switch (cls) {
+    case kEditClass: return packed ? occ_t<kEditClass, 1, GEN>(smem) : occ_t<kEditClass, 0, GEN>(smem);
+    case kLinearClass: return packed ? occ_t<kLinearClass, 1, GEN>(smem) : occ_t<kLinearClass, 0, GEN>(smem);
+    case kAffineClass: return packed ? occ_t<kAffineClass, 1, GEN>(smem) : occ_t<kAffineClass, 0, GEN>(smem);
+    default: return packed ? occ_t<kAffine2pClass, 1, GEN>(smem) : occ_t<kAffine2pClass, 0, GEN>(smem);
   }
-#undef OCC
-  if (e != cudaSuccess || nb < 1) nb = 1;
-  return nb;
+}
+
+int occupancy_blocks_per_sm(const AlignParams& P, int metric_class, size_t smem) {
+  const bool packed = P.format == WFA_SEQ_PACKED2;
+  return needs_general(P) ? occ_g<true>(metric_class, packed, smem)
+                          : occ_g<false>(metric_class, packed, smem);
 }
 
 }  // namespace wfab
