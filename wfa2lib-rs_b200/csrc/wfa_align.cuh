@@ -252,6 +252,12 @@ struct PairAligner {
   int32_t p0, pf, t0, tf;
   bool endsfree;
   int32_t hist_lo, hist_hi;
+  int32_t cscore, cidx;  // current score and its ring index
+  // Scores that are not multiples of gstep can have no wavefront: every input
+  // score differs from them by a multiple of gstep (the gcd of the score
+  // offsets the recurrences use, and of the begin-free seed scores).  Their
+  // steps are the reference's all-null steps; only the null-step count moves.
+  int32_t gstep, gphase;
   int32_t num_null_steps;
   int32_t status;
   int32_t end_score, end_k, end_off;
@@ -268,7 +274,17 @@ struct PairAligner {
   WFA_D bool ef() const { return GEN && endsfree; }
 
   // ---- slots --------------------------------------------------------------
-  WFA_D WfD& slot(int c, int s) { return ws.ring[(s % scope) * NC + c]; }
+  // Ring index of score t (cscore - scope < t <= cscore), kept without a
+  // division: cidx == cscore % scope is advanced with the score loop.
+  WFA_D int sidx(int t) const {
+    int i = cidx - (cscore - t);
+    return i < 0 ? i + scope : i;
+  }
+  WFA_D void advance() {
+    ++cscore;
+    cidx = cidx + 1 == scope ? 0 : cidx + 1;
+  }
+  WFA_D WfD& slot(int c, int s) { return ws.ring[sidx(s) * NC + c]; }
   // Slot (c, s) holds a live wavefront: present and not null (flags are
   // 0 none, kPresent, or kPresent|kNullFlag).
   WFA_D bool live(int c, int s) { return s >= 0 && slot(c, s).flags == kPresent; }
@@ -290,7 +306,7 @@ struct PairAligner {
   WFA_D int32_t* alloc(int c, int s, int L, int H) {
     int64_t w = (int64_t)H - L + 1;
     if (w > wmax) { retry = true; return nullptr; }
-    return ws.ringv + ((int64_t)((s % scope) * NC + c)) * wmax;
+    return ws.ringv + ((int64_t)(sidx(s) * NC + c)) * wmax;
   }
   // High memory: once M at score s is final (after its extend step), copy its
   // initialised range to the history arena for the backtrace.
@@ -309,7 +325,7 @@ struct PairAligner {
       hused += w;
     }
     if (lane == 0) ws.hist[s] = r;
-    Warp::sync();
+    // No sync: the history is read only by the backtrace, which starts with one.
   }
 
   // ---- helpers --------------------------------------------------------------
@@ -433,7 +449,26 @@ struct PairAligner {
   }
 
   // ---- init_alignment, src/aligner.rs:846-1000 ------------------------------
+  static WFA_D int gcd(int a, int b) {
+    a = a < 0 ? -a : a;
+    b = b < 0 ? -b : b;
+    while (b) { int t = a % b; a = b; b = t; }
+    return a;
+  }
+  WFA_D int score_step_gcd() const {
+    int g;
+    if (CLS == kEditClass) return 1;
+    if (CLS == kLinearClass) g = gcd(P.mismatch, P.o1);
+    else g = gcd(gcd(P.mismatch, P.o1 + P.e1), P.e1);
+    if (TWO) g = gcd(gcd(g, P.o2 + P.e2), P.e2);
+    if (ef() && P.match != 0 && (p0 > 0 || t0 > 0)) g = gcd(g, -P.match);
+    return g < 1 ? 1 : g;
+  }
   WFA_D void init_alignment() {
+    cscore = 0;
+    cidx = 0;
+    gstep = score_step_gcd();
+    gphase = 0;
     for (int i = lane; i < scope * NC; i += WFA_WARP) ws.ring[i] = wf_none();
     Warp::sync();
     hist_lo = -(n + scope + 2);
@@ -1015,6 +1050,7 @@ struct PairAligner {
   }
 
   WFA_D void backtrace_from(int score, int k, int offset) {  // src/aligner.rs:1414-1436
+    Warp::sync();
     cg_end = cg_cap;
     cg_begin = cg_cap - 1;
     if (AFF) backtrace_singletrack(score, k, offset);
@@ -1179,12 +1215,25 @@ struct PairAligner {
     const int hard_limit = 1 << 26;  // no reference alignment runs this long
     if (!retry) {
       for (;;) {
-        bool done = extend_step(score);
-        hist_commit(score);
+        bool done;
+        if (gphase != 0) {  // all-null score: no M to extend (extend_end2end, null branch)
+          done = num_null_steps > scope;
+          if (done) status = WFA_STATUS_END_UNREACHABLE;
+          if (!modular) {
+            if (score >= P.hist_scores) { retry = true; break; }
+            if (lane == 0) ws.hist[score] = int4{1, 0, 0, 0};
+          }
+        } else {
+          done = extend_step(score);
+          hist_commit(score);
+        }
         if (done || retry) break;
         ++score;
+        advance();
+        gphase = gphase + 1 == gstep ? 0 : gphase + 1;
         if (!has_slot(score)) { status = WFA_STATUS_MAX_STEPS_REACHED; break; }
-        compute_step(score);
+        if (gphase != 0) ++num_null_steps;
+        else compute_step(score);
         if (retry) break;
         if (score >= P.max_steps || score >= hard_limit) { status = WFA_STATUS_MAX_STEPS_REACHED; break; }
       }
