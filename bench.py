@@ -1,5 +1,8 @@
 """Benchmark: short-read batch (1,000,000 pairs, 100-150 bp, 0-4% edits,
-2-bit packed), gap-affine (0,4,6,2), end-to-end, score + CIGAR.
+2-bit packed), gap-affine (0,4,6,2), end-to-end, score + CIGAR.  Other
+workloads (`--workload small|longread`): 10,000 x 100 bp pairs at 5% edits,
+and an uneven long-read batch (1-20 kbp, 5-15% edits, gap-affine 2-piece,
+BiWFA).
 
 A step is one batched alignment of the whole pair set.  `value` is pairs/s
 with inputs resident in HBM (device-buffer API, CUDA events on the launching
@@ -45,10 +48,27 @@ def dist_env():
     return rank, world, local
 
 
-def make_workload(num_pairs, rank):
+# Workloads: (description, generator, metric, penalties, span, oracle mode).
+# span 0 = align_end2end, 2 = BiWFA (align_biwfa).
+WORKLOADS = {
+    "shortread": (WORKLOAD, "short", 3, [0, 4, 6, 2], 0, 0),
+    "small": ("plain method, small: 10,000 x 100 bp, p=0.05, gap-affine 0,4,6,2, end-to-end, "
+              "score+CIGAR (2-bit packed)", "small", 3, [0, 4, 6, 2], 0, 0),
+    "longread": ("uneven long-read batch: 20,000 pairs, n log-uniform [1,20] kbp, p~U[0.05,0.15], "
+                 "60% indels (geometric, mean 3), gap-affine 2-piece 0,4,6,2,24,1, BiWFA, CIGAR "
+                 "(2-bit packed)", "long", 4, [0, 4, 6, 2, 24, 1], 2, 2),
+}
+
+
+def make_workload(num_pairs, rank, kind="short"):
     pkg = load_pkg()
     from wfa_b200 import synth
-    ps = synth.uniform_pairs(num_pairs, 100, 150, 0.0, 0.04, synth.SEED_BASE + 2 + 1000 * rank)
+    if kind == "short":
+        ps = synth.uniform_pairs(num_pairs, 100, 150, 0.0, 0.04, synth.SEED_BASE + 2 + 1000 * rank)
+    elif kind == "small":
+        ps = synth.uniform_pairs(num_pairs, 100, 100, 0.05, 0.05, synth.SEED_BASE + 1 + 1000 * rank)
+    else:
+        ps = synth.config3(num_pairs, synth.SEED_BASE + 3 + 1000 * rank)
     words, pwo, two = synth.pack2bits(ps)
     words = np.concatenate([words, np.zeros(4, np.uint32)])
     return pkg, synth, ps, words, pwo, two
@@ -116,14 +136,15 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def cpu_baseline(ps, threads, max_pairs=None):
+def cpu_baseline(ps, threads, max_pairs=None, metric=3, pen=PEN, mode=0):
     """The oracle (C++ restatement) on the host cores; returns (pairs/s, pairs, secs)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     n = len(ps) if max_pairs is None else min(len(ps), max_pairs)
     sub = ps.subset(np.arange(n))
-    secs, _, _, _ = O.batch(3, PEN, ps.buf.tobytes(), sub.p_off, sub.p_len, sub.t_off, sub.t_len,
-                            compute_alignment=True, mode=0, threads=threads, want_results=False)
+    secs, _, _, _ = O.batch(metric, pen, ps.buf.tobytes(), sub.p_off, sub.p_len, sub.t_off,
+                            sub.t_len, compute_alignment=True, mode=mode, threads=threads,
+                            want_results=False)
     return n / secs, n, secs
 
 
@@ -131,14 +152,15 @@ def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    pkg, synth, ps, _, _, _ = make_workload(args.pairs, 0)
+    desc, kind, metric, pen, span, omode = WORKLOADS[args.workload]
+    pkg, synth, ps, _, _, _ = make_workload(args.pairs, 0, kind)
     threads = os.cpu_count() or 1
     sample = min(len(ps), args.cpu_sample)
     for _ in range(args.warmup):
-        cpu_baseline(ps, threads, max_pairs=min(sample, 20_000))
+        cpu_baseline(ps, threads, max_pairs=min(sample, 2 * threads), metric=metric, pen=pen, mode=omode)
     tot_secs, tot_pairs = 0.0, 0
     for _ in range(args.steps):
-        rate, n, secs = cpu_baseline(ps, threads, max_pairs=sample)
+        rate, n, secs = cpu_baseline(ps, threads, max_pairs=sample, metric=metric, pen=pen, mode=omode)
         tot_secs += secs
         tot_pairs += n
     value = tot_pairs / tot_secs
@@ -147,7 +169,7 @@ def run_reference(args):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000 * tot_secs / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)",
-            "config": {"workload": WORKLOAD, "sample_pairs_per_step": sample},
+            "config": {"workload": desc, "sample_pairs_per_step": sample},
             "gcups": value * cells / 1e9,
             "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": threads, "kind": "port",
                              "sample": f"{sample} pairs of the workload per step"},
@@ -165,9 +187,10 @@ def run_gpu(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    pkg, synth, ps, words, pwo, two = make_workload(args.pairs, rank)
+    desc, kind, metric, pen, span, omode = WORKLOADS[args.workload]
+    pkg, synth, ps, words, pwo, two = make_workload(args.pairs, rank, kind)
     n = len(ps)
-    a = pkg.WavefrontAligner(pkg.GAP_AFFINE, PEN, device=local)
+    a = pkg.WavefrontAligner(metric, pen, device=local)
     a.set_alignment_scope(True)
 
     # Device-resident inputs and outputs.
@@ -186,7 +209,7 @@ def run_gpu(args):
         a.align_batch_device(t_words.data_ptr(), t_words.numel() * 4, t_po.data_ptr(),
                              t_pl.data_ptr(), t_to.data_ptr(), t_tl.data_ptr(), n, res.data_ptr(),
                              cig.data_ptr(), t_co.data_ptr(), int(caps.sum()), packed=True,
-                             stream=stream.cuda_stream)
+                             span=span, stream=stream.cuda_stream)
 
     for _ in range(args.warmup):
         step()
@@ -246,7 +269,7 @@ def run_gpu(args):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         hr, hc = a.align_batch(h_words, h_po, h_pl, h_to, h_tl, packed=True, out_results=h_res,
-                               out_cigars=h_cig)
+                               out_cigars=h_cig, span=span)
         t1 = time.perf_counter()
         if i >= args.warmup:
             e2e_ms.append((t1 - t0) * 1000)
@@ -263,11 +286,12 @@ def run_gpu(args):
     # Plain per-call form: one pair per call (host buffers), on a sample.
     plain_n = min(args.plain_pairs, n)
     raw = [ps.pair(i) for i in range(plain_n)]
-    for p, t in raw[:50]:
-        a.align_end2end(p, t)
+    plain = a.align_biwfa if span == 2 else a.align_end2end
+    for p, t in raw[:min(50, plain_n)]:
+        plain(p, t)
     t0 = time.perf_counter()
     for p, t in raw:
-        a.align_end2end(p, t)
+        plain(p, t)
     plain_secs = time.perf_counter() - t0
     plain_value = plain_n / plain_secs
 
@@ -275,13 +299,14 @@ def run_gpu(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic (seeded)",
-            "config": {"workload": WORKLOAD, "pairs_per_gpu": n, "l2": "flushed (512 MiB write) between steps",
+            "config": {"workload": desc, "pairs_per_gpu": n, "l2": "flushed (512 MiB write) between steps",
                        "form": "batched persistent kernel, device-resident inputs"},
             "gcups": world * cells * args.steps / (total_ms / 1000.0) / 1e9,
             "e2e": {"value": e2e_value, "unit": "pairs/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "api": "wfa_batch_align (pinned host buffers)"},
             "plain": {"value": plain_value, "unit": "pairs/s", "pairs": plain_n,
-                      "api": "wfa_align_end2end, one pair per call"},
+                      "api": ("wfa_align_biwfa" if span == 2 else "wfa_align_end2end")
+                             + ", one pair per call"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved / hbm_peak, "traffic": None, "peak_kind": peak_kind,
                          "kernel_ms": kms, "algorithmic_bytes_per_launch": alg_bytes},
@@ -289,7 +314,8 @@ def run_gpu(args):
             "clocks": clk.summary()}
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        rate, m, secs = cpu_baseline(ps, threads, max_pairs=args.cpu_sample)
+        rate, m, secs = cpu_baseline(ps, threads, max_pairs=args.cpu_sample, metric=metric, pen=pen,
+                                     mode=omode)
         line["cpu_baseline"] = {"value": rate, "unit": "pairs/s", "cores": threads, "kind": "port",
                                 "sample": f"first {m} pairs of the workload ({secs:.2f} s wall)"}
     if rank == 0:
@@ -305,12 +331,20 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--pairs", type=int, default=1_000_000)
-    ap.add_argument("--plain-pairs", type=int, default=2000)
-    ap.add_argument("--cpu-sample", type=int, default=1_000_000)
+    ap.add_argument("--workload", default="shortread", choices=sorted(WORKLOADS))
+    ap.add_argument("--pairs", type=int, default=None)
+    ap.add_argument("--plain-pairs", type=int, default=None)
+    ap.add_argument("--cpu-sample", type=int, default=None)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer and plain forms")
     args = ap.parse_args()
+    # Defaults per workload: pairs, plain per-call sample, CPU sample (about
+    # 10-30 s of CPU work on a 16-core host).
+    pairs, plain, cpu = {"shortread": (1_000_000, 2000, 1_000_000), "small": (10_000, 2000, 10_000),
+                         "longread": (20_000, 40, 160)}[args.workload]
+    args.pairs = pairs if args.pairs is None else args.pairs
+    args.plain_pairs = plain if args.plain_pairs is None else args.plain_pairs
+    args.cpu_sample = cpu if args.cpu_sample is None else args.cpu_sample
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -170,7 +170,9 @@ WFA_API const char* wfa_last_error_string(const wfa_aligner_t* h);
  * cigar_begin is relative to that slot; wfa_batch_align: the CIGARs are
  * packed densely in input order and cigar_begin is the offset into `cigars`). */
 typedef enum { WFA_SEQ_ASCII = 0, WFA_SEQ_PACKED2 = 1 } wfa_seq_format_t;
-typedef enum { WFA_SPAN_END2END = 0, WFA_SPAN_ENDSFREE = 1 } wfa_span_mode_t;
+/* Which reference call each pair follows: align_end2end, align_endsfree, or
+ * BiWFA (align_biwfa in alignment scope, align_biwfa_score in score scope). */
+typedef enum { WFA_SPAN_END2END = 0, WFA_SPAN_ENDSFREE = 1, WFA_SPAN_BIWFA = 2 } wfa_span_mode_t;
 
 typedef struct {
   int32_t score;        /* what align_* returns */

@@ -333,7 +333,11 @@ struct Wavefront {
   }
   void reallocate(int32_t n) {  // Wavefront::resize :283 (content lost)
     alloc = n;
-    mem.assign((size_t)n, POISON);
+#ifdef WFO_CHECKS
+    mem.assign((size_t)n, POISON);  // never-initialised cells are detectable
+#else
+    mem.resize((size_t)n);
+#endif
   }
   void init(int32_t min_lo, int32_t /*max_hi*/) {  // :307
     null = false; lo = 1; hi = -1; base_k = min_lo; init_min = 0; init_max = 0;

@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "../../wfa2lib-rs_b200/csrc/wfa_align.cuh"
+#include "../../wfa2lib-rs_b200/csrc/wfa_biwfa.cuh"
 #include "../../wfa2lib-rs_b200/csrc/wfa_params.h"
 
 using namespace wfab;
@@ -107,6 +108,111 @@ extern "C" int64_t wfa_emu_batch(int metric, const int32_t* pen6, int compute_al
       case kLinearClass: r = run_pair<kLinearClass>(P, i); break;
       case kAffineClass: r = run_pair<kAffineClass>(P, i); break;
       default: r = run_pair<kAffine2pClass>(P, i); break;
+    }
+    if (r) { results[i].status = kStatusRetry; ++retries; }
+  }
+  return retries;
+}
+
+template <int CLS, class S>
+static bool bi_lane(const AlignParams& P, const BiWorkspace& bw, int64_t i, S pat, S txt, S rpat, S rtxt) {
+  return biwfa_one<CLS, S>(P, bw, i, pat, txt, rpat, rtxt);
+}
+
+template <int CLS>
+static bool bi_pair(const AlignParams& P, int64_t i) {
+  constexpr int NC = CLS == kAffine2pClass ? 5 : CLS == kAffineClass ? 3 : 1;
+  const size_t ring = (size_t)P.scope * NC;
+  std::vector<WfD> d1(ring), d2(ring), d3(ring);
+  std::vector<int32_t> v1(ring * P.wmax, 0x5A5A5A5A), v2(ring * P.wmax, 0x5A5A5A5A), v3(ring * P.wmax, 0x5A5A5A5A);
+  std::vector<int4> hist((size_t)P.hist_scores, int4{0, -1, 0, 0});
+  std::vector<int32_t> harena((size_t)P.hist_words, 0x5A5A5A5A);
+  const int n = P.p_len[i], m = P.t_len[i];
+  std::vector<uint32_t> rev((size_t)(n + m) / 4 + 16, 0);
+  std::vector<uint8_t> tmp((size_t)2 * (n + m) + 16, 0);
+  BiWorkspace bw;
+  bw.fwd = Workspace{d1.data(), v1.data(), nullptr, nullptr};
+  bw.rev = Workspace{d2.data(), v2.data(), nullptr, nullptr};
+  bw.base = Workspace{d3.data(), v3.data(), hist.data(), harena.data()};
+  bw.rev_seq = reinterpret_cast<uint8_t*>(rev.data());
+  bw.cig_tmp = tmp.data();
+  auto go = [&]() -> bool {
+    if (P.format == WFA_SEQ_PACKED2) {
+      const uint32_t* w = reinterpret_cast<const uint32_t*>(P.seq);
+      SeqPacked sp{w + P.p_off[i], n, (n + 15) >> 4};
+      SeqPacked st{w + P.t_off[i], m, (m + 15) >> 4};
+      uint32_t* rp = rev.data();
+      uint32_t* rt = rp + ((n + 15) >> 4) + 1;
+      reverse_into(sp, rp);
+      reverse_into(st, rt);
+      Warp::sync();
+      SeqPacked rsp{rp, n, (n + 15) >> 4};
+      SeqPacked rst{rt, m, (m + 15) >> 4};
+      return bi_lane<CLS, SeqPacked>(P, bw, i, sp, st, rsp, rst);
+    }
+    SeqAscii sp{P.seq + P.p_off[i], n};
+    SeqAscii st{P.seq + P.t_off[i], m};
+    uint8_t* rp = bw.rev_seq;
+    uint8_t* rt = rp + n + 8;
+    reverse_into(sp, rp);
+    reverse_into(st, rt);
+    Warp::sync();
+    SeqAscii rsp{rp, n};
+    SeqAscii rst{rt, m};
+    return bi_lane<CLS, SeqAscii>(P, bw, i, sp, st, rsp, rst);
+  };
+#ifdef WFA_EMU_THREADS
+  EmuWarp warp;
+  g_emu_warp = &warp;
+  bool retry[32];
+  std::vector<std::thread> lanes;
+  for (int l = 0; l < 32; ++l)
+    lanes.emplace_back([&, l]() {
+      g_emu_lane = l;
+      retry[l] = go();
+    });
+  for (auto& t : lanes) t.join();
+  for (int l = 1; l < 32; ++l)
+    if (retry[l] != retry[0]) std::abort();
+  return retry[0];
+#else
+  return go();
+#endif
+}
+
+extern "C" int64_t wfa_emu_biwfa(int metric, const int32_t* pen6, int compute_alignment, int hkind,
+                                 const int32_t* hp3, int32_t max_steps, int format, const uint8_t* seq,
+                                 const int64_t* p_off, const int32_t* p_len, const int64_t* t_off,
+                                 const int32_t* t_len, int64_t num_pairs, const int64_t* cigar_off,
+                                 uint8_t* cigars, wfa_result_t* results, int32_t wmax,
+                                 int32_t hist_scores, int64_t hist_words) {
+  AlignParams P;
+  std::memset(&P, 0, sizeof P);
+  wfa_penalties_t u = {pen6[0], pen6[1], pen6[2], pen6[3], pen6[4], pen6[5]};
+  if (set_penalties(metric, &u, P) != WFA_OK) return -1;
+  P.hkind = hkind;
+  if (hp3) { P.hp0 = hp3[0]; P.hp1 = hp3[1]; P.hp2 = hp3[2]; }
+  P.compute_alignment = compute_alignment;
+  P.max_steps = max_steps;
+  P.format = format;
+  P.seq = seq;
+  P.p_off = p_off; P.p_len = p_len; P.t_off = t_off; P.t_len = t_len;
+  P.cigar_off = cigar_off;
+  P.cigars = cigars;
+  P.results = results;
+  P.num_pairs = num_pairs;
+  P.wmax = wmax;
+  P.hist_scores = hist_scores;
+  P.hist_words = hist_words;
+  int64_t retries = 0;
+  int cls = metric_class(metric);
+  for (int64_t i = 0; i < num_pairs; ++i) {
+    bool r;
+    switch (cls) {
+      case kEditClass: r = bi_pair<kEditClass>(P, i); break;
+      case kLinearClass: r = bi_pair<kLinearClass>(P, i); break;
+      case kAffineClass: r = bi_pair<kAffineClass>(P, i); break;
+      default: r = bi_pair<kAffine2pClass>(P, i); break;
     }
     if (r) { results[i].status = kStatusRetry; ++retries; }
   }

@@ -123,12 +123,14 @@ WFA_D int64_t lmax(int64_t a, int64_t b) { return a > b ? a : b; }
 // callers clamp to the sequence lengths (the reference's sentinels end every
 // extension at the end of either sequence, src/sequences.rs:12-19).
 // ---------------------------------------------------------------------------
-struct SeqPacked {  // 2-bit codes, 16 per word, word-aligned start
+struct SeqPacked {  // 2-bit codes, 16 per word; a view may start at base `off` of w
   static constexpr int UNITS = 16, BITS = 2;
   const uint32_t* w;
   int32_t len, nw;
+  int32_t off = 0;
   WFA_D uint32_t word(int i) const { return (i >= 0 && i < nw) ? w[i] : 0u; }
   WFA_D uint32_t fetch(int pos) const {
+    pos += off;
     if (pos < 0) {
       int s = -pos;
       return s >= 16 ? 0u : (word(0) << (2 * s));
@@ -252,6 +254,14 @@ struct PairAligner {
   int32_t p0, pf, t0, tf;
   bool endsfree;
   int32_t hist_lo, hist_hi;
+  // Heuristic (the aligner's own copy: BiWFA shifts the band per sub-problem).
+  int32_t hkind, hp0, hp1, hp2;
+  // History components (1: M only, for Singletrack / linear; NC: all, for the
+  // classic affine backtrace of the BiWFA base case) and whether all-null
+  // steps store null slots (BiWFA's overlap scans read every ring slot).
+  int32_t hist_nc;
+  bool keep_null_slots;
+  int32_t comp_end;  // component whose end diagonal terminates (BiWFA), else M
   int32_t cscore, cidx;  // current score and its ring index
   // Scores that are not multiples of gstep can have no wavefront: every input
   // score differs from them by a multiple of gstep (the gcd of the score
@@ -270,7 +280,7 @@ struct PairAligner {
   int32_t cg_score, cg_ev, cg_eh;
 
   WFA_D PairAligner(const AlignParams& p) : P(p) {}
-  WFA_D int hk() const { return GEN ? P.hkind : (int)WFA_HEURISTIC_NONE; }
+  WFA_D int hk() const { return GEN ? hkind : (int)WFA_HEURISTIC_NONE; }
   WFA_D bool ef() const { return GEN && endsfree; }
 
   // ---- slots --------------------------------------------------------------
@@ -312,19 +322,21 @@ struct PairAligner {
   // initialised range to the history arena for the backtrace.
   WFA_D void hist_commit(int s) {
     if (modular) return;
-    if (s >= P.hist_scores) { retry = true; return; }
-    WfD d = slot(CM, s);
-    int4 r;
-    r.x = d.a; r.y = d.b; r.z = 0; r.w = 0;
-    if (wf_present(d)) {
-      int64_t w = d.b >= d.a ? (int64_t)d.b - d.a + 1 : 0;
-      if (hused + w > P.hist_words) { retry = true; return; }
-      for (int64_t i = lane; i < w; i += WFA_WARP) ws.harena[hused + i] = d.vals[i];
-      r.z = (int32_t)hused;
-      r.w = 1;
-      hused += w;
+    if ((int64_t)(s + 1) * hist_nc > P.hist_scores) { retry = true; return; }
+    for (int c = 0; c < hist_nc; ++c) {
+      WfD d = slot(c, s);
+      int4 r;
+      r.x = d.a; r.y = d.b; r.z = 0; r.w = 0;
+      if (wf_present(d)) {
+        int64_t w = d.b >= d.a ? (int64_t)d.b - d.a + 1 : 0;
+        if (hused + w > P.hist_words) { retry = true; return; }
+        for (int64_t i = lane; i < w; i += WFA_WARP) ws.harena[hused + i] = d.vals[i];
+        r.z = (int32_t)hused;
+        r.w = 1;
+        hused += w;
+      }
+      if (lane == 0) ws.hist[(int64_t)s * hist_nc + c] = r;
     }
-    if (lane == 0) ws.hist[s] = r;
     // No sync: the history is read only by the backtrace, which starts with one.
   }
 
@@ -357,8 +369,8 @@ struct PairAligner {
 
   WFA_D void clamp_band(int& lo, int& hi) const {  // src/aligner.rs:3308-3317
     if (hk() == WFA_HEURISTIC_BANDED_STATIC || hk() == WFA_HEURISTIC_BANDED_ADAPTIVE) {
-      lo = imax(lo, P.hp0);
-      hi = imin(hi, P.hp1);
+      lo = imax(lo, hp0);
+      hi = imin(hi, hp1);
     }
   }
 
@@ -476,8 +488,8 @@ struct PairAligner {
     num_null_steps = 0;
     status = WFA_STATUS_OK;
     end_score = -1; end_k = kDiagNull; end_off = kOffsetNull;
-    hs.steps_wait = (hk() == WFA_HEURISTIC_WFADAPTIVE || hk() == WFA_HEURISTIC_BANDED_ADAPTIVE) ? P.hp2
-                    : (hk() == WFA_HEURISTIC_XDROP || hk() == WFA_HEURISTIC_ZDROP) ? P.hp1 : 0;
+    hs.steps_wait = (hk() == WFA_HEURISTIC_WFADAPTIVE || hk() == WFA_HEURISTIC_BANDED_ADAPTIVE) ? hp2
+                    : (hk() == WFA_HEURISTIC_XDROP || hk() == WFA_HEURISTIC_ZDROP) ? hp1 : 0;
     hs.max_sw_score = 0; hs.max_wf_score = 0; hs.max_sw_k = kDiagNull;
     hs.max_sw_off = kOffsetNull; hs.zdrop_last = 0;
     int lo0 = 0, hi0 = 0;
@@ -507,7 +519,7 @@ struct PairAligner {
     // initialised range only; outside it they already read as NULL).
     if (lane == 0) {
       int ks[4] = {prev.lo - 2, prev.lo - 1, prev.hi + 1, prev.hi + 2};
-      int4 hr = modular ? int4{0, -1, 0, 0} : ws.hist[s - 1];
+      int4 hr = modular ? int4{0, -1, 0, 0} : ws.hist[(int64_t)(s - 1) * hist_nc];
       for (int i = 0; i < 4; ++i) {
         if (ks[i] >= prev.a && ks[i] <= prev.b) prev.vals[ks[i] - prev.a] = kOffsetNull;
         if (hr.w && ks[i] >= hr.x && ks[i] <= hr.y) ws.harena[hr.z + ks[i] - hr.x] = kOffsetNull;
@@ -761,11 +773,11 @@ struct PairAligner {
       case WFA_HEURISTIC_WFADAPTIVE: {
         if (hs.steps_wait > 0) return false;
         int blo = d.lo, bhi = d.hi;
-        if (bhi - blo + 1 < P.hp0) return false;
+        if (bhi - blo + 1 < hp0) return false;
         int mn = INT_MAX;
         for (int k = blo + lane; k <= bhi; k += WFA_WARP) mn = imin(mn, dist(d, k));
         int min_d = imin(Warp::min(mn), imax(n, m));
-        int ak = m - n, thr = P.hp1;
+        int ak = m - n, thr = hp1;
         auto ok = [&](int k) { return (int32_t)((uint32_t)dist(d, k) - (uint32_t)min_d) <= thr; };
         int top = imin(ak, d.hi), nlo = d.lo;
         if (top > d.lo) {
@@ -783,18 +795,18 @@ struct PairAligner {
         }
         d.lo = nlo;
         d.hi = nhi;
-        hs.steps_wait = P.hp2;
+        hs.steps_wait = hp2;
         return false;
       }
       case WFA_HEURISTIC_BANDED_STATIC:
-        if (d.lo < P.hp0) d.lo = P.hp0;
-        if (d.hi > P.hp1) d.hi = P.hp1;
+        if (d.lo < hp0) d.lo = hp0;
+        if (d.hi > hp1) d.hi = hp1;
         return false;
       case WFA_HEURISTIC_BANDED_ADAPTIVE: {
         if (hs.steps_wait > 0) return false;
         int lo = d.lo, hi = d.hi, len = hi - lo + 1;
         if (len < 4) return false;
-        int maxlen = P.hp1 - P.hp0 + 1;
+        int maxlen = hp1 - hp0 + 1;
         if (len > maxlen) {
           int leeway = (len - maxlen) / 2, q = len / 4;
           int d0 = dist(d, lo), d1 = dist(d, lo + q), d2 = dist(d, lo + 2 * q), d3 = dist(d, hi);
@@ -804,7 +816,7 @@ struct PairAligner {
           d.lo = imax(nl, lo);
           d.hi = imin(nl + maxlen - 1, hi);
         }
-        hs.steps_wait = P.hp2;
+        hs.steps_wait = hp2;
         return false;
       }
       case WFA_HEURISTIC_XDROP: {
@@ -812,7 +824,7 @@ struct PairAligner {
         int cmax, ck, co;
         sw_max(d, score, cmax, ck, co);
         if (hs.max_sw_k != kDiagNull) {
-          int mx = hs.max_sw_score, xd = P.hp0;
+          int mx = hs.max_sw_score, xd = hp0;
           auto keep = [&](int k) {
             bool ok;
             int sw = sw_score(d, k, score, ok);
@@ -831,7 +843,7 @@ struct PairAligner {
           hs.max_sw_score = cmax;
           hs.max_sw_k = ck;
         }
-        hs.steps_wait = P.hp1;
+        hs.steps_wait = hp1;
         return false;
       }
       case WFA_HEURISTIC_ZDROP: {
@@ -841,12 +853,12 @@ struct PairAligner {
         if (hs.max_sw_k == kDiagNull || cmax > hs.max_sw_score) {
           hs.max_sw_score = cmax; hs.max_wf_score = score; hs.max_sw_k = ck;
           hs.max_sw_off = co; hs.zdrop_last = score;
-        } else if (hs.max_sw_score - cmax <= P.hp0) {
+        } else if (hs.max_sw_score - cmax <= hp0) {
           hs.zdrop_last = score;
         } else if (score - hs.zdrop_last >= scope - 1) {
           return true;
         }
-        hs.steps_wait = P.hp1;
+        hs.steps_wait = hp1;
         return false;
       }
       default:
@@ -857,7 +869,7 @@ struct PairAligner {
   // apply_heuristic_cutoff, src/aligner.rs:1644-1766.  True on a Z-drop.
   WFA_D bool apply_heuristic(int score) {
     WfD d = slot(CM, score);
-    if (hk() == WFA_HEURISTIC_BANDED_STATIC && d.lo >= P.hp0 && d.hi <= P.hp1) return false;
+    if (hk() == WFA_HEURISTIC_BANDED_STATIC && d.lo >= hp0 && d.hi <= hp1) return false;
     int lo_base = d.lo, hi_base = d.hi;
     bool z = heuristic_cutoff(d, score);
     if (z) {
@@ -914,6 +926,176 @@ struct PairAligner {
     return false;
   }
 
+  // ---- BiWFA sub-aligner steps ---------------------------------------------------
+  // init_alignment_component, src/aligner.rs:3205-3265: a single cell (k = 0,
+  // offset 0) in component `comp` at score 0.
+  WFA_D void init_alignment_component(int comp) {
+    cscore = 0;
+    cidx = 0;
+    gstep = score_step_gcd();
+    gphase = 0;
+    for (int i = lane; i < scope * NC; i += WFA_WARP) ws.ring[i] = wf_none();
+    Warp::sync();
+    hist_lo = -(n + scope + 2);
+    hist_hi = m + scope + 2;
+    num_null_steps = 0;
+    status = WFA_STATUS_OK;
+    end_score = 0; end_k = 0; end_off = 0;
+    hs.steps_wait = (hk() == WFA_HEURISTIC_WFADAPTIVE || hk() == WFA_HEURISTIC_BANDED_ADAPTIVE) ? hp2
+                    : (hk() == WFA_HEURISTIC_XDROP || hk() == WFA_HEURISTIC_ZDROP) ? hp1 : 0;
+    hs.max_sw_score = 0; hs.max_wf_score = 0; hs.max_sw_k = kDiagNull;
+    hs.max_sw_off = kOffsetNull; hs.zdrop_last = 0;
+    hused = 0;
+    int32_t* v = alloc(comp, 0, 0, 0);
+    if (retry) return;
+    if (lane == 0) v[0] = 0;
+    WfD d;
+    d.vals = v; d.lo = 0; d.hi = 0; d.a = 0; d.b = 0; d.flags = kPresent; d.pad = 0;
+    put(comp, 0, d);
+  }
+
+  // One step of the score loop for a BiWFA sub-aligner: the compute step at
+  // score s (s > 0), honouring the all-null scores, with null slots stored.
+  WFA_D void bi_compute(int s) {
+    advance();
+    gphase = gphase + 1 == gstep ? 0 : gphase + 1;
+    if (gphase != 0) {
+      ++num_null_steps;
+      for (int c = 0; c < NC; ++c) put_ns(c, s, wf_none());
+      Warp::sync();
+    } else {
+      compute_step(s);
+    }
+  }
+
+  // extend_biwfa_step, src/aligner.rs:3516-3554: extend M (with the maximum
+  // antidiagonal when `max`), then the end test on `comp_end` and the
+  // heuristic.  Returns true when done; max_ak as the reference reports it.
+  WFA_D bool bi_extend(int score, bool max, int& max_ak) {
+    max_ak = 0;
+    WfD d = slot(CM, score);
+    if (!wf_present(d)) {
+      if (num_null_steps > scope) { status = WFA_STATUS_END_UNREACHABLE; return true; }
+      return false;
+    }
+    int ak = 0;
+    for (int k = d.lo + lane; k <= d.hi; k += WFA_WARP) {
+      int32_t off = d.vals[k - d.a];
+      if (off >= 0) {
+        int v = off - k, h = off;
+        int R = imin(n - v, m - h);
+        if (R > 0) {
+          off += lcp_fwd(pat, v, txt, h, R);
+          d.vals[k - d.a] = off;
+        }
+        if (max) ak = imax(ak, 2 * off - k);
+      }
+    }
+    Warp::sync();
+    if (max) ak = Warp::max(ak);
+    // check_component_termination, src/aligner.rs:3268-3302
+    WfD e = slot(comp_end, score);
+    int kend = m - n;
+    if (wf_present(e) && kend >= e.lo && kend <= e.hi && rd(e, kend) >= m) {
+      end_score = score; end_k = kend; end_off = m;
+      status = WFA_STATUS_END_REACHED;
+      return true;
+    }
+    if (hk() != WFA_HEURISTIC_NONE && apply_heuristic(score)) {
+      status = WFA_STATUS_END_UNREACHABLE;
+      return true;
+    }
+    max_ak = ak;
+    return false;
+  }
+
+  // backtrace_affine_c, src/backtrace.rs:492-635: the classic backtrace over
+  // every component's history (BiWFA base case), ending in `comp_end`.
+  WFA_D void backtrace_affine_classic(int ascore, int k, int offset, int cend) {
+    cg_end = cg_cap;
+    cg_begin = cg_cap - 1;
+    int matrix = cend;
+    int score = ascore, v = offset - k, h = offset;
+    if (cend == CM) {
+      run('D', imax(n - v, 0));
+      run('I', imax(m - h, 0));
+    }
+    constexpr int64_t I1O = 1, I1E = 2, I2O = 3, I2E = 4, D1O = 5, D1E = 6, D2O = 7, D2E = 8, MM = 9;
+    while (v > 0 && h > 0 && score > 0 && status != WFA_STATUS_OOM) {
+      int mis = score - P.mismatch;
+      int go1 = score - P.o1 - P.e1, go2 = TWO ? score - P.o2 - P.e2 : -1;
+      int ge1 = score - P.e1, ge2 = TWO ? score - P.e2 : -1;
+      int64_t mx;
+      if (matrix == CM) {
+        int64_t misms = bt_pack(mis, k, 0, 1, MM, false, CM);
+        int64_t mi1 = lmax(bt_pack(go1, k, -1, 1, I1O, true, CM), bt_pack(ge1, k, -1, 1, I1E, true, CI1));
+        int64_t md1 = lmax(bt_pack(go1, k, 1, 0, D1O, false, CM), bt_pack(ge1, k, 1, 0, D1E, false, CD1));
+        if (TWO) {
+          int64_t mi2 = lmax(bt_pack(go2, k, -1, 1, I2O, true, CM), bt_pack(ge2, k, -1, 1, I2E, true, CI2));
+          int64_t md2 = lmax(bt_pack(go2, k, 1, 0, D2O, false, CM), bt_pack(ge2, k, 1, 0, D2E, false, CD2));
+          mx = lmax(misms, lmax(lmax(mi1, mi2), lmax(md1, md2)));
+        } else {
+          mx = lmax(misms, lmax(mi1, md1));
+        }
+      } else if (matrix == CI1) {
+        mx = lmax(bt_pack(go1, k, -1, 1, I1O, true, CM), bt_pack(ge1, k, -1, 1, I1E, true, CI1));
+      } else if (matrix == CD1) {
+        mx = lmax(bt_pack(go1, k, 1, 0, D1O, false, CM), bt_pack(ge1, k, 1, 0, D1E, false, CD1));
+      } else if (matrix == CI2) {
+        mx = lmax(bt_pack(go2, k, -1, 1, I2O, true, CM), bt_pack(ge2, k, -1, 1, I2E, true, CI2));
+      } else {
+        mx = lmax(bt_pack(go2, k, 1, 0, D2O, false, CM), bt_pack(ge2, k, 1, 0, D2E, false, CD2));
+      }
+      if (mx < 0) break;
+      if (matrix == CM) {
+        int moff = (int)(mx >> 4);
+        matches(offset - moff);
+        offset = moff;
+        v = offset - k; h = offset;
+        if (v <= 0 || h <= 0) break;
+      }
+      int64_t t = mx & 0xF;
+      if (t == MM) { score = mis; matrix = CM; }
+      else if (t == I1O || t == D1O) { score = go1; matrix = CM; }
+      else if (t == I2O || t == D2O) { score = go2; matrix = CM; }
+      else if (t == I1E) { score = ge1; matrix = CI1; }
+      else if (t == I2E) { score = ge2; matrix = CI2; }
+      else if (t == D1E) { score = ge1; matrix = CD1; }
+      else { score = ge2; matrix = CD2; }
+      if (t == MM) { push('X'); offset -= 1; }
+      else if (t == I1O || t == I1E || t == I2O || t == I2E) { push('I'); k -= 1; offset -= 1; }
+      else { push('D'); k += 1; }
+      v = offset - k; h = offset;
+    }
+    if (matrix == CM) {
+      if (v > 0 && h > 0) {
+        int nm = imin(v, h);
+        matches(nm);
+        v -= nm; h -= nm;
+      }
+      run('D', v);
+      run('I', h);
+    }
+    cg_begin += 1;
+    cg_score = ascore;
+    Warp::sync();
+  }
+
+  // backtrace_components (src/aligner.rs:1489-1535): the BiWFA base case's.
+  WFA_D void backtrace_components(int score, int k, int offset, int cend) {
+    Warp::sync();
+    if (AFF) {
+      backtrace_affine_classic(score, k, offset, cend);
+    } else {
+      cg_end = cg_cap;
+      cg_begin = cg_cap - 1;
+      backtrace_linear(score, k, offset);
+      cg_begin += 1;
+      cg_score = score;
+      Warp::sync();
+    }
+  }
+
   // ---- CIGAR output ------------------------------------------------------------
   WFA_D void run(uint8_t op, int cnt) {  // write_ops, src/backtrace.rs:689-698
     if (cnt <= 0) return;
@@ -932,7 +1114,7 @@ struct PairAligner {
   // false, as outside the initialised range).
   WFA_D bool m_cell(int score, int k, int32_t& out) const {
     if (score < 0 || !has_slot(score)) return false;
-    int4 r = ws.hist[score];
+    int4 r = ws.hist[(int64_t)score * hist_nc];
     if (!r.w || k < r.x || k > r.y) return false;
     out = ws.harena[r.z + (k - r.x)];
     return true;
@@ -1004,10 +1186,13 @@ struct PairAligner {
   }
 
   // backtrace_linear, src/backtrace.rs:132-258
-  WFA_D int64_t bt_pack(int score, int k, int dk, int add, int64_t type, bool ins) const {
-    // bt_misms (dk 0), bt_ins1_open (dk -1, cell k-1), bt_del1_open (dk +1)
+  // Backtrace lookups of src/backtrace.rs:44-330 (bt_misms: dk 0; bt_ins*: dk
+  // -1, cell k-1; bt_del*: dk +1, cell k+1) on component c of the history:
+  // the packed (offset << 4 | type), or OFFSET_NULL outside the initialised
+  // range / for a missing wavefront.
+  WFA_D int64_t bt_pack(int score, int k, int dk, int add, int64_t type, bool ins, int c = CM) const {
     if (score < 0) return kOffsetNull;
-    int4 r = ws.hist[score];
+    int4 r = ws.hist[(int64_t)score * hist_nc + c];
     if (!r.w) return kOffsetNull;
     bool inside;
     if (dk == 0) inside = r.x <= k && k <= r.y;
@@ -1220,8 +1405,9 @@ struct PairAligner {
           done = num_null_steps > scope;
           if (done) status = WFA_STATUS_END_UNREACHABLE;
           if (!modular) {
-            if (score >= P.hist_scores) { retry = true; break; }
-            if (lane == 0) ws.hist[score] = int4{1, 0, 0, 0};
+            if ((int64_t)(score + 1) * hist_nc > P.hist_scores) { retry = true; break; }
+            if (lane == 0)
+              for (int c = 0; c < hist_nc; ++c) ws.hist[(int64_t)score * hist_nc + c] = int4{1, 0, 0, 0};
           }
         } else {
           done = extend_step(score);
@@ -1296,6 +1482,10 @@ WFA_D bool align_one(const AlignParams& P, const Workspace& ws, int64_t pair, S 
   A.modular = P.compute_alignment == 0;
   A.cap = A.modular ? INT_MAX : imax(A.dims_num(1000, 1000), A.dims_num(A.n, A.m));
   A.endsfree = P.span == WFA_SPAN_ENDSFREE;
+  A.hkind = P.hkind; A.hp0 = P.hp0; A.hp1 = P.hp1; A.hp2 = P.hp2;
+  A.hist_nc = 1;
+  A.keep_null_slots = false;
+  A.comp_end = CM;
   if (P.extension) { A.p0 = 0; A.pf = A.n; A.t0 = 0; A.tf = A.m; }
   else if (A.endsfree) { A.p0 = P.p0; A.pf = P.pf; A.t0 = P.t0; A.tf = P.tf; }
   else { A.p0 = A.pf = A.t0 = A.tf = 0; }

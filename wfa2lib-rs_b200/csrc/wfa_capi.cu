@@ -148,11 +148,10 @@ __global__ void max_lengths(const int32_t* pl, const int32_t* tl, int64_t n, int
 // Configuration checks
 // ---------------------------------------------------------------------------
 static int check_supported(wfa_aligner_t* h, bool biwfa) {
-  if (biwfa) return fail(h, WFA_ERR_UNSUPPORTED, "BiWFA is not available in this build");
-  if (h->scope == WFA_SCOPE_ALIGNMENT && h->memory_mode != WFA_MEMORY_HIGH)
+  if (!biwfa && h->scope == WFA_SCOPE_ALIGNMENT && h->memory_mode != WFA_MEMORY_HIGH)
     return fail(h, WFA_ERR_UNSUPPORTED,
                 "med/low memory (piggyback backtrace) is not available in this build");
-  if (h->compat == WFA_COMPAT_CORRECTED && h->pen.match < 0 && h->span == WFA_SPAN_ENDSFREE)
+  if (!biwfa && h->compat == WFA_COMPAT_CORRECTED && h->pen.match < 0 && h->span == WFA_SPAN_ENDSFREE)
     return fail(h, WFA_ERR_UNSUPPORTED, "Compat::Corrected ends-free with a match reward");
   if (h->pen.scope > 1024) return fail(h, WFA_ERR_UNSUPPORTED, "max_score_scope above 1024");
   return WFA_OK;
@@ -160,7 +159,7 @@ static int check_supported(wfa_aligner_t* h, bool biwfa) {
 
 static void fill_params(const wfa_aligner_t* h, const wfa_batch_t* b, AlignParams& P) {
   P = h->pen;
-  P.span = b->span;
+  P.span = b->span == WFA_SPAN_BIWFA ? WFA_SPAN_END2END : b->span;
   P.extension = b->span == WFA_SPAN_ENDSFREE ? h->extension : 0;
   P.p0 = h->p0; P.pf = h->pf; P.t0 = h->t0; P.tf = h->tf;
   P.hkind = h->hkind; P.hp0 = h->hp0; P.hp1 = h->hp1; P.hp2 = h->hp2;
@@ -303,6 +302,84 @@ static int run_device_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t
   return WFA_OK;
 }
 
+// BiWFA batch: the same round structure as run_device_batch with the BiWFA
+// kernel and its workspace layout.
+static int run_biwfa_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* d_results,
+                           uint8_t* d_cigars, cudaStream_t st, int32_t max_len_sum) {
+  AlignParams P;
+  fill_params(h, b, P);
+  P.results = d_results;
+  P.cigars = d_cigars;
+  if (P.compute_alignment && (!d_cigars || !b->cigar_off))
+    return fail(h, WFA_ERR_ARGUMENT, "CIGAR output buffers are required in alignment scope");
+  const int cls = metric_class(P.metric);
+  const int nc = metric_components(P.metric);
+  P.max_len_sum = max_len_sum;
+  ScratchCfg cfg;
+  cfg.wmax = std::max(8, std::min(max_len_sum + 3, 1024));
+  cfg.hist_scores = 1024 * nc;
+  cfg.hist_words = 65536;
+  const size_t smem = (size_t)kWarpsPerBlock * 3 * P.scope * nc * kDescBytes;
+  if (smem > 200 * 1024) return fail(h, WFA_ERR_UNSUPPORTED, "wavefront ring too large");
+  int64_t todo = b->num_pairs;
+  const int64_t* list = nullptr;
+  h->last_kernel_ms = 0.0;
+  CUDA_TRY(h, h->counters.ensure(64), "counters");
+  P.work_counter = h->counters.as<unsigned long long>();
+  P.retry_count = reinterpret_cast<int32_t*>(P.work_counter + 1);
+  for (int round = 0; todo > 0; ++round) {
+    if (round > 8) return fail(h, WFA_ERR_OOM, "alignment needs more scratch than available");
+    const BiLayout L = bi_layout(P.scope, nc, cfg.wmax, cfg.hist_scores, cfg.hist_words, max_len_sum);
+    int64_t max_warps = (int64_t)h->num_sms * 2 * kWarpsPerBlock;
+    int64_t warps = std::max<int64_t>(std::min<int64_t>(max_warps, todo), 1);
+    while (warps > 1 && (size_t)warps * L.words * 4 > kScratchBudget) warps /= 2;
+    int blocks = (int)((warps + kWarpsPerBlock - 1) / kWarpsPerBlock);
+    CUDA_TRY(h, h->scratch.ensure((size_t)blocks * kWarpsPerBlock * L.words * 4), "scratch");
+    P.scratch = h->scratch.as<int32_t>();
+    P.warp_words = L.words;
+    P.wmax = cfg.wmax;
+    P.hist_scores = cfg.hist_scores;
+    P.hist_words = cfg.hist_words;
+    P.pair_list = list;
+    P.num_pairs = todo;
+    CUDA_TRY(h, cudaMemsetAsync(P.work_counter, 0, 16, st), "memset");
+    CUDA_TRY(h, cudaEventRecord(h->ev0, st), "event");
+    CUDA_TRY(h, launch_biwfa(P, cls, blocks, smem, st), "kernel launch");
+    CUDA_TRY(h, cudaEventRecord(h->ev1, st), "event");
+    h->launches++;
+    int32_t retries = 0;
+    CUDA_TRY(h, cudaMemcpyAsync(&retries, P.retry_count, 4, cudaMemcpyDeviceToHost, st), "retry count");
+    CUDA_TRY(h, cudaStreamSynchronize(st), "kernel");
+    float ms = 0.f;
+    CUDA_TRY(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1), "event");
+    h->last_kernel_ms += ms;
+    if (retries == 0) break;
+    CUDA_TRY(h, h->pairlist.ensure(2 * (size_t)std::max<int64_t>(b->num_pairs, 1) * 8), "pair list");
+    int64_t* half0 = h->pairlist.as<int64_t>();
+    int64_t* half1 = half0 + b->num_pairs;
+    int64_t* out = (list == half0) ? half1 : half0;
+    CUDA_TRY(h, cudaMemsetAsync(P.retry_count, 0, 4, st), "memset");
+    collect_retries<<<(unsigned)((todo + 255) / 256), 256, 0, st>>>(d_results, list, todo, out, P.retry_count);
+    h->launches++;
+    CUDA_TRY(h, cudaGetLastError(), "collect retries");
+    int32_t got = 0;
+    CUDA_TRY(h, cudaMemcpyAsync(&got, P.retry_count, 4, cudaMemcpyDeviceToHost, st), "retry count");
+    CUDA_TRY(h, cudaStreamSynchronize(st), "collect retries");
+    list = out;
+    todo = got;
+    cfg.wmax = std::min(max_len_sum + 3, cfg.wmax * 4);
+    cfg.hist_scores *= 4;
+    cfg.hist_words *= 4;
+  }
+  return WFA_OK;
+}
+
+static int run_batch_kind(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* d_results,
+                          uint8_t* d_cigars, cudaStream_t st, int32_t max_len_sum) {
+  if (b->span == WFA_SPAN_BIWFA) return run_biwfa_batch(h, b, d_results, d_cigars, st, max_len_sum);
+  return run_device_batch(h, b, d_results, d_cigars, st, max_len_sum);
+}
+
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
@@ -428,7 +505,7 @@ static int32_t align_plain(wfa_aligner_t* h, const uint8_t* p, int32_t n, const 
   h->cigar.clear();
   int saved_span = h->span;
   h->span = span;
-  int r = check_supported(h, false);
+  int r = check_supported(h, span == WFA_SPAN_BIWFA);
   h->span = saved_span;
   if (r != WFA_OK) return r;
   cudaSetDevice(h->device);
@@ -481,8 +558,12 @@ static int32_t align_plain(wfa_aligner_t* h, const uint8_t* p, int32_t n, const 
   P.results = h->results.as<wfa_result_t>();
   P.cigars = h->cigars.as<uint8_t>();
   const bool aln = P.compute_alignment != 0;
-  Round rd = first_round(P, metric_components(P.metric), n + m);
-  r = launch_round(h, P, rd, 1, nullptr, st);
+  if (span == WFA_SPAN_BIWFA) {
+    r = run_biwfa_batch(h, &b, P.results, P.cigars, st, n + m);
+  } else {
+    Round rd = first_round(P, metric_components(P.metric), n + m);
+    r = launch_round(h, P, rd, 1, nullptr, st);
+  }
   if (r != WFA_OK) return r;
   wfa_result_t res;
   uint8_t* hbuf = h->pinned;  // reuse staging for the way back
@@ -539,13 +620,18 @@ int32_t wfa_align_endsfree(wfa_aligner_t* h, const uint8_t* p, int32_t n, const 
 int32_t wfa_align_packed2bits(wfa_aligner_t* h, const uint8_t* p, int32_t n, const uint8_t* t, int32_t m) {
   return align_plain(h, p, n, t, m, WFA_SPAN_END2END, true);
 }
-int32_t wfa_align_biwfa(wfa_aligner_t* h, const uint8_t*, int32_t, const uint8_t*, int32_t) {
+int32_t wfa_align_biwfa(wfa_aligner_t* h, const uint8_t* p, int32_t n, const uint8_t* t, int32_t m) {
   if (!h) return WFA_ERR_ARGUMENT;
-  return check_supported(h, true);
+  h->scope = WFA_SCOPE_ALIGNMENT;  // align_biwfa sets ComputeAlignment (src/aligner.rs:2565)
+  return align_plain(h, p, n, t, m, WFA_SPAN_BIWFA, false);
 }
-int32_t wfa_align_biwfa_score(wfa_aligner_t* h, const uint8_t*, int32_t, const uint8_t*, int32_t) {
+int32_t wfa_align_biwfa_score(wfa_aligner_t* h, const uint8_t* p, int32_t n, const uint8_t* t, int32_t m) {
   if (!h) return WFA_ERR_ARGUMENT;
-  return check_supported(h, true);
+  int saved = h->scope;
+  h->scope = WFA_SCOPE_SCORE;
+  int32_t r = align_plain(h, p, n, t, m, WFA_SPAN_BIWFA, false);
+  h->scope = saved;
+  return r;
 }
 int32_t wfa_align_lambda(wfa_aligner_t* h, int (*)(int32_t, int32_t, void*), void*, int32_t, int32_t) {
   return fail(h, WFA_ERR_UNSUPPORTED, "lambda sequences need a host callback per comparison");
@@ -578,11 +664,12 @@ static int batch_common(wfa_aligner_t* h, const wfa_batch_t* b) {
   if (!h || !b || b->num_pairs < 0 || !b->seq || !b->p_off || !b->p_len || !b->t_off || !b->t_len)
     return WFA_ERR_ARGUMENT;
   if (b->format != WFA_SEQ_ASCII && b->format != WFA_SEQ_PACKED2) return WFA_ERR_ARGUMENT;
-  if (b->span != WFA_SPAN_END2END && b->span != WFA_SPAN_ENDSFREE) return WFA_ERR_ARGUMENT;
+  if (b->span != WFA_SPAN_END2END && b->span != WFA_SPAN_ENDSFREE && b->span != WFA_SPAN_BIWFA)
+    return WFA_ERR_ARGUMENT;
   h->last_err = WFA_OK;
   int saved = h->span;
   h->span = b->span;
-  int r = check_supported(h, false);
+  int r = check_supported(h, b->span == WFA_SPAN_BIWFA);
   h->span = saved;
   return r;
 }
@@ -603,7 +690,68 @@ int wfa_batch_align_device(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t*
   int32_t mx = 0;
   CUDA_TRY(h, cudaMemcpyAsync(&mx, d_max, 4, cudaMemcpyDeviceToHost, st), "D2H");
   CUDA_TRY(h, cudaStreamSynchronize(st), "max lengths");
-  return run_device_batch(h, b, results, cigars, st, mx);
+  return run_batch_kind(h, b, results, cigars, st, mx);
+}
+
+// Host-buffer batch without pipelining (BiWFA): copy in, align, dense CIGARs out.
+static int batch_align_simple(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* results,
+                              uint8_t* cigars) {
+  const int64_t n = b->num_pairs;
+  const bool aln = h->scope == WFA_SCOPE_ALIGNMENT;
+  cudaStream_t st = h->stream;
+  int32_t mx = 0;
+  int64_t slot_total = 0;
+  std::vector<int64_t> slot_off(aln ? (size_t)n : 0);
+  for (int64_t i = 0; i < n; ++i) {
+    int32_t s = b->p_len[i] + b->t_len[i];
+    mx = std::max(mx, s);
+    if (aln) { slot_off[(size_t)i] = slot_total; slot_total += 2 * (int64_t)s + 1; }
+  }
+  size_t seq_bytes = ((size_t)b->seq_bytes + 15) & ~(size_t)15;
+  CUDA_TRY(h, h->seq.ensure(seq_bytes + 16), "seq");
+  CUDA_TRY(h, h->poff.ensure((size_t)n * 8), "p_off");
+  CUDA_TRY(h, h->toff.ensure((size_t)n * 8), "t_off");
+  CUDA_TRY(h, h->plen.ensure((size_t)n * 4), "p_len");
+  CUDA_TRY(h, h->tlen.ensure((size_t)n * 4), "t_len");
+  CUDA_TRY(h, h->results.ensure((size_t)n * sizeof(wfa_result_t)), "results");
+  CUDA_TRY(h, cudaMemcpyAsync(h->seq.p, b->seq, (size_t)b->seq_bytes, cudaMemcpyHostToDevice, st), "H2D");
+  CUDA_TRY(h, cudaMemcpyAsync(h->poff.p, b->p_off, (size_t)n * 8, cudaMemcpyHostToDevice, st), "H2D");
+  CUDA_TRY(h, cudaMemcpyAsync(h->toff.p, b->t_off, (size_t)n * 8, cudaMemcpyHostToDevice, st), "H2D");
+  CUDA_TRY(h, cudaMemcpyAsync(h->plen.p, b->p_len, (size_t)n * 4, cudaMemcpyHostToDevice, st), "H2D");
+  CUDA_TRY(h, cudaMemcpyAsync(h->tlen.p, b->t_len, (size_t)n * 4, cudaMemcpyHostToDevice, st), "H2D");
+  wfa_batch_t d = *b;
+  d.seq = h->seq.p;
+  d.seq_bytes = (int64_t)seq_bytes;
+  d.p_off = h->poff.as<int64_t>(); d.t_off = h->toff.as<int64_t>();
+  d.p_len = h->plen.as<int32_t>(); d.t_len = h->tlen.as<int32_t>();
+  d.cigar_off = nullptr;
+  if (aln) {
+    CUDA_TRY(h, h->coff.ensure((size_t)n * 8), "cigar_off");
+    CUDA_TRY(h, h->cigars.ensure((size_t)slot_total + 16), "cigar slots");
+    CUDA_TRY(h, cudaMemcpyAsync(h->coff.p, slot_off.data(), (size_t)n * 8, cudaMemcpyHostToDevice, st), "H2D");
+    d.cigar_off = h->coff.as<int64_t>();
+    d.cigar_bytes = slot_total;
+  }
+  int r = run_batch_kind(h, &d, h->results.as<wfa_result_t>(), aln ? h->cigars.as<uint8_t>() : nullptr, st, mx);
+  if (r != WFA_OK) return r;
+  CUDA_TRY(h, cudaMemcpyAsync(results, h->results.p, (size_t)n * sizeof(wfa_result_t), cudaMemcpyDeviceToHost, st), "D2H");
+  CUDA_TRY(h, cudaStreamSynchronize(st), "D2H");
+  if (!aln) return WFA_OK;
+  std::vector<int64_t> dst((size_t)n);
+  int64_t total = 0;
+  for (int64_t i = 0; i < n; ++i) { dst[(size_t)i] = total; total += results[i].cigar_length; }
+  CUDA_TRY(h, h->dense.ensure((size_t)total + 16), "dense cigars");
+  CUDA_TRY(h, h->pairlist.ensure((size_t)n * 8), "offsets");
+  CUDA_TRY(h, cudaMemcpyAsync(h->pairlist.p, dst.data(), (size_t)n * 8, cudaMemcpyHostToDevice, st), "H2D");
+  compact_cigars<<<(unsigned)((n * 32 + 255) / 256), 256, 0, st>>>(
+      h->results.as<wfa_result_t>(), d.cigar_off, h->cigars.as<uint8_t>(), h->pairlist.as<int64_t>(),
+      h->dense.as<uint8_t>(), n);
+  h->launches++;
+  CUDA_TRY(h, cudaGetLastError(), "compact cigars");
+  CUDA_TRY(h, cudaMemcpyAsync(cigars, h->dense.p, (size_t)total, cudaMemcpyDeviceToHost, st), "D2H");
+  CUDA_TRY(h, cudaStreamSynchronize(st), "D2H");
+  for (int64_t i = 0; i < n; ++i) results[i].cigar_begin = (int32_t)dst[(size_t)i];
+  return WFA_OK;
 }
 
 // Host-buffer batch, pipelined in chunks of pairs: while chunk c aligns on
@@ -621,6 +769,7 @@ int wfa_batch_align(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* result
   const bool aln = h->scope == WFA_SCOPE_ALIGNMENT;
   if (aln && !cigars) return WFA_ERR_ARGUMENT;
   cudaSetDevice(h->device);
+  if (b->span == WFA_SPAN_BIWFA) return batch_align_simple(h, b, results, cigars);
   cudaStream_t sc = h->stream, si = h->s_in, so = h->s_out;
   const int64_t chunk = std::max<int64_t>(65536, std::min<int64_t>(262144, (n + 3) / 4));
   const int64_t nchunks = (n + chunk - 1) / chunk;

@@ -31,7 +31,32 @@ inline SmemLayout smem_layout(int scope, int nc, int ring_wmax, int seq_words) {
   return L;
 }
 
+// BiWFA per-warp scratch slice (int32 word offsets).  seq_len_sum is the
+// longest n + m of the launch (sizes the reversed sequences and the base CIGAR).
+struct BiLayout {
+  int64_t ring_f, ring_r, ring_b, hist, harena, rev, cig, words;
+};
+#if defined(__CUDACC__)
+__host__ __device__
+#endif
+inline BiLayout bi_layout(int scope, int nc, int wmax, int hist_scores, int64_t hist_words,
+                          int seq_len_sum) {
+  BiLayout L;
+  const int64_t ring = ((int64_t)scope * nc * wmax + 3) & ~(int64_t)3;
+  L.ring_f = 0;
+  L.ring_r = L.ring_f + ring;
+  L.ring_b = L.ring_r + ring;
+  L.hist = L.ring_b + ring;
+  L.harena = L.hist + (int64_t)hist_scores * 4;
+  L.rev = L.harena + ((hist_words + 3) & ~(int64_t)3);
+  L.cig = L.rev + ((int64_t)seq_len_sum + 48) / 4 + 8;
+  L.words = L.cig + ((int64_t)2 * seq_len_sum + 16) / 4 + 8;
+  L.words = (L.words + 63) & ~(int64_t)63;
+  return L;
+}
+
 bool needs_general(const AlignParams& P);
+cudaError_t launch_biwfa(const AlignParams& P, int cls, int blocks, size_t smem, cudaStream_t st);
 cudaError_t launch_unialign(const AlignParams& P, int metric_class, int blocks, size_t smem,
                             cudaStream_t st);
 int occupancy_blocks_per_sm(const AlignParams& P, int metric_class, size_t smem);

@@ -134,3 +134,39 @@ def pack2bits(ps):
     shifts = (2 * np.arange(16, dtype=np.uint32))
     packed = np.bitwise_or.reduce(q << shifts, axis=1).astype(np.uint32)
     return packed, woff[0::2].astype(np.int64), woff[1::2].astype(np.int64)
+
+
+def config3(num=20_000, seed=SEED_BASE + 3):
+    """Uneven long reads: n log-uniform in [1 kbp, 20 kbp], per-pair edit rate
+    U[0.05, 0.15]; 40% substitutions, 30% insertions and 30% deletions, indel
+    lengths geometric with mean 3.  (Gap-affine 2-piece, BiWFA.)"""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    p_len = np.exp(rng.uniform(np.log(1000), np.log(20000), num)).astype(np.int32)
+    rate = rng.uniform(0.05, 0.15, num)
+    total = int(p_len.sum())
+    patterns = ACGT[rng.integers(0, 4, total)]
+    pair_of = np.repeat(np.arange(num), p_len)
+    starts = np.concatenate([[0], np.cumsum(p_len)[:-1]])
+    pair_end = (starts + p_len)[pair_of]
+    u = rng.random(total)
+    edit = u < rate[pair_of]
+    kind = rng.random(total)
+    sub = edit & (kind < 0.4)
+    ins = edit & (kind >= 0.4) & (kind < 0.7)
+    dele = edit & (kind >= 0.7)
+    glen = rng.geometric(1.0 / 3.0, total)
+    pos = np.arange(total)
+    # A deletion at i removes i .. i+len-1 (within its pair).
+    end = np.where(dele, np.minimum(pos + glen, pair_end), -1)
+    deleted = np.maximum.accumulate(end) > pos
+    keep = ~deleted
+    counts = np.where(keep, np.where(ins, glen + 1, 1), 0).astype(np.int64)
+    src = np.repeat(pos, counts)
+    out = patterns[src].copy()
+    last = np.ones(len(src), dtype=bool)
+    last[:-1] = src[1:] != src[:-1]
+    rnd = ACGT[rng.integers(0, 4, len(src))]
+    repl = (ins[src] & ~last) | sub[src]
+    out[repl] = rnd[repl]
+    t_len = np.bincount(pair_of, weights=counts, minlength=num).astype(np.int32)
+    return _interleave(patterns, p_len, out, t_len)
