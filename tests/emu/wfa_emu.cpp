@@ -124,7 +124,8 @@ static bool bi_pair(const AlignParams& P, int64_t i) {
   constexpr int NC = CLS == kAffine2pClass ? 5 : CLS == kAffineClass ? 3 : 1;
   const size_t ring = (size_t)P.scope * NC;
   std::vector<WfD> d1(ring), d2(ring), d3(ring);
-  std::vector<int32_t> v1(ring * P.wmax, 0x5A5A5A5A), v2(ring * P.wmax, 0x5A5A5A5A), v3(ring * P.wmax, 0x5A5A5A5A);
+  std::vector<int32_t> v1(ring * P.wmax, 0x5A5A5A5A), v2(ring * P.wmax, 0x5A5A5A5A);
+  std::vector<int32_t> v3(ring * P.wmax_base, 0x5A5A5A5A);
   std::vector<int4> hist((size_t)P.hist_scores, int4{0, -1, 0, 0});
   std::vector<int32_t> harena((size_t)P.hist_words, 0x5A5A5A5A);
   const int n = P.p_len[i], m = P.t_len[i];
@@ -202,6 +203,7 @@ extern "C" int64_t wfa_emu_biwfa(int metric, const int32_t* pen6, int compute_al
   P.results = results;
   P.num_pairs = num_pairs;
   P.wmax = wmax;
+  P.wmax_base = wmax < 1152 ? wmax : 1152;
   P.hist_scores = hist_scores;
   P.hist_words = hist_words;
   int64_t retries = 0;

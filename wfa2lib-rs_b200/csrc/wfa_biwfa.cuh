@@ -57,7 +57,7 @@ struct BiDriver {
     a.ws = ws;
     a.lane = lane;
     a.scope = P.scope;
-    a.wmax = P.wmax;
+    a.wmax = modular ? P.wmax : P.wmax_base;
     a.modular = modular;
     a.endsfree = false;
     a.p0 = a.pf = a.t0 = a.tf = 0;

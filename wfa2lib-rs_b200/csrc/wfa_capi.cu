@@ -183,6 +183,17 @@ static constexpr int kRingSmemWidth = 64, kSeqSmemWords = 64;
 static constexpr size_t kRingSmemBudget = 8 * 1024;  // bytes per warp
 static constexpr size_t kScratchBudget = (size_t)6 << 30;
 
+// Scratch may grow to half of the device memory that is free (counting the
+// scratch buffer already held), at least kScratchBudget and at most 64 GiB.
+static size_t scratch_budget(wfa_aligner_t* h) {
+  size_t fr = 0, tot = 0;
+  if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+    cudaGetLastError();
+    return kScratchBudget;
+  }
+  return std::max(kScratchBudget, std::min((size_t)64 << 30, (fr + h->scratch.cap) / 2));
+}
+
 struct Round {
   ScratchCfg cfg;
   bool ring_smem;
@@ -315,10 +326,17 @@ static int run_biwfa_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t*
   const int cls = metric_class(P.metric);
   const int nc = metric_components(P.metric);
   P.max_len_sum = max_len_sum;
+  // Forward/reverse rings start at half the longest n + m (a wavefront at
+  // score s spans at most 2s + 1 diagonals, and each half-search stops near
+  // half the pair's score); pairs that outgrow a ring are re-run with twice
+  // the width.  The base-case ring needs about 2 * 530 + 1 cells.
   ScratchCfg cfg;
-  cfg.wmax = std::max(8, std::min(max_len_sum + 3, 1024));
+  const int32_t wfull = std::max(8, max_len_sum + 3);
+  cfg.wmax = std::min(wfull, std::max(1024, ((wfull / 2) + 63) & ~63));
+  int32_t wbase = std::min(cfg.wmax, 1152);
   cfg.hist_scores = 1024 * nc;
-  cfg.hist_words = 65536;
+  cfg.hist_words = 1 << 18;
+  const size_t budget = scratch_budget(h);
   const size_t smem = (size_t)kWarpsPerBlock * 3 * P.scope * nc * kDescBytes;
   if (smem > 200 * 1024) return fail(h, WFA_ERR_UNSUPPORTED, "wavefront ring too large");
   int64_t todo = b->num_pairs;
@@ -329,15 +347,17 @@ static int run_biwfa_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t*
   P.retry_count = reinterpret_cast<int32_t*>(P.work_counter + 1);
   for (int round = 0; todo > 0; ++round) {
     if (round > 8) return fail(h, WFA_ERR_OOM, "alignment needs more scratch than available");
-    const BiLayout L = bi_layout(P.scope, nc, cfg.wmax, cfg.hist_scores, cfg.hist_words, max_len_sum);
+    const BiLayout L = bi_layout(P.scope, nc, cfg.wmax, wbase, cfg.hist_scores, cfg.hist_words,
+                                 max_len_sum);
     int64_t max_warps = (int64_t)h->num_sms * 2 * kWarpsPerBlock;
     int64_t warps = std::max<int64_t>(std::min<int64_t>(max_warps, todo), 1);
-    while (warps > 1 && (size_t)warps * L.words * 4 > kScratchBudget) warps /= 2;
+    while (warps > 1 && (size_t)warps * L.words * 4 > budget) warps = warps * 3 / 4;
     int blocks = (int)((warps + kWarpsPerBlock - 1) / kWarpsPerBlock);
     CUDA_TRY(h, h->scratch.ensure((size_t)blocks * kWarpsPerBlock * L.words * 4), "scratch");
     P.scratch = h->scratch.as<int32_t>();
     P.warp_words = L.words;
     P.wmax = cfg.wmax;
+    P.wmax_base = wbase;
     P.hist_scores = cfg.hist_scores;
     P.hist_words = cfg.hist_words;
     P.pair_list = list;
@@ -367,7 +387,8 @@ static int run_biwfa_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t*
     CUDA_TRY(h, cudaStreamSynchronize(st), "collect retries");
     list = out;
     todo = got;
-    cfg.wmax = std::min(max_len_sum + 3, cfg.wmax * 4);
+    cfg.wmax = std::min(wfull, cfg.wmax * 2);
+    wbase = std::min(cfg.wmax, wbase * 2);
     cfg.hist_scores *= 4;
     cfg.hist_words *= 4;
   }

@@ -49,6 +49,7 @@ struct AlignParams {
   int32_t* scratch;
   int64_t warp_words;  // ints per warp slice
   int32_t wmax;        // ring slot width (cells)
+  int32_t wmax_base;   // BiWFA base-case ring slot width (cells)
   int32_t ring_smem;   // 1: ring cells in shared memory (else in the scratch slice)
   int32_t seq_smem_words;  // per sequence staged in shared memory (0: none)
   int32_t max_len_sum;     // longest n + m of the launch

@@ -162,7 +162,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) biwfa_kernel(const Ali
   const int lane = threadIdx.x & 31;
   const int64_t gwarp = (int64_t)blockIdx.x * kWarpsPerBlock + wib;
   constexpr int NC = CLS == kAffine2pClass ? 5 : CLS == kAffineClass ? 3 : 1;
-  const BiLayout L = bi_layout(P.scope, NC, P.wmax, P.hist_scores, P.hist_words, P.max_len_sum);
+  const BiLayout L = bi_layout(P.scope, NC, P.wmax, P.wmax_base, P.hist_scores, P.hist_words, P.max_len_sum);
   WfD* desc = reinterpret_cast<WfD*>(smem) + (size_t)wib * 3 * P.scope * NC;
   int32_t* slice = P.scratch + gwarp * P.warp_words;
   BiWorkspace bw;

@@ -33,20 +33,24 @@ inline SmemLayout smem_layout(int scope, int nc, int ring_wmax, int seq_words) {
 
 // BiWFA per-warp scratch slice (int32 word offsets).  seq_len_sum is the
 // longest n + m of the launch (sizes the reversed sequences and the base CIGAR).
+// The forward and reverse rings are wmax cells wide; the base-case ring only
+// wmax_base: a base case ends by score 500 (plus one scope), and a wavefront
+// at score s spans at most 2s + 1 diagonals.
 struct BiLayout {
   int64_t ring_f, ring_r, ring_b, hist, harena, rev, cig, words;
 };
 #if defined(__CUDACC__)
 __host__ __device__
 #endif
-inline BiLayout bi_layout(int scope, int nc, int wmax, int hist_scores, int64_t hist_words,
-                          int seq_len_sum) {
+inline BiLayout bi_layout(int scope, int nc, int wmax, int wmax_base, int hist_scores,
+                          int64_t hist_words, int seq_len_sum) {
   BiLayout L;
   const int64_t ring = ((int64_t)scope * nc * wmax + 3) & ~(int64_t)3;
+  const int64_t ring_b = ((int64_t)scope * nc * wmax_base + 3) & ~(int64_t)3;
   L.ring_f = 0;
   L.ring_r = L.ring_f + ring;
   L.ring_b = L.ring_r + ring;
-  L.hist = L.ring_b + ring;
+  L.hist = L.ring_b + ring_b;
   L.harena = L.hist + (int64_t)hist_scores * 4;
   L.rev = L.harena + ((hist_words + 3) & ~(int64_t)3);
   L.cig = L.rev + ((int64_t)seq_len_sum + 48) / 4 + 8;
