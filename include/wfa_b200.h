@@ -214,6 +214,38 @@ WFA_API int wfa_batch_align(wfa_aligner_t* h, const wfa_batch_t* batch, wfa_resu
 WFA_API int wfa_batch_align_device(wfa_aligner_t* h, const wfa_batch_t* batch, wfa_result_t* results,
                            uint8_t* cigars, void* stream);
 
+/* ---- device-buffer batch that allocates nothing -----------------------------
+ * No counterpart in the reference: an addition of this library.
+ *
+ * wfa_batch_align_device grows a scratch buffer with cudaMalloc/cudaFree as
+ * batches need it.  Some callers cannot allow that: a plug-in inside a host
+ * program whose own allocator has already reserved the device memory (a
+ * framework's caching allocator, a server's arena) can see cudaMalloc fail
+ * although the caller has room to spare, and cudaFree waits for the whole
+ * device, stalling every other stream of the program.  This entry point
+ * takes the same arguments and gives the same results, but its scratch is
+ * one fixed device array of WFA_NOALLOC_SCRATCH_BYTES that the library holds
+ * on each device where it has been used, until the process exits; it calls
+ * no allocation routine.
+ *
+ * - The first call on a device looks up the array's device address; make
+ *   that first call before any stream capture.
+ * - Limits: the longest pair of the batch must have p_len + t_len <=
+ *   WFA_NOALLOC_MAX_LEN_SUM, else WFA_ERR_ARGUMENT; an alignment that needs
+ *   more scratch than a quarter of the array fails with WFA_ERR_OOM (use
+ *   wfa_batch_align_device for it).  Spans end-to-end and ends-free; BiWFA
+ *   gives WFA_ERR_UNSUPPORTED.
+ * - Every call on a device shares the one array, which keeps what the last
+ *   call left in it (each call zeroes the counters it needs first).  Calls
+ *   whose work overlaps on the same device (two streams, two handles, two
+ *   threads) race on it: serialise them.
+ * - Like wfa_batch_align_device it synchronises `stream` to read the longest
+ *   pair and the number of pairs to re-run. */
+#define WFA_NOALLOC_SCRATCH_BYTES (64ull << 20)
+#define WFA_NOALLOC_MAX_LEN_SUM 4096
+WFA_API int wfa_batch_align_device_noalloc(wfa_aligner_t* h, const wfa_batch_t* batch,
+                                           wfa_result_t* results, uint8_t* cigars, void* stream);
+
 /* Number of the library's own kernel launches issued so far by this handle. */
 WFA_API int64_t wfa_kernel_launches(const wfa_aligner_t* h);
 

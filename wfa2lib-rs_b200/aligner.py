@@ -84,6 +84,7 @@ def lib():
         "wfa_last_error_string": (ctypes.c_char_p, [vp]),
         "wfa_batch_align": (ctypes.c_int, [vp, ctypes.POINTER(Batch), vp, vp]),
         "wfa_batch_align_device": (ctypes.c_int, [vp, ctypes.POINTER(Batch), vp, vp, vp]),
+        "wfa_batch_align_device_noalloc": (ctypes.c_int, [vp, ctypes.POINTER(Batch), vp, vp, vp]),
         "wfa_kernel_launches": (i64, [vp]),
         "wfa_last_kernel_ms": (ctypes.c_double, [vp]),
         "wfa_cigar_rle": (i32, [vp, i32, ctypes.c_char_p, i32]),
@@ -271,6 +272,19 @@ class WavefrontAligner:
                   p_off, p_len, t_off, t_len, cigar_off, cigar_bytes)
         return self._check(self._L.wfa_batch_align_device(self._h, ctypes.byref(b), results_ptr,
                                                           cigars_ptr, stream))
+
+    def align_batch_device_noalloc(self, seq_ptr, seq_bytes, p_off, p_len, t_off, t_len,
+                                   num_pairs, results_ptr, cigars_ptr=None, cigar_off=None,
+                                   cigar_bytes=0, packed=False, span=SPAN_END2END, stream=0):
+        """align_batch_device without any device allocation: for callers that
+        must not allocate device memory (their own allocator holds it, or a
+        cudaFree would stall their other streams).  Scratch is one fixed
+        64 MiB device array shared by all calls on a device, so calls that
+        overlap on the GPU race; the longest pair may have n + m <= 4096."""
+        b = Batch(SEQ_PACKED2 if packed else SEQ_ASCII, span, num_pairs, seq_ptr, seq_bytes,
+                  p_off, p_len, t_off, t_len, cigar_off, cigar_bytes)
+        return self._check(self._L.wfa_batch_align_device_noalloc(
+            self._h, ctypes.byref(b), results_ptr, cigars_ptr, stream))
 
 
 def cigar_rle(ops):

@@ -16,6 +16,7 @@
 
 #include "wfa_common.h"
 #include "wfa_kernels.h"
+#include "wfa_noalloc.h"
 #include "wfa_params.h"
 
 using namespace wfab;
@@ -402,6 +403,119 @@ static int run_batch_kind(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* 
 }
 
 // ---------------------------------------------------------------------------
+// Batch without allocation: the scratch is the fixed array of wfa_noalloc.cu.
+// Its layout (int32 words): a 64-word header (work counter, retry count,
+// longest n + m, retry-list fill), the retry list (int64 pair indices), then
+// the per-warp slices.
+// ---------------------------------------------------------------------------
+static constexpr int64_t kNaHeaderWords = 64;
+static constexpr int32_t kNaListCap = 65536;  // pairs re-run per round
+static constexpr int64_t kNaSliceOff = kNaHeaderWords + 2 * (int64_t)kNaListCap;
+static constexpr int64_t kNaSliceWords = (int64_t)(kNoAllocScratchBytes / 4) - kNaSliceOff;
+
+// Every pair of 0..n-1 still marked for re-running, up to `cap` of them, into
+// out[]; *count ends as the number of such pairs (it may exceed cap).
+__global__ void collect_retries_capped(const wfa_result_t* res, int64_t n, int64_t* out,
+                                       int32_t* count, int32_t cap) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || res[i].status != kStatusRetry) return;
+  int32_t slot = atomicAdd(count, 1);
+  if (slot < cap) out[slot] = i;
+}
+
+// The rounds of run_device_batch over the fixed array: the first round gives
+// each warp a small M history so that many warps fit; pairs that need more
+// are gathered (at most kNaListCap per round) and re-run with larger slices,
+// until a slice no longer fits a block's warps in the array.
+static int run_noalloc_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* d_results,
+                             uint8_t* d_cigars, cudaStream_t st, int32_t* base, int32_t max_len_sum) {
+  AlignParams P;
+  fill_params(h, b, P);
+  P.results = d_results;
+  P.cigars = d_cigars;
+  if (P.compute_alignment && (!d_cigars || !b->cigar_off))
+    return fail(h, WFA_ERR_ARGUMENT, "CIGAR output buffers are required in alignment scope");
+  const int cls = metric_class(P.metric);
+  const int nc = metric_components(P.metric);
+  unsigned long long* work = reinterpret_cast<unsigned long long*>(base);
+  int32_t* retry = base + 2;
+  int32_t* fill = base + 4;
+  int64_t* list = reinterpret_cast<int64_t*>(base + kNaHeaderWords);
+  Round r = first_round(P, nc, max_len_sum);
+  if (P.compute_alignment) {
+    r.cfg.hist_scores = 256;
+    r.cfg.hist_words = 4096;
+  }
+  int64_t todo = b->num_pairs, pending = 0;
+  int grown = 0;
+  const int64_t* lst = nullptr;
+  h->last_kernel_ms = 0.0;
+  for (;;) {
+    P.seq_smem_words = kSeqSmemWords;
+    P.ring_smem = r.ring_smem ? 1 : 0;
+    P.wmax = r.cfg.wmax;
+    const SmemLayout L = smem_layout(P.scope, nc, r.ring_smem ? r.cfg.wmax : 0, P.seq_smem_words);
+    if (L.total > 200 * 1024) return fail(h, WFA_ERR_UNSUPPORTED, "wavefront ring too large");
+    const int key = cls * 4 + (P.format == WFA_SEQ_PACKED2) * 2 + (needs_general(P) ? 1 : 0);
+    if (key != h->occ_key || L.total != h->occ_smem) {
+      h->occ_val = occupancy_blocks_per_sm(P, cls, L.total);
+      h->occ_key = key;
+      h->occ_smem = L.total;
+    }
+    int64_t ring_words = r.ring_smem ? 0 : (((int64_t)P.scope * nc * r.cfg.wmax + 3) & ~(int64_t)3);
+    int64_t warp_words = ring_words + (int64_t)r.cfg.hist_scores * 4 + r.cfg.hist_words;
+    warp_words = std::max<int64_t>((warp_words + 63) & ~(int64_t)63, 64);
+    const int64_t fit_blocks = kNaSliceWords / (warp_words * kWarpsPerBlock);
+    if (fit_blocks < 1)
+      return fail(h, WFA_ERR_OOM, "an alignment needs more scratch than the fixed no-allocation "
+                                  "array holds (use wfa_batch_align_device)");
+    int64_t warps = std::min<int64_t>((int64_t)h->num_sms * h->occ_val * kWarpsPerBlock, todo);
+    int64_t blocks = std::min<int64_t>((std::max<int64_t>(warps, 1) + kWarpsPerBlock - 1) / kWarpsPerBlock,
+                                       fit_blocks);
+    P.scratch = base + kNaSliceOff;
+    P.warp_words = warp_words;
+    P.hist_scores = r.cfg.hist_scores;
+    P.hist_words = r.cfg.hist_words;
+    P.work_counter = work;
+    P.retry_count = retry;
+    P.pair_list = lst;
+    P.num_pairs = todo;
+    CUDA_TRY(h, cudaMemsetAsync(base, 0, 16, st), "memset");
+    CUDA_TRY(h, cudaEventRecord(h->ev0, st), "event");
+    CUDA_TRY(h, launch_unialign(P, cls, (int)blocks, L.total, st), "kernel launch");
+    CUDA_TRY(h, cudaEventRecord(h->ev1, st), "event");
+    h->launches++;
+    int32_t retries = 0;
+    CUDA_TRY(h, cudaMemcpyAsync(&retries, retry, 4, cudaMemcpyDeviceToHost, st), "retry count");
+    CUDA_TRY(h, cudaStreamSynchronize(st), "kernel");
+    float ms = 0.f;
+    CUDA_TRY(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1), "event");
+    h->last_kernel_ms += ms;
+    if (retries == 0 && pending == 0) break;
+    // Pairs that failed in this round need larger slices; pairs left over
+    // from an earlier gathering are re-run at the current size first.
+    if (retries > 0) {
+      if (++grown > 16) return fail(h, WFA_ERR_OOM, "alignment needs more scratch than available");
+      next_round(r, P, max_len_sum);
+    }
+    CUDA_TRY(h, cudaMemsetAsync(fill, 0, 4, st), "memset");
+    const int64_t n = b->num_pairs;
+    collect_retries_capped<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d_results, n, list, fill,
+                                                                        kNaListCap);
+    h->launches++;
+    CUDA_TRY(h, cudaGetLastError(), "collect retries");
+    int32_t got = 0;
+    CUDA_TRY(h, cudaMemcpyAsync(&got, fill, 4, cudaMemcpyDeviceToHost, st), "retry count");
+    CUDA_TRY(h, cudaStreamSynchronize(st), "collect retries");
+    if (got == 0) break;
+    todo = std::min(got, kNaListCap);
+    pending = got - todo;
+    lst = list;
+  }
+  return WFA_OK;
+}
+
+// ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
 extern "C" {
@@ -712,6 +826,34 @@ int wfa_batch_align_device(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t*
   CUDA_TRY(h, cudaMemcpyAsync(&mx, d_max, 4, cudaMemcpyDeviceToHost, st), "D2H");
   CUDA_TRY(h, cudaStreamSynchronize(st), "max lengths");
   return run_batch_kind(h, b, results, cigars, st, mx);
+}
+
+// The device-buffer batch on the fixed array of wfa_noalloc.cu: no cudaMalloc,
+// cudaFree or other allocation on any path.  Declared with its limits in
+// wfa_b200.h.
+int wfa_batch_align_device_noalloc(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* results,
+                                   uint8_t* cigars, void* stream) {
+  int r = batch_common(h, b);
+  if (r != WFA_OK) return r;
+  if (b->span == WFA_SPAN_BIWFA)
+    return fail(h, WFA_ERR_UNSUPPORTED, "the no-allocation batch runs end-to-end and ends-free spans only");
+  if (b->num_pairs == 0) return WFA_OK;
+  CUDA_TRY(h, cudaSetDevice(h->device), "set device");
+  int32_t* base = nullptr;
+  CUDA_TRY(h, noalloc_scratch(h->device, &base), "address of the no-allocation scratch array");
+  cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+  int32_t* d_max = base + 3;
+  CUDA_TRY(h, cudaMemsetAsync(base, 0, kNaHeaderWords * 4, st), "memset");
+  max_lengths<<<256, 256, 0, st>>>(b->p_len, b->t_len, b->num_pairs, d_max);
+  h->launches++;
+  CUDA_TRY(h, cudaGetLastError(), "max lengths");
+  int32_t mx = 0;
+  CUDA_TRY(h, cudaMemcpyAsync(&mx, d_max, 4, cudaMemcpyDeviceToHost, st), "D2H");
+  CUDA_TRY(h, cudaStreamSynchronize(st), "max lengths");
+  if (mx > WFA_NOALLOC_MAX_LEN_SUM)
+    return fail(h, WFA_ERR_ARGUMENT, "a pair has p_len + t_len above WFA_NOALLOC_MAX_LEN_SUM (4096), "
+                                     "the limit of the no-allocation batch");
+  return run_noalloc_batch(h, b, results, cigars, st, base, mx);
 }
 
 // Host-buffer batch without pipelining (BiWFA): copy in, align, dense CIGARs out.
