@@ -236,8 +236,11 @@ struct Workspace {
 
 // GEN = false compiles the common configuration only (end-to-end, no
 // heuristic): the ends-free and heuristic code paths drop out, which keeps
-// the kernel body small.
-template <int CLS, class S, bool GEN = true>
+// the kernel body small.  UNR diagonals per lane per pass of the affine
+// compute and of the BiWFA extend: their loads are all issued before any
+// result is stored, so a lane keeps UNR cells' loads in flight (wide
+// wavefronts of long pairs, whose cells live in device memory).
+template <int CLS, class S, bool GEN = true, int UNR = 1>
 struct PairAligner {
   static constexpr int NC = CLS == kAffine2pClass ? 5 : CLS == kAffineClass ? 3 : 1;
   static constexpr bool AFF = CLS >= kAffineClass;
@@ -645,29 +648,46 @@ struct PairAligner {
     if (retry) return;
     int mn_m = INT_MAX, mx_m = INT_MIN, mn_i1 = INT_MAX, mx_i1 = INT_MIN, mn_d1 = INT_MAX, mx_d1 = INT_MIN;
     int mn_i2 = INT_MAX, mx_i2 = INT_MIN, mn_d2 = INT_MAX, mx_d2 = INT_MIN;
-    for (int k = lo + lane; k <= hi; k += WFA_WARP) {
-      int32_t i1 = imax(rd(mo1, k - 1), rd(i1e, k - 1)) + 1;
-      int32_t d1 = imax(rd(mo1, k + 1), rd(d1e, k + 1));
-      int32_t mi = rd(mm, k) + 1;
-      int32_t mx;
-      if (!TWO || affine_kernel) {
-        mx = imax(mi, imax(i1, d1));
-      } else {
-        int32_t i2 = imax(rd(mo2, k - 1), rd(i2e, k - 1)) + 1;
-        int32_t d2 = imax(rd(mo2, k + 1), rd(d2e, k + 1));
-        mx = imax(mi, imax(imax(i1, i2), imax(d1, d2)));
-        oi2[k - lo] = i2;
-        od2[k - lo] = d2;
-        if (cell_in_bounds(i2, k, n, m)) { mn_i2 = imin(mn_i2, k); mx_i2 = imax(mx_i2, k); }
-        if (cell_in_bounds(d2, k, n, m)) { mn_d2 = imin(mn_d2, k); mx_d2 = imax(mx_d2, k); }
+    const bool two = TWO && !affine_kernel;
+    for (int k0 = lo + lane; k0 <= hi; k0 += WFA_WARP * UNR) {
+      // Inputs of UNR diagonals first (reads stay inside each input's
+      // initialised range, also for k > hi), then the results.
+      int32_t vi1[UNR], vd1[UNR], vm[UNR], vi2[UNR], vd2[UNR];
+#pragma unroll
+      for (int u = 0; u < UNR; ++u) {
+        const int k = k0 + u * WFA_WARP;
+        vi1[u] = imax(rd(mo1, k - 1), rd(i1e, k - 1)) + 1;
+        vd1[u] = imax(rd(mo1, k + 1), rd(d1e, k + 1));
+        vm[u] = rd(mm, k) + 1;
+        if (two) {
+          vi2[u] = imax(rd(mo2, k - 1), rd(i2e, k - 1)) + 1;
+          vd2[u] = imax(rd(mo2, k + 1), rd(d2e, k + 1));
+        }
       }
-      if (!cell_in_bounds(mx, k, n, m)) mx = kOffsetNull;
-      om[k - L] = mx;
-      oi1[k - lo] = i1;
-      od1[k - lo] = d1;
-      if (mx != kOffsetNull) { mn_m = imin(mn_m, k); mx_m = imax(mx_m, k); }
-      if (cell_in_bounds(i1, k, n, m)) { mn_i1 = imin(mn_i1, k); mx_i1 = imax(mx_i1, k); }
-      if (cell_in_bounds(d1, k, n, m)) { mn_d1 = imin(mn_d1, k); mx_d1 = imax(mx_d1, k); }
+#pragma unroll
+      for (int u = 0; u < UNR; ++u) {
+        const int k = k0 + u * WFA_WARP;
+        if (k > hi) break;
+        const int32_t i1 = vi1[u], d1 = vd1[u];
+        int32_t mx;
+        if (!two) {
+          mx = imax(vm[u], imax(i1, d1));
+        } else {
+          const int32_t i2 = vi2[u], d2 = vd2[u];
+          mx = imax(vm[u], imax(imax(i1, i2), imax(d1, d2)));
+          oi2[k - lo] = i2;
+          od2[k - lo] = d2;
+          if (cell_in_bounds(i2, k, n, m)) { mn_i2 = imin(mn_i2, k); mx_i2 = imax(mx_i2, k); }
+          if (cell_in_bounds(d2, k, n, m)) { mn_d2 = imin(mn_d2, k); mx_d2 = imax(mx_d2, k); }
+        }
+        if (!cell_in_bounds(mx, k, n, m)) mx = kOffsetNull;
+        om[k - L] = mx;
+        oi1[k - lo] = i1;
+        od1[k - lo] = d1;
+        if (mx != kOffsetNull) { mn_m = imin(mn_m, k); mx_m = imax(mx_m, k); }
+        if (cell_in_bounds(i1, k, n, m)) { mn_i1 = imin(mn_i1, k); mx_i1 = imax(mx_i1, k); }
+        if (cell_in_bounds(d1, k, n, m)) { mn_d1 = imin(mn_d1, k); mx_d1 = imax(mx_d1, k); }
+      }
     }
     mn_i1 = Warp::min(mn_i1); mx_i1 = Warp::max(mx_i1);
     mn_d1 = Warp::min(mn_d1); mx_d1 = Warp::max(mx_d1);
@@ -979,16 +999,43 @@ struct PairAligner {
       return false;
     }
     int ak = 0;
-    for (int k = d.lo + lane; k <= d.hi; k += WFA_WARP) {
-      int32_t off = d.vals[k - d.a];
-      if (off >= 0) {
-        int v = off - k, h = off;
-        int R = imin(n - v, m - h);
-        if (R > 0) {
-          off += lcp_fwd(pat, v, txt, h, R);
-          d.vals[k - d.a] = off;
+    for (int k0 = d.lo + lane; k0 <= d.hi; k0 += WFA_WARP * UNR) {
+      // Offsets and first sequence words of UNR diagonals, then the rest.
+      int32_t off[UNR], R[UNR];
+      uint32_t x[UNR];
+#pragma unroll
+      for (int u = 0; u < UNR; ++u) {
+        const int k = k0 + u * WFA_WARP;
+        off[u] = k <= d.hi ? d.vals[k - d.a] : -1;
+      }
+#pragma unroll
+      for (int u = 0; u < UNR; ++u) {
+        const int k = k0 + u * WFA_WARP;
+        R[u] = 0;
+        x[u] = 0;
+        if (off[u] >= 0) {
+          R[u] = imin(n - (off[u] - k), m - off[u]);
+          if (R[u] > 0) x[u] = pat.fetch(off[u] - k) ^ txt.fetch(off[u]);
         }
-        if (max) ak = imax(ak, 2 * off - k);
+      }
+#pragma unroll
+      for (int u = 0; u < UNR; ++u) {
+        const int k = k0 + u * WFA_WARP;
+        if (off[u] < 0) continue;
+        if (R[u] > 0) {
+          // lcp_fwd with its first compare done above
+          int l;
+          if (x[u]) {
+            l = (int)((Warp::ffs(x[u]) - 1) / S::BITS);
+          } else {
+            l = S::UNITS;
+            if (R[u] > S::UNITS)
+              l += lcp_fwd(pat, off[u] - k + S::UNITS, txt, off[u] + S::UNITS, R[u] - S::UNITS);
+          }
+          off[u] += imin(l, R[u]);
+          d.vals[k - d.a] = off[u];
+        }
+        if (max) ak = imax(ak, 2 * off[u] - k);
       }
     }
     Warp::sync();

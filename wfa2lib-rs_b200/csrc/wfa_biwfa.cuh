@@ -33,9 +33,12 @@ struct BiWorkspace {
   uint8_t* cig_tmp;          // base-case CIGAR, written backwards
 };
 
+// Diagonals per lane per pass in the BiWFA aligners (see PairAligner).
+constexpr int kBiUnroll = 4;
+
 template <int CLS, class S>
 struct BiDriver {
-  using A = PairAligner<CLS, S, true>;
+  using A = PairAligner<CLS, S, true, kBiUnroll>;
   static constexpr int NC = A::NC;
   static constexpr bool AFF = A::AFF;
   static constexpr bool TWO = A::TWO;

@@ -343,6 +343,27 @@ static int run_biwfa_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t*
   int64_t todo = b->num_pairs;
   const int64_t* list = nullptr;
   h->last_kernel_ms = 0.0;
+  // Longest pairs first: the kernel's work queue hands pairs out in list
+  // order, so the pairs that take longest start first and the launch does
+  // not end waiting on one long pair started late.  The list takes the
+  // first third of the pair-list buffer, the re-run lists the other two.
+  const int64_t np = b->num_pairs;
+  CUDA_TRY(h, h->pairlist.ensure(3 * (size_t)std::max<int64_t>(np, 1) * 8), "pair list");
+  int64_t* order_d = h->pairlist.as<int64_t>();
+  if (np > 1) {
+    std::vector<int32_t> hl((size_t)np), ht((size_t)np);
+    CUDA_TRY(h, cudaMemcpyAsync(hl.data(), b->p_len, (size_t)np * 4, cudaMemcpyDeviceToHost, st), "D2H");
+    CUDA_TRY(h, cudaMemcpyAsync(ht.data(), b->t_len, (size_t)np * 4, cudaMemcpyDeviceToHost, st), "D2H");
+    CUDA_TRY(h, cudaStreamSynchronize(st), "lengths");
+    std::vector<int64_t> order((size_t)np);
+    for (int64_t i = 0; i < np; ++i) order[(size_t)i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int64_t x, int64_t y) {
+      return (int64_t)hl[(size_t)x] + ht[(size_t)x] > (int64_t)hl[(size_t)y] + ht[(size_t)y];
+    });
+    CUDA_TRY(h, cudaMemcpyAsync(order_d, order.data(), (size_t)np * 8, cudaMemcpyHostToDevice, st), "H2D");
+    CUDA_TRY(h, cudaStreamSynchronize(st), "pair order");
+    list = order_d;
+  }
   CUDA_TRY(h, h->counters.ensure(64), "counters");
   P.work_counter = h->counters.as<unsigned long long>();
   P.retry_count = reinterpret_cast<int32_t*>(P.work_counter + 1);
@@ -375,9 +396,8 @@ static int run_biwfa_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t*
     CUDA_TRY(h, cudaEventElapsedTime(&ms, h->ev0, h->ev1), "event");
     h->last_kernel_ms += ms;
     if (retries == 0) break;
-    CUDA_TRY(h, h->pairlist.ensure(2 * (size_t)std::max<int64_t>(b->num_pairs, 1) * 8), "pair list");
-    int64_t* half0 = h->pairlist.as<int64_t>();
-    int64_t* half1 = half0 + b->num_pairs;
+    int64_t* half0 = order_d + np;
+    int64_t* half1 = half0 + np;
     int64_t* out = (list == half0) ? half1 : half0;
     CUDA_TRY(h, cudaMemsetAsync(P.retry_count, 0, 4, st), "memset");
     collect_retries<<<(unsigned)((todo + 255) / 256), 256, 0, st>>>(d_results, list, todo, out, P.retry_count);
