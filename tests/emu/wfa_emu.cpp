@@ -114,9 +114,12 @@ extern "C" int64_t wfa_emu_batch(int metric, const int32_t* pen6, int compute_al
   return retries;
 }
 
+// Same dispatch as the kernel launcher: the lean instantiation without a
+// heuristic, the general one with.
 template <int CLS, class S>
 static bool bi_lane(const AlignParams& P, const BiWorkspace& bw, int64_t i, S pat, S txt, S rpat, S rtxt) {
-  return biwfa_one<CLS, S>(P, bw, i, pat, txt, rpat, rtxt);
+  if (P.hkind == WFA_HEURISTIC_NONE) return biwfa_one<CLS, S, false>(P, bw, i, pat, txt, rpat, rtxt);
+  return biwfa_one<CLS, S, true>(P, bw, i, pat, txt, rpat, rtxt);
 }
 
 template <int CLS>

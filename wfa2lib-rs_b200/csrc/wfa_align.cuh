@@ -195,6 +195,7 @@ WFA_D int lcp_bwd(const S& P, int v, const S& T, int h, int R) {
 // Wavefront descriptors
 // ---------------------------------------------------------------------------
 constexpr int kPresent = 1, kNullFlag = 2;
+constexpr int32_t kAdUnknown = INT32_MAX / 4, kAdNone = INT32_MIN / 4;
 constexpr int CM = 0, CI1 = 1, CD1 = 2, CI2 = 3, CD2 = 4;
 
 struct WfD {
@@ -202,20 +203,27 @@ struct WfD {
   int32_t lo, hi; // limits
   int32_t a, b;   // initialised range
   int32_t flags;
-  int32_t pad;
+  // Upper bound on the antidiagonal 2 * offset - k of the stored cells
+  // (kAdUnknown: none known).  BiWFA's breakpoint scans skip wavefront
+  // pairs whose bounds cannot add up to a meeting.
+  int32_t adub;
 };
 
 WFA_D bool wf_present(const WfD& d) { return (d.flags & kPresent) != 0; }
 WFA_D bool wf_is_null(const WfD& d) { return !(d.flags & kPresent) || (d.flags & kNullFlag); }
 WFA_D WfD wf_none() {
   WfD d;
-  d.vals = nullptr; d.lo = 1; d.hi = -1; d.a = 1; d.b = 0; d.flags = 0; d.pad = 0;
+  d.vals = nullptr; d.lo = 1; d.hi = -1; d.a = 1; d.b = 0; d.flags = 0; d.adub = kAdUnknown;
   return d;
 }
 // Cell read with the reference's semantics (OFFSET_NULL outside the
 // initialised range; null inputs read as the null wavefront).
 WFA_D int32_t rd(const WfD& d, int k) {
   return (k >= d.a && k <= d.b) ? d.vals[k - d.a] : kOffsetNull;
+}
+// Antidiagonal bound of a live wavefront (kAdNone for an absent or null one).
+WFA_D int32_t ad_of(const WfD& d) {
+  return (d.flags == kPresent) ? d.adub : kAdNone;
 }
 WFA_D bool cell_in_bounds(int32_t off, int k, int n, int m) {
   return (uint32_t)off <= (uint32_t)m && (uint32_t)(off - k) <= (uint32_t)n;
@@ -382,7 +390,7 @@ struct PairAligner {
   WFA_D WfD finish(int32_t* base, int L, int lo, int hi, int vmin, int vmax) {
     WfD d;
     d.flags = kPresent;
-    d.pad = 0;
+    d.adub = kAdUnknown;
     if (vmax >= vmin && vmax != INT_MIN) {
       d.lo = vmin; d.hi = vmax;
     } else {
@@ -450,7 +458,7 @@ struct PairAligner {
     }
     Warp::sync();
     WfD d;
-    d.vals = v; d.lo = lo; d.hi = hi; d.a = lo; d.b = hi; d.flags = kPresent; d.pad = 0;
+    d.vals = v; d.lo = lo; d.hi = hi; d.a = lo; d.b = hi; d.flags = kPresent; d.adub = kAdUnknown;
     return d;
   }
 
@@ -506,7 +514,7 @@ struct PairAligner {
     }
     Warp::sync();
     WfD d;
-    d.vals = v; d.lo = lo0; d.hi = hi0; d.a = lo0; d.b = hi0; d.flags = kPresent; d.pad = 0;
+    d.vals = v; d.lo = lo0; d.hi = hi0; d.a = lo0; d.b = hi0; d.flags = kPresent; d.adub = kAdUnknown;
     set_m(0, d);
   }
 
@@ -646,6 +654,13 @@ struct PairAligner {
     int32_t *oi2 = nullptr, *od2 = nullptr;
     if (TWO && !affine_kernel) { oi2 = alloc(CI2, s, lo, hi); od2 = alloc(CD2, s, lo, hi); }
     if (retry) return;
+    if constexpr (UNR > 1) {
+      if (!bf) {
+        affine_wide(s, lo, hi, mm, mo1, i1e, d1e, mo2, i2e, d2e, TWO && !affine_kernel, om, oi1, od1,
+                    oi2, od2);
+        return;
+      }
+    }
     int mn_m = INT_MAX, mx_m = INT_MIN, mn_i1 = INT_MAX, mx_i1 = INT_MIN, mn_d1 = INT_MAX, mx_d1 = INT_MIN;
     int mn_i2 = INT_MAX, mx_i2 = INT_MIN, mn_d2 = INT_MAX, mx_d2 = INT_MIN;
     const bool two = TWO && !affine_kernel;
@@ -712,6 +727,151 @@ struct PairAligner {
       mn_m = Warp::min(mn_m); mx_m = Warp::max(mx_m);
       set_m(s, finish(om, L, lo, hi, mn_m, mx_m));
     }
+  }
+
+
+  // ---- wide affine compute (UNR > 1: BiWFA) -----------------------------------
+  // The same cells as compute_affine's loop.  Cells whose every input lies
+  // inside the input's initialised range are read without range checks, UNR
+  // per lane per pass; the trim (trim_ends, src/compute/mod.rs:14-49) is
+  // found by scanning in from both ends of each stored row.
+  template <bool CHK, int U>
+  WFA_D void wide_pass(int kb, int ke, int lo, const WfD& mm, const WfD& mo1, const WfD& i1e,
+                       const WfD& d1e, const WfD& mo2, const WfD& i2e, const WfD& d2e, bool two,
+                       int32_t* om, int32_t* oi1, int32_t* od1, int32_t* oi2, int32_t* od2) {
+    for (int k0 = kb + lane; k0 <= ke; k0 += WFA_WARP * U) {
+      int32_t vi1[U], vd1[U], vm[U], vi2[U], vd2[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int k = imin(k0 + u * WFA_WARP, ke);  // lanes past ke repeat ke's reads
+        if (CHK) {
+          vi1[u] = imax(rd(mo1, k - 1), rd(i1e, k - 1)) + 1;
+          vd1[u] = imax(rd(mo1, k + 1), rd(d1e, k + 1));
+          vm[u] = rd(mm, k) + 1;
+          if (two) {
+            vi2[u] = imax(rd(mo2, k - 1), rd(i2e, k - 1)) + 1;
+            vd2[u] = imax(rd(mo2, k + 1), rd(d2e, k + 1));
+          }
+        } else {
+          vi1[u] = imax(mo1.vals[k - 1 - mo1.a], i1e.vals[k - 1 - i1e.a]) + 1;
+          vd1[u] = imax(mo1.vals[k + 1 - mo1.a], d1e.vals[k + 1 - d1e.a]);
+          vm[u] = mm.vals[k - mm.a] + 1;
+          if (two) {
+            vi2[u] = imax(mo2.vals[k - 1 - mo2.a], i2e.vals[k - 1 - i2e.a]) + 1;
+            vd2[u] = imax(mo2.vals[k + 1 - mo2.a], d2e.vals[k + 1 - d2e.a]);
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int k = k0 + u * WFA_WARP;
+        if (k > ke) break;
+        int32_t mx = imax(vm[u], imax(vi1[u], vd1[u]));
+        if (two) mx = imax(mx, imax(vi2[u], vd2[u]));
+        if (!cell_in_bounds(mx, k, n, m)) mx = kOffsetNull;
+        om[k - lo] = mx;
+        oi1[k - lo] = vi1[u];
+        od1[k - lo] = vd1[u];
+        if (two) {
+          oi2[k - lo] = vi2[u];
+          od2[k - lo] = vd2[u];
+        }
+      }
+    }
+  }
+  // Highest / lowest k of row[lo..hi] (row[0] is cell lo) holding an
+  // in-bounds offset; INT_MIN / INT_MAX if none.
+  WFA_D int row_last(const int32_t* row, int lo, int hi) const {
+    for (int top = hi; top >= lo; top -= WFA_WARP) {
+      const int k = top - lane;
+      const bool ok = k >= lo && cell_in_bounds(row[k - lo], k, n, m);
+      const int best = Warp::max(ok ? k : INT_MIN);
+      if (best != INT_MIN) return best;
+    }
+    return INT_MIN;
+  }
+  WFA_D int row_first(const int32_t* row, int lo, int hi) const {
+    for (int bot = lo; bot <= hi; bot += WFA_WARP) {
+      const int k = bot + lane;
+      const bool ok = k <= hi && cell_in_bounds(row[k - lo], k, n, m);
+      const int best = Warp::min(ok ? k : INT_MAX);
+      if (best != INT_MAX) return best;
+    }
+    return INT_MAX;
+  }
+  WFA_D void affine_wide(int s, int lo, int hi, const WfD& mm, const WfD& mo1, const WfD& i1e,
+                         const WfD& d1e, const WfD& mo2, const WfD& i2e, const WfD& d2e, bool two,
+                         int32_t* om, int32_t* oi1, int32_t* od1, int32_t* oi2, int32_t* od2) {
+    // Interior: every read of every input inside its initialised range
+    // (mm at k, mo1/mo2 at k-1 and k+1, i1e/i2e at k-1, d1e/d2e at k+1).
+    int ilo = imax(mm.a, imax(mo1.a + 1, imax(i1e.a + 1, d1e.a - 1)));
+    int ihi = imin(mm.b, imin(mo1.b - 1, imin(i1e.b + 1, d1e.b - 1)));
+    if (two) {
+      ilo = imax(ilo, imax(mo2.a + 1, imax(i2e.a + 1, d2e.a - 1)));
+      ihi = imin(ihi, imin(mo2.b - 1, imin(i2e.b + 1, d2e.b - 1)));
+    }
+    ilo = imax(ilo, lo);
+    ihi = imin(ihi, hi);
+    if (ilo > ihi) { ilo = hi + 1; ihi = hi; }  // no interior: all checked
+    // Edges (checked, one diagonal per lane per pass), then the interior.
+    for (int e = 0; e < 2; ++e) {
+      const int kb = e == 0 ? lo : ihi + 1, ke = e == 0 ? ilo - 1 : hi;
+      if (kb <= ke)
+        wide_pass<true, 1>(kb, ke, lo, mm, mo1, i1e, d1e, mo2, i2e, d2e, two, om, oi1, od1, oi2, od2);
+    }
+    if (ilo <= ihi)
+      wide_pass<false, UNR>(ilo, ihi, lo, mm, mo1, i1e, d1e, mo2, i2e, d2e, two, om, oi1, od1, oi2, od2);
+    Warp::sync();  // the scans read cells other lanes stored
+    // Trims of the rows I1, D1 (, I2, D2) and M: the top and then the bottom
+    // WFA_WARP cells of every row are checked together; a row whose end
+    // chunk holds no in-bounds cell continues with a scan.
+    constexpr int RN = TWO ? 5 : 3;
+    int32_t* rows[RN];
+    rows[0] = oi1;
+    rows[1] = od1;
+    if (TWO) { rows[2] = oi2; rows[3] = od2; }
+    rows[RN - 1] = om;
+    int last[RN], first[RN];
+    {
+      const int k = hi - lane;
+      int32_t v[RN];
+#pragma unroll
+      for (int r = 0; r < RN; ++r) v[r] = (k >= lo && (two || r < 2 || r == RN - 1)) ? rows[r][k - lo] : kOffsetNull;
+#pragma unroll
+      for (int r = 0; r < RN; ++r) last[r] = Warp::max(cell_in_bounds(v[r], k, n, m) ? k : INT_MIN);
+    }
+#pragma unroll
+    for (int r = 0; r < RN; ++r)
+      if (last[r] == INT_MIN && (two || r < 2 || r == RN - 1) && hi - WFA_WARP >= lo)
+        last[r] = row_last(rows[r], lo, hi - WFA_WARP);
+    {
+      const int k = lo + lane;
+      int32_t v[RN];
+#pragma unroll
+      for (int r = 0; r < RN; ++r) v[r] = (k <= last[r]) ? rows[r][k - lo] : kOffsetNull;
+#pragma unroll
+      for (int r = 0; r < RN; ++r) first[r] = Warp::min(cell_in_bounds(v[r], k, n, m) ? k : INT_MAX);
+    }
+#pragma unroll
+    for (int r = 0; r < RN; ++r)
+      if (first[r] == INT_MAX && last[r] != INT_MIN)
+        first[r] = row_first(rows[r] + WFA_WARP, lo + WFA_WARP, last[r]);
+    // Antidiagonal bounds: I[k] = max(M'[k-1], I'[k-1]) + 1 and
+    // D[k] = max(M'[k+1], D'[k+1]) both lie one antidiagonal above a source
+    // cell.  M's bound is set by the extend step.
+    WfD r;
+    r = finish(oi1, lo, lo, hi, first[0], last[0]); r.adub = imax(ad_of(mo1), ad_of(i1e)) + 1; put_ns(CI1, s, r);
+    r = finish(od1, lo, lo, hi, first[1], last[1]); r.adub = imax(ad_of(mo1), ad_of(d1e)) + 1; put_ns(CD1, s, r);
+    if (TWO) {
+      if (two) {
+        r = finish(oi2, lo, lo, hi, first[2], last[2]); r.adub = imax(ad_of(mo2), ad_of(i2e)) + 1; put_ns(CI2, s, r);
+        r = finish(od2, lo, lo, hi, first[3], last[3]); r.adub = imax(ad_of(mo2), ad_of(d2e)) + 1; put_ns(CD2, s, r);
+      } else {
+        put_ns(CI2, s, wf_none());
+        put_ns(CD2, s, wf_none());
+      }
+    }
+    set_m(s, finish(om, lo, lo, hi, first[RN - 1], last[RN - 1]));
   }
 
   WFA_D void compute_step(int s) {
@@ -970,7 +1130,7 @@ struct PairAligner {
     if (retry) return;
     if (lane == 0) v[0] = 0;
     WfD d;
-    d.vals = v; d.lo = 0; d.hi = 0; d.a = 0; d.b = 0; d.flags = kPresent; d.pad = 0;
+    d.vals = v; d.lo = 0; d.hi = 0; d.a = 0; d.b = 0; d.flags = kPresent; d.adub = 0;
     put(comp, 0, d);
   }
 
@@ -1035,11 +1195,12 @@ struct PairAligner {
           off[u] += imin(l, R[u]);
           d.vals[k - d.a] = off[u];
         }
-        if (max) ak = imax(ak, 2 * off[u] - k);
+        ak = imax(ak, 2 * off[u] - k);
       }
     }
+    ak = Warp::max(ak);
+    if (lane == 0) slot(CM, score).adub = ak;
     Warp::sync();
-    if (max) ak = Warp::max(ak);
     // check_component_termination, src/aligner.rs:3268-3302
     WfD e = slot(comp_end, score);
     int kend = m - n;
@@ -1052,7 +1213,7 @@ struct PairAligner {
       status = WFA_STATUS_END_UNREACHABLE;
       return true;
     }
-    max_ak = ak;
+    max_ak = max ? ak : 0;
     return false;
   }
 

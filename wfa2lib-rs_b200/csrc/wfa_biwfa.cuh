@@ -36,15 +36,20 @@ struct BiWorkspace {
 // Diagonals per lane per pass in the BiWFA aligners (see PairAligner).
 constexpr int kBiUnroll = 4;
 
-template <int CLS, class S>
+// GEN = false: no heuristic (the lean aligner instantiation).
+template <int CLS, class S, bool GEN>
 struct BiDriver {
-  using A = PairAligner<CLS, S, true, kBiUnroll>;
+  using A = PairAligner<CLS, S, GEN, kBiUnroll>;
   static constexpr int NC = A::NC;
   static constexpr bool AFF = A::AFF;
   static constexpr bool TWO = A::TWO;
 
   const AlignParams& P;
-  A fwd, rev, base;
+  A fwd, rev;
+  // The base-case aligner is built by each base case (its state is dead
+  // during the breakpoint searches, which keeps their registers free).
+  Workspace base_ws;
+  uint8_t* base_cg;
   S pat, txt, rpat, rtxt;  // whole-pair views: forward and reversed
   int32_t n, m, lane;
   uint8_t* cg;  // output CIGAR (forward appends)
@@ -52,7 +57,7 @@ struct BiDriver {
   int32_t hkind, hp0, hp1, hp2;
   bool retry;
 
-  WFA_D BiDriver(const AlignParams& p) : P(p), fwd(p), rev(p), base(p) {}
+  WFA_D BiDriver(const AlignParams& p) : P(p), fwd(p), rev(p) {}
 
   static WFA_D S sub(const S& x, int begin, int len);
 
@@ -60,7 +65,10 @@ struct BiDriver {
     a.ws = ws;
     a.lane = lane;
     a.scope = P.scope;
-    a.wmax = modular ? P.wmax : P.wmax_base;
+    // Ring rows as wide as this pair's wavefronts can be (trimmed inputs
+    // span at most n + m + 1 diagonals, a computed range two more), so a
+    // short pair's rows sit close together in the warp's slice.
+    a.wmax = imin(modular ? P.wmax : P.wmax_base, n + m + 3);
     a.modular = modular;
     a.endsfree = false;
     a.p0 = a.pf = a.t0 = a.tf = 0;
@@ -93,7 +101,7 @@ struct BiDriver {
     for (int64_t i = lane; i < len; i += WFA_WARP) cg[cg_len + i] = op;
     cg_len += len;
   }
-  WFA_D void append_base() {  // base.cigar [cg_begin, cg_end) forward
+  WFA_D void append_base(const A& base) {  // base.cigar [cg_begin, cg_end) forward
     int64_t len = base.cg_end - base.cg_begin;
     if (len <= 0) return;
     if (cg_len + len > cg_cap) { retry = true; return; }
@@ -108,6 +116,9 @@ struct BiDriver {
   WFA_D void scan(const WfD& w0, const WfD& w1, int plen, int tlen, int s0, int s1, int go, int comp,
                   bool indel, bool forward, BiBreakpoint& bp) {
     if (s0 + s1 - go >= bp.score) return;
+    // A meeting o0 + o1 >= tlen on diagonals k1 = (tlen - plen) - k0 needs
+    // antidiagonals adding up to tlen + plen: skip pairs whose bounds cannot.
+    if (ad_of(w0) + ad_of(w1) < tlen + plen) return;
     int lo0 = w0.lo, hi0 = w0.hi;
     int lo1i = (tlen - plen) - w1.hi, hi1i = (tlen - plen) - w1.lo;
     if (hi1i < lo0 || hi0 < lo1i) return;
@@ -232,6 +243,9 @@ struct BiDriver {
 
   // bialign_base, src/aligner.rs:3127-3202
   WFA_D int base_case(int pb, int pe, int tb, int te, int cb, int ce, int32_t& result) {
+    A base(P);
+    setup(base, base_ws, false);
+    base.cg = base_cg;
     set_heur(base, hp0 - (tb - pb), hp1 - (tb - pb));
     set_seqs(base, false, pb, pe, tb, te);
     base.cap = imax(base.dims_num(1000, 1000), base.dims_num(base.n, base.m));
@@ -268,7 +282,7 @@ struct BiDriver {
       st = BI_UNATTAINABLE;
     }
     if (base.status == WFA_STATUS_OOM) return BI_RETRY;
-    append_base();
+    append_base(base);
     return st;
   }
 
@@ -341,8 +355,8 @@ struct BiDriver {
   }
 };
 
-template <int CLS, class S>
-WFA_D S BiDriver<CLS, S>::sub(const S& x, int begin, int len) {
+template <int CLS, class S, bool GEN>
+WFA_D S BiDriver<CLS, S, GEN>::sub(const S& x, int begin, int len) {
   S v = x;
   if constexpr (S::UNITS == 16) {
     v.off = x.off + begin;
@@ -355,10 +369,10 @@ WFA_D S BiDriver<CLS, S>::sub(const S& x, int begin, int len) {
 
 // align_biwfa (src/aligner.rs:2563-2644) or align_biwfa_score (:2650-2698)
 // of pair `pair`; writes its result.  Returns true to retry with more scratch.
-template <int CLS, class S>
+template <int CLS, class S, bool GEN>
 WFA_D bool biwfa_one(const AlignParams& P, const BiWorkspace& bw, int64_t pair, S pat, S txt,
                      S rpat, S rtxt) {
-  BiDriver<CLS, S> D(P);
+  BiDriver<CLS, S, GEN> D(P);
   D.lane = Warp::lane();
   D.n = P.p_len[pair];
   D.m = P.t_len[pair];
@@ -367,8 +381,8 @@ WFA_D bool biwfa_one(const AlignParams& P, const BiWorkspace& bw, int64_t pair, 
   D.retry = false;
   D.setup(D.fwd, bw.fwd, true);
   D.setup(D.rev, bw.rev, true);
-  D.setup(D.base, bw.base, false);
-  D.base.cg = bw.cig_tmp;
+  D.base_ws = bw.base;
+  D.base_cg = bw.cig_tmp;
   const int n = D.n, m = D.m;
   int32_t score = 0, status;
   D.cg = nullptr;
@@ -396,10 +410,10 @@ WFA_D bool biwfa_one(const AlignParams& P, const BiWorkspace& bw, int64_t pair, 
     if (st == BI_OK) {
       bool heur = P.hkind != WFA_HEURISTIC_NONE && D.cg_len > 0;
       if (n == 0 || m == 0 || heur) {
-        uint8_t* saved = D.base.cg;
-        D.base.cg = D.cg;
-        score = D.base.cigar_wfa_score(0, D.cg_len, n, m);
-        D.base.cg = saved;
+        typename BiDriver<CLS, S, GEN>::A sc(P);
+        D.setup(sc, bw.base, false);
+        sc.cg = D.cg;
+        score = sc.cigar_wfa_score(0, D.cg_len, n, m);
       } else {
         score = result;
       }

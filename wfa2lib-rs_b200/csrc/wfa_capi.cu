@@ -327,16 +327,19 @@ static int run_biwfa_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t*
   const int cls = metric_class(P.metric);
   const int nc = metric_components(P.metric);
   P.max_len_sum = max_len_sum;
-  // Forward/reverse rings start at half the longest n + m (a wavefront at
-  // score s spans at most 2s + 1 diagonals, and each half-search stops near
-  // half the pair's score); pairs that outgrow a ring are re-run with twice
-  // the width.  The base-case ring needs about 2 * 530 + 1 cells.
+  // Forward/reverse rings are as wide as any wavefront of the launch can be
+  // (n + m + 3 cells for the longest pair): a pair re-run for a narrow ring
+  // costs its whole alignment again, and ring cells beyond a wavefront's
+  // width are never touched.  The base-case ring needs about 2 * 530 + 1
+  // cells (a base case ends by score 500 plus one scope).
   ScratchCfg cfg;
   const int32_t wfull = std::max(8, max_len_sum + 3);
-  cfg.wmax = std::min(wfull, std::max(1024, ((wfull / 2) + 63) & ~63));
+  cfg.wmax = wfull;
   int32_t wbase = std::min(cfg.wmax, 1152);
+  // Base-case history: every component of scores up to about 550, each at
+  // most 2s + 1 cells wide.
   cfg.hist_scores = 1024 * nc;
-  cfg.hist_words = 1 << 18;
+  cfg.hist_words = (int64_t)nc * 600 * 600;
   const size_t budget = scratch_budget(h);
   const size_t smem = (size_t)kWarpsPerBlock * 3 * P.scope * nc * kDescBytes;
   if (smem > 200 * 1024) return fail(h, WFA_ERR_UNSUPPORTED, "wavefront ring too large");
