@@ -200,12 +200,20 @@ struct Round {
   bool ring_smem;
 };
 
+// Long pairs (n + m above kLongPair) start with the ring in the scratch
+// slice and an M history sized from the lengths: a re-run after an overflow
+// late in a long alignment repeats most of its work.
+static constexpr int32_t kLongPair = 2048;
+
 static Round first_round(const AlignParams& P, int nc, int32_t max_len_sum) {
   Round r;
+  const bool longp = max_len_sum > kLongPair;
   r.cfg.wmax = std::max(8, std::min(max_len_sum + 3, 8192));
-  r.cfg.hist_scores = P.compute_alignment ? 1024 : 0;
-  r.cfg.hist_words = P.compute_alignment ? (int64_t)std::max(32768, 16 * (max_len_sum + 3)) : 0;
-  r.ring_smem = (size_t)P.scope * nc * kRingSmemWidth * 4 <= kRingSmemBudget;
+  r.cfg.hist_scores = P.compute_alignment ? (longp ? max_len_sum + 3 : 1024) : 0;
+  r.cfg.hist_words = P.compute_alignment
+                         ? (int64_t)std::max(32768, (longp ? 64 : 16) * (max_len_sum + 3))
+                         : 0;
+  r.ring_smem = !longp && (size_t)P.scope * nc * kRingSmemWidth * 4 <= kRingSmemBudget;
   if (r.ring_smem) r.cfg.wmax = std::min(r.cfg.wmax, kRingSmemWidth);
   return r;
 }
@@ -246,7 +254,8 @@ static int launch_round(wfa_aligner_t* h, AlignParams& P, const Round& r, int64_
   warp_words = std::max<int64_t>((warp_words + 63) & ~(int64_t)63, 64);
   int64_t max_warps = (int64_t)h->num_sms * h->occ_val * kWarpsPerBlock;
   int64_t warps = std::max<int64_t>(std::min<int64_t>(max_warps, todo), 1);
-  while (warps > kWarpsPerBlock && (size_t)warps * warp_words * 4 > kScratchBudget) warps /= 2;
+  const size_t budget = (size_t)warps * warp_words * 4 > kScratchBudget ? scratch_budget(h) : kScratchBudget;
+  while (warps > kWarpsPerBlock && (size_t)warps * warp_words * 4 > budget) warps /= 2;
   int blocks = (int)((warps + kWarpsPerBlock - 1) / kWarpsPerBlock);
   size_t scratch_bytes = (size_t)blocks * kWarpsPerBlock * warp_words * 4;
   CUDA_TRY(h, h->scratch.ensure(scratch_bytes), "scratch");

@@ -107,6 +107,47 @@ def config2(num=1_000_000):
     return uniform_pairs(num, 100, 150, 0.0, 0.04, SEED_BASE + 2)
 
 
+def config4(num=200_000, seed=SEED_BASE + 4, chunk=10_000):
+    """Ends-free / extension: core length U[500, 5000] at a 10% edit rate
+    (the per-position sub/ins/del model), and every sequence (pattern and
+    text, independently) flanked on each side by a random ACGT tail of
+    U[0, 0.2 * core] bases.  Generated in chunks of `chunk` pairs (chunk i
+    seeded with seed + i) to bound the memory of the generator."""
+    parts = [_config4_chunk(min(chunk, num - i), seed + i // chunk) for i in range(0, num, chunk)]
+    if len(parts) == 1:
+        return parts[0]
+    base = np.concatenate([[0], np.cumsum([len(q.buf) for q in parts])[:-1]]).astype(np.int64)
+    return PairSet(np.concatenate([q.buf for q in parts]),
+                   np.concatenate([q.p_off + b for q, b in zip(parts, base)]),
+                   np.concatenate([q.p_len for q in parts]),
+                   np.concatenate([q.t_off + b for q, b in zip(parts, base)]),
+                   np.concatenate([q.t_len for q in parts]))
+
+
+def _config4_chunk(num, seed):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    core_len = rng.integers(500, 5001, num).astype(np.int32)
+    cores = ACGT[rng.integers(0, 4, int(core_len.sum()))]
+    texts, t_core = _mutate(rng, cores, core_len, np.full(num, 0.10))
+    # Flank lengths: pattern left/right, text left/right.
+    fl = (rng.random((num, 4)) * (0.2 * core_len[:, None] + 1)).astype(np.int64)
+    fl = np.minimum(fl, (0.2 * core_len[:, None]).astype(np.int64))
+    p_len = (core_len + fl[:, 0] + fl[:, 1]).astype(np.int32)
+    t_len = (t_core + fl[:, 2] + fl[:, 3]).astype(np.int32)
+    total = int(p_len.sum()) + int(t_len.sum())
+    rnd = ACGT[rng.integers(0, 4, total)]  # flank bases (cores overwrite their part)
+    p_off = np.concatenate([[0], np.cumsum(p_len.astype(np.int64) + t_len)[:-1]]).astype(np.int64)
+    t_off = p_off + p_len
+    buf = rnd.copy()
+    c_start = np.concatenate([[0], np.cumsum(core_len.astype(np.int64))[:-1]])
+    t_start = np.concatenate([[0], np.cumsum(t_core.astype(np.int64))[:-1]])
+    pos_p = np.repeat(p_off + fl[:, 0] - c_start, core_len) + np.arange(int(core_len.sum()))
+    pos_t = np.repeat(t_off + fl[:, 2] - t_start, t_core) + np.arange(int(t_core.sum()))
+    buf[pos_p] = cores
+    buf[pos_t] = texts
+    return PairSet(buf, p_off, p_len, t_off, t_len)
+
+
 def pack2bits(ps):
     """2-bit pack every sequence of a PairSet (A0 C1 G2 T3, LSB-first, 16 bases
     per 32-bit word; the byte order equals the reference's 4-per-byte packing,
