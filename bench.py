@@ -367,19 +367,114 @@ def run_gpu(args):
         torch.distributed.destroy_process_group()
 
 
+SERVE = ("serving: open-loop Poisson arrivals, request mix 70% 150 bp at 2%, 25% log-uniform "
+         "1-10 kbp at 8%, 5% 50 kbp at 10% edits, gap-affine 0,4,6,2, CIGAR; high-memory "
+         "end-to-end, BiWFA above a 256 MiB predicted footprint")
+
+
+def run_serve(args):
+    """Open-loop serving sweep: requests arrive as a Poisson process at each
+    rate; latency is submit -> result ready (the server's clock); throughput
+    is requests completed over the span from the first arrival to the last
+    result.  Rank 0 only (one server per GPU)."""
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    import torch
+    torch.cuda.set_device(local)
+    pkg = load_pkg()
+    from wfa_b200 import synth
+    rates = [float(x) for x in args.rates.split(",")]
+    per_rate = args.pairs
+    srv = pkg.Server(pkg.GAP_AFFINE, PEN, device=local, workers=args.workers,
+                     short_workers=args.workers, biwfa_workers=args.workers,
+                     max_batch_bytes=16 << 30)
+    # Warm-up: a few requests of each kind.
+    wps, _ = synth.config5(64, synth.SEED_BASE + 55)
+    for i in range(len(wps)):
+        srv.submit(*wps.pair(i))
+    left = len(wps)
+    while left:
+        left -= len(srv.poll(timeout_ms=500))
+    table = []
+    for j, lam in enumerate(rates):
+        ps, kind = synth.config5(per_rate, synth.SEED_BASE + 5 + 1000 * j)
+        reqs = [ps.pair(i) for i in range(len(ps))]
+        rng = np.random.default_rng(j)
+        arrive = np.cumsum(rng.exponential(1.0 / lam, len(reqs)))
+        recs = {}
+        stop = threading.Event()
+
+        def poller():
+            while True:
+                for r in srv.poll(timeout_ms=50):
+                    recs[r["id"]] = (r, time.perf_counter())
+                if stop.is_set() and len(recs) >= len(reqs):
+                    break
+
+        th = threading.Thread(target=poller, daemon=True)
+        th.start()
+        ids = []
+        t0 = time.perf_counter()
+        with ClockSampler(local) as clk:
+            for i, (p, t) in enumerate(reqs):
+                wait = t0 + arrive[i] - time.perf_counter()
+                if wait > 0:
+                    time.sleep(wait)
+                ids.append(srv.submit(p, t))
+            stop.set()
+            th.join()
+        t_end = max(v[1] for v in recs.values())
+        lat = np.array([recs[i][0]["latency_ns"] for i in ids]) / 1e6
+        kinds = np.asarray(kind)
+        bad = [i for i in ids if recs[i][0]["status"] < 0]
+        assert not bad, f"requests failed: {srv.last_error()}"
+        pct = lambda q, sel: float(np.percentile(lat[sel], q)) if np.any(sel) else None
+        row = {"rate_req_s": lam, "requests": len(reqs),
+               "throughput_req_s": len(reqs) / (t_end - t0),
+               "p50_ms": pct(50, kinds >= 0), "p99_ms": pct(99, kinds >= 0),
+               "p50_ms_by_kind": [pct(50, kinds == k) for k in range(3)],
+               "p99_ms_by_kind": [pct(99, kinds == k) for k in range(3)],
+               "biwfa_requests": int(sum(recs[i][0]["mode"] for i in ids)),
+               "clocks": clk.summary()}
+        table.append(row)
+    srv.stop()
+    best = max(table, key=lambda r: r["throughput_req_s"])
+    line = {"metric": METRIC, "value": best["throughput_req_s"], "unit": "requests/s",
+            "n_gpus": 1, "steps": len(rates), "warmup": 1, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)",
+            "config": {"workload": SERVE, "requests_per_rate": per_rate,
+                       "workers_per_lane": args.workers, "lanes": "short (n+m<=1024), long, BiWFA",
+                       "form": "wfa_server_* continuous batching, host request buffers"},
+            "p50_ms": best["p50_ms"], "p99_ms": best["p99_ms"], "sweep": table}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="shortread", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="shortread", choices=sorted(WORKLOADS) + ["serve"])
+    ap.add_argument("--rates", default="50,200,800", help="serve: arrival rates (requests/s)")
+    ap.add_argument("--workers", type=int, default=2, help="serve: workers per lane")
     ap.add_argument("--pairs", type=int, default=None)
     ap.add_argument("--plain-pairs", type=int, default=None)
     ap.add_argument("--cpu-sample", type=int, default=None)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer and plain forms")
     args = ap.parse_args()
+    if args.workload == "serve":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "the serving sweep measures the GPU request loop; the CPU arm is "
+                              "timed on the batch workloads"}), flush=True)
+            return
+        args.pairs = 1000 if args.pairs is None else args.pairs
+        args.steps = 3 if args.steps is None else args.steps
+        run_serve(args)
+        return
     # Defaults per workload: pairs, plain per-call sample, CPU sample (about
     # 10-30 s of CPU work on a 16-core host).
     pairs, plain, cpu, steps = {"shortread": (1_000_000, 2000, 1_000_000, 40),

@@ -208,9 +208,11 @@ WFA_API int wfa_batch_align(wfa_aligner_t* h, const wfa_batch_t* batch, wfa_resu
                     uint8_t* cigars);
 
 /* Device-buffer batch: every pointer of `batch`, `results` and `cigars` is
- * device memory; the work is enqueued on `stream` (a cudaStream_t, 0 for the
- * default stream) and the call returns without waiting.  Scratch memory is
- * owned by the handle and reused across calls. */
+ * device memory; the work runs on `stream` (a cudaStream_t, 0 for the
+ * handle's own stream).  The call synchronises that stream to read the
+ * longest pair and the number of pairs to re-run with more scratch, so the
+ * results are complete when it returns.  Scratch memory is owned by the
+ * handle and reused across calls. */
 WFA_API int wfa_batch_align_device(wfa_aligner_t* h, const wfa_batch_t* batch, wfa_result_t* results,
                            uint8_t* cigars, void* stream);
 
@@ -245,6 +247,78 @@ WFA_API int wfa_batch_align_device(wfa_aligner_t* h, const wfa_batch_t* batch, w
 #define WFA_NOALLOC_MAX_LEN_SUM 4096
 WFA_API int wfa_batch_align_device_noalloc(wfa_aligner_t* h, const wfa_batch_t* batch,
                                            wfa_result_t* results, uint8_t* cigars, void* stream);
+
+/* ---- serving: continuous batching of single requests ------------------------
+ * No counterpart in the reference (its aligner is one pair per call): a
+ * request loop in front of the batched kernels.  Requests are submitted one
+ * at a time from any thread and sorted into three lanes: short (n + m up to
+ * `short_max_len`), long high-memory and BiWFA.  Each lane has its own
+ * workers, each worker its own aligner handle, stream and buffers, so
+ * several batches are on the GPU at once and a short request never waits
+ * behind a long batch.  A worker that frees up takes every waiting request
+ * of its lane that fits into its next batch, so a request arriving while
+ * others are on the GPU joins the next free batch instead of waiting for
+ * the whole queue.
+ *
+ * Admission is by predicted wavefront memory: a request's high-memory
+ * footprint is taken as (n + m)^2 / 4 bytes (M history of O(s^2) cells with
+ * s about (n + m) / 4) and its BiWFA footprint as O(n + m).  A request whose
+ * high-memory estimate is above `biwfa_above_bytes` runs in BiWFA; a batch
+ * takes requests in arrival order while the sum of their estimates stays
+ * within `max_batch_bytes` (a request larger than that alone gets a batch
+ * of its own).  The mode of a request depends only on its lengths and the
+ * configuration, never on the load, so a request gets the same result alone
+ * or in a mix (the result of align_end2end, or of align_biwfa, with the
+ * server's metric, penalties and scope). */
+typedef struct {
+  int32_t metric;               /* wfa_metric_t */
+  wfa_penalties_t penalties;
+  int32_t device;
+  int32_t score_only;           /* 1: alignment scope score only */
+  int32_t workers;              /* long high-memory lane workers (default 2) */
+  int32_t max_batch_pairs;      /* per batch (default 65536) */
+  int64_t max_batch_bytes;      /* predicted wavefront bytes per batch (default 4 GiB) */
+  int64_t biwfa_above_bytes;    /* BiWFA above this estimate (default 256 MiB) */
+  int32_t short_workers;        /* short lane workers (default 2) */
+  int32_t biwfa_workers;        /* BiWFA lane workers (default 2) */
+  int32_t short_max_len;        /* n + m of the short lane (default 1024) */
+  int32_t reserved;
+} wfa_server_config_t;
+
+typedef struct wfa_server wfa_server_t;
+
+typedef struct {
+  int64_t id;            /* as returned by wfa_server_submit */
+  int32_t score;         /* what align_end2end / align_biwfa returns */
+  int32_t status;        /* wfa_status_t, or the batch's error code (< 0) */
+  int32_t cigar_length;  /* ops at cigars[cigar_offset] of the poll buffer */
+  int32_t cigar_score;
+  int32_t end_v, end_h;
+  int32_t mode;          /* 0 high memory (end-to-end), 1 BiWFA */
+  int32_t pad;
+  int64_t cigar_offset;
+  int64_t latency_ns;    /* submit to result ready */
+} wfa_served_t;
+
+/* Starts the workers; NULL on error (*err set). */
+WFA_API wfa_server_t* wfa_server_start(const wfa_server_config_t* config, int* err);
+/* Queues one pair (copied); returns its id (>= 0) or a negative error code.
+ * Thread-safe. */
+WFA_API int64_t wfa_server_submit(wfa_server_t* s, const uint8_t* pattern, int32_t pattern_length,
+                                  const uint8_t* text, int32_t text_length);
+/* Moves up to `max` finished requests into `out` (their CIGAR ops densely
+ * into `cigars`, at most cigar_cap bytes), waiting up to timeout_ms for the
+ * first one.  Returns the count (0 on timeout) or a negative error code.
+ * Thread-safe. */
+WFA_API int32_t wfa_server_poll(wfa_server_t* s, wfa_served_t* out, int32_t max, uint8_t* cigars,
+                                int64_t cigar_cap, int32_t timeout_ms);
+/* Message of the last batch that failed (its requests carry the error code
+ * as their status); "" if none.  Valid until the next failure. */
+WFA_API const char* wfa_server_last_error(wfa_server_t* s);
+/* Requests submitted and not yet polled. */
+WFA_API int64_t wfa_server_pending(wfa_server_t* s);
+/* Finishes the queued requests, stops the workers and frees the server. */
+WFA_API int wfa_server_stop(wfa_server_t* s);
 
 /* Number of the library's own kernel launches issued so far by this handle. */
 WFA_API int64_t wfa_kernel_launches(const wfa_aligner_t* h);

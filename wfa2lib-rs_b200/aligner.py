@@ -50,6 +50,23 @@ class Batch(ctypes.Structure):
                 ("cigar_off", ctypes.c_void_p), ("cigar_bytes", ctypes.c_int64)]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("metric", ctypes.c_int32), ("penalties", Penalties), ("device", ctypes.c_int32),
+                ("score_only", ctypes.c_int32), ("workers", ctypes.c_int32),
+                ("max_batch_pairs", ctypes.c_int32), ("max_batch_bytes", ctypes.c_int64),
+                ("biwfa_above_bytes", ctypes.c_int64), ("short_workers", ctypes.c_int32),
+                ("biwfa_workers", ctypes.c_int32), ("short_max_len", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
+
+
+class Served(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_int64), ("score", ctypes.c_int32), ("status", ctypes.c_int32),
+                ("cigar_length", ctypes.c_int32), ("cigar_score", ctypes.c_int32),
+                ("end_v", ctypes.c_int32), ("end_h", ctypes.c_int32), ("mode", ctypes.c_int32),
+                ("pad", ctypes.c_int32), ("cigar_offset", ctypes.c_int64),
+                ("latency_ns", ctypes.c_int64)]
+
+
 _lib = None
 
 
@@ -85,6 +102,12 @@ def lib():
         "wfa_batch_align": (ctypes.c_int, [vp, ctypes.POINTER(Batch), vp, vp]),
         "wfa_batch_align_device": (ctypes.c_int, [vp, ctypes.POINTER(Batch), vp, vp, vp]),
         "wfa_batch_align_device_noalloc": (ctypes.c_int, [vp, ctypes.POINTER(Batch), vp, vp, vp]),
+        "wfa_server_start": (vp, [ctypes.POINTER(ServerConfig), ctypes.POINTER(ctypes.c_int)]),
+        "wfa_server_submit": (i64, [vp, ctypes.c_char_p, i32, ctypes.c_char_p, i32]),
+        "wfa_server_poll": (i32, [vp, ctypes.POINTER(Served), i32, vp, i64, i32]),
+        "wfa_server_last_error": (ctypes.c_char_p, [vp]),
+        "wfa_server_pending": (i64, [vp]),
+        "wfa_server_stop": (ctypes.c_int, [vp]),
         "wfa_kernel_launches": (i64, [vp]),
         "wfa_last_kernel_ms": (ctypes.c_double, [vp]),
         "wfa_cigar_rle": (i32, [vp, i32, ctypes.c_char_p, i32]),
@@ -285,6 +308,69 @@ class WavefrontAligner:
                   p_off, p_len, t_off, t_len, cigar_off, cigar_bytes)
         return self._check(self._L.wfa_batch_align_device_noalloc(
             self._h, ctypes.byref(b), results_ptr, cigars_ptr, stream))
+
+
+class Server:
+    """Continuous-batching request loop over the GPU (wfa_server_* of the C
+    ABI): submit single pairs from any thread, poll finished ones.  Requests
+    go to a short, a long high-memory or a BiWFA lane; a request runs BiWFA
+    when its predicted high-memory footprint ((n + m)^2 / 4 bytes) exceeds
+    `biwfa_above_bytes`.  Either way its result is that of the plain aligner
+    call in that mode, alone or in any mix."""
+
+    def __init__(self, metric, penalties=None, device=0, score_only=False, workers=2,
+                 max_batch_pairs=65536, max_batch_bytes=4 << 30, biwfa_above_bytes=256 << 20,
+                 short_workers=2, biwfa_workers=2, short_max_len=1024):
+        self._L = lib()
+        cfg = ServerConfig(metric, _pen(metric, penalties), device, int(score_only), workers,
+                           max_batch_pairs, max_batch_bytes, biwfa_above_bytes, short_workers,
+                           biwfa_workers, short_max_len, 0)
+        err = ctypes.c_int(0)
+        self._s = self._L.wfa_server_start(ctypes.byref(cfg), ctypes.byref(err))
+        if not self._s:
+            raise RuntimeError(f"wfa_server_start: {ERRORS.get(err.value, err.value)}")
+        self._recs = (Served * 4096)()
+        self._cig = ctypes.create_string_buffer(64 << 20)
+
+    def submit(self, pattern, text):
+        r = self._L.wfa_server_submit(self._s, pattern, len(pattern), text, len(text))
+        if r < 0:
+            raise RuntimeError(f"wfa_server_submit: {ERRORS.get(r, r)}")
+        return r
+
+    def poll(self, timeout_ms=100, max_records=4096):
+        """Finished requests: list of dicts (id, score, status, cigar bytes,
+        cigar_score, end_v, end_h, mode, latency_ns)."""
+        c = self._L.wfa_server_poll(self._s, self._recs, min(max_records, 4096), self._cig,
+                                    len(self._cig), timeout_ms)
+        if c < 0:
+            raise RuntimeError(f"wfa_server_poll: {ERRORS.get(c, c)}")
+        out = []
+        raw = self._cig.raw
+        for i in range(c):
+            r = self._recs[i]
+            cig = raw[r.cigar_offset:r.cigar_offset + r.cigar_length] if r.cigar_offset >= 0 else b""
+            out.append({"id": r.id, "score": r.score, "status": r.status, "cigar": cig,
+                        "cigar_score": r.cigar_score, "end_v": r.end_v, "end_h": r.end_h,
+                        "mode": r.mode, "latency_ns": r.latency_ns})
+        return out
+
+    def pending(self):
+        return self._L.wfa_server_pending(self._s)
+
+    def last_error(self):
+        return self._L.wfa_server_last_error(self._s).decode()
+
+    def stop(self):
+        if self._s:
+            self._L.wfa_server_stop(self._s)
+            self._s = None
+
+    def __del__(self):
+        try:
+            self.stop()
+        except Exception:
+            pass
 
 
 def cigar_rle(ops):

@@ -5,6 +5,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include "wfa_biwfa.cuh"
 #include "wfa_kernels.h"
 
@@ -75,11 +77,17 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) biwfa_kernel(const Ali
 template <int CLS, int ENC, bool GEN>
 static cudaError_t launch_bi_t(const AlignParams& P, int blocks, size_t smem, cudaStream_t st) {
   auto k = biwfa_kernel<CLS, ENC, GEN>;
+  // Dynamic shared memory already allowed for k; only ever raised, under a
+  // lock (handles on several host threads launch the same kernels).
   static size_t configured = 0;
-  if (smem > configured) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    configured = smem;
+  static std::mutex mu;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if (smem > configured) {
+      cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      configured = smem;
+    }
   }
   k<<<blocks, kWarpsPerBlock * 32, smem, st>>>(P);
   return cudaGetLastError();

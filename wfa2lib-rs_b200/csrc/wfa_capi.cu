@@ -270,7 +270,8 @@ static int launch_round(wfa_aligner_t* h, AlignParams& P, const Round& r, int64_
   P.num_pairs = todo;
   CUDA_TRY(h, cudaMemsetAsync(P.work_counter, 0, 16, st), "memset");
   CUDA_TRY(h, cudaEventRecord(h->ev0, st), "event");
-  CUDA_TRY(h, launch_unialign(P, cls, blocks, smem, st), "kernel launch");
+  CUDA_TRY(h, cudaGetLastError(), "an earlier CUDA call of this thread");
+  CUDA_TRY(h, launch_unialign(P, cls, blocks, smem, st), "alignment kernel launch");
   CUDA_TRY(h, cudaEventRecord(h->ev1, st), "event");
   h->launches++;
   return WFA_OK;
@@ -398,7 +399,8 @@ static int run_biwfa_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t*
     P.num_pairs = todo;
     CUDA_TRY(h, cudaMemsetAsync(P.work_counter, 0, 16, st), "memset");
     CUDA_TRY(h, cudaEventRecord(h->ev0, st), "event");
-    CUDA_TRY(h, launch_biwfa(P, cls, blocks, smem, st), "kernel launch");
+    CUDA_TRY(h, cudaGetLastError(), "an earlier CUDA call of this thread");
+    CUDA_TRY(h, launch_biwfa(P, cls, blocks, smem, st), "BiWFA kernel launch");
     CUDA_TRY(h, cudaEventRecord(h->ev1, st), "event");
     h->launches++;
     int32_t retries = 0;

@@ -9,6 +9,8 @@
 // of the scratch buffer, as does the M history of CIGAR mode.
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include "wfa_align.cuh"
 #include "wfa_kernels.h"
 
@@ -84,15 +86,29 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (min_blocks<CLS, GEN>()))
   }
 }
 
+// Allows the kernel `smem` bytes of dynamic shared memory.  The allowance
+// is only ever raised, under a lock: handles on several host threads launch
+// the same kernels, and lowering it under another thread's launch would make
+// that launch fail.
 template <int CLS, int ENC, bool GEN>
-static cudaError_t launch_t(const AlignParams& P, int blocks, size_t smem, cudaStream_t st) {
-  auto k = unialign_kernel<CLS, ENC, GEN>;
-  static size_t configured = 0;  // dynamic shared memory already allowed for k
+static cudaError_t allow_smem(size_t smem) {
+  static size_t configured = 0;
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lock(mu);
   if (smem > configured) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(unialign_kernel<CLS, ENC, GEN>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     configured = smem;
   }
+  return cudaSuccess;
+}
+
+template <int CLS, int ENC, bool GEN>
+static cudaError_t launch_t(const AlignParams& P, int blocks, size_t smem, cudaStream_t st) {
+  auto k = unialign_kernel<CLS, ENC, GEN>;
+  cudaError_t e = allow_smem<CLS, ENC, GEN>(smem);
+  if (e != cudaSuccess) return e;
   k<<<blocks, kWarpsPerBlock * 32, smem, st>>>(P);
   return cudaGetLastError();
 }
@@ -127,9 +143,11 @@ template <int CLS, int ENC, bool GEN>
 static int occ_t(size_t smem) {
   int nb = 0;
   auto k = unialign_kernel<CLS, ENC, GEN>;
-  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, kWarpsPerBlock * 32, smem) != cudaSuccess)
+  if (allow_smem<CLS, ENC, GEN>(smem) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, kWarpsPerBlock * 32, smem) != cudaSuccess) {
+    cudaGetLastError();
     nb = 1;
+  }
   return nb < 1 ? 1 : nb;
 }
 

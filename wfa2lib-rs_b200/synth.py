@@ -97,6 +97,29 @@ def uniform_pairs(num, len_lo, len_hi, rate_lo, rate_hi, seed):
     return _interleave(patterns, p_len, texts, t_len)
 
 
+def pairs_with_lengths(p_len, rate, seed):
+    """Patterns of the given lengths, texts by the per-position model at
+    per-pair edit rates `rate`."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    p_len = np.asarray(p_len, dtype=np.int32)
+    patterns = ACGT[rng.integers(0, 4, int(p_len.sum()))]
+    texts, t_len = _mutate(rng, patterns, p_len, np.asarray(rate, dtype=np.float64))
+    return _interleave(patterns, p_len, texts, t_len)
+
+
+def config5(num, seed=SEED_BASE + 5):
+    """Serving request mix: 70% 150 bp pairs at 2% edits, 25% log-uniform
+    1-10 kbp at 8%, 5% 50 kbp at 10% (the per-position model), in a random
+    arrival order.  Returns (PairSet, kind per request: 0 short, 1 medium,
+    2 long)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    kind = rng.choice(3, size=num, p=[0.70, 0.25, 0.05])
+    p_len = np.where(kind == 0, 150,
+                     np.where(kind == 1, np.exp(rng.uniform(np.log(1000), np.log(10000), num)), 50000))
+    rate = np.choose(kind, [0.02, 0.08, 0.10])
+    return pairs_with_lengths(p_len.astype(np.int32), rate, seed + 1), kind
+
+
 def config1(num=10_000):
     """Plain method, small: n = 100, p = 0.05 (gap-affine 0,4,6,2 end-to-end)."""
     return uniform_pairs(num, 100, 100, 0.05, 0.05, SEED_BASE + 1)
