@@ -23,21 +23,29 @@ using namespace wfab;
 
 namespace {
 
+// A device buffer that grows on demand.  Growing uses stream-ordered
+// allocation on the handle's stream: cudaFree would wait for every kernel on
+// the device (other handles' and other threads' included), while the
+// stream-ordered free waits only for this stream, whose earlier work the
+// callers have already synchronised.
 struct DevBuf {
   void* p = nullptr;
   size_t cap = 0;
+  cudaStream_t st = nullptr;
   cudaError_t ensure(size_t bytes) {
     if (bytes <= cap) return cudaSuccess;
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, st);
     p = nullptr;
     cap = 0;
     size_t want = std::max(bytes, (size_t)256);
-    cudaError_t e = cudaMalloc(&p, want);
+    cudaError_t e = cudaMallocAsync(&p, want, st);
+    // Usable from the handle's other streams once the allocation is done.
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e == cudaSuccess) cap = want;
     return e;
   }
   void release() {
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, st);
     p = nullptr;
     cap = 0;
   }
@@ -87,7 +95,22 @@ struct wfa_aligner {
   int occ_val = 1;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_kernel_ms = 0.0;
+  // Events of the pipelined host-buffer batch, created once and reused:
+  // creating and destroying events waits for work running on the device
+  // (other handles' kernels included).
+  std::vector<cudaEvent_t> evpool;
 };
+
+// At least `count` pooled events in h->evpool.
+static cudaError_t event_pool(wfa_aligner_t* h, size_t count) {
+  while (h->evpool.size() < count) {
+    cudaEvent_t e = nullptr;
+    cudaError_t r = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    if (r != cudaSuccess) return r;
+    h->evpool.push_back(e);
+  }
+  return cudaSuccess;
+}
 
 static int fail(wfa_aligner_t* h, int code, const char* what, cudaError_t e = cudaSuccess) {
   if (h) {
@@ -588,6 +611,14 @@ wfa_aligner_t* wfa_aligner_create(wfa_metric_t metric, const wfa_penalties_t* pe
     if (err) *err = WFA_ERR_CUDA;
     return nullptr;
   }
+  for (DevBuf* b : {&h->seq, &h->poff, &h->plen, &h->toff, &h->tlen, &h->coff, &h->results,
+                    &h->cigars, &h->dense, &h->scratch, &h->counters, &h->pairlist})
+    b->st = h->stream;
+  if (event_pool(h, 32) != cudaSuccess) {
+    wfa_aligner_destroy(h);
+    if (err) *err = WFA_ERR_CUDA;
+    return nullptr;
+  }
   if (err) *err = WFA_OK;
   return h;
 }
@@ -599,9 +630,11 @@ void wfa_aligner_destroy(wfa_aligner_t* h) {
   for (DevBuf* b : {&h->seq, &h->poff, &h->plen, &h->toff, &h->tlen, &h->coff, &h->results,
                     &h->cigars, &h->dense, &h->scratch, &h->counters, &h->pairlist})
     b->release();
+  if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->pinned) cudaFreeHost(h->pinned);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
+  for (cudaEvent_t e : h->evpool) cudaEventDestroy(e);
   if (h->stream) cudaStreamDestroy(h->stream);
   if (h->s_in) cudaStreamDestroy(h->s_in);
   if (h->s_out) cudaStreamDestroy(h->s_out);
@@ -1014,23 +1047,12 @@ int wfa_batch_align(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* result
     CUDA_TRY(h, h->dense.ensure((size_t)slot_total + 16), "dense cigars");
     CUDA_TRY(h, h->pairlist.ensure((size_t)n * 8), "dense offsets");
   }
-  std::vector<cudaEvent_t> ev_in((size_t)nchunks), ev_k((size_t)nchunks), ev_res((size_t)nchunks),
-      ev_off((size_t)nchunks);
-  auto destroy = [&]() {
-    for (auto* v : {&ev_in, &ev_k, &ev_res, &ev_off})
-      for (auto& e : *v)
-        if (e) cudaEventDestroy(e);
-  };
-  for (int64_t ci = 0; ci < nchunks; ++ci) {
-    for (auto* v : {&ev_in, &ev_k, &ev_res, &ev_off}) {
-      cudaEvent_t e = nullptr;
-      if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
-        destroy();
-        return fail(h, WFA_ERR_CUDA, "event");
-      }
-      (*v)[(size_t)ci] = e;
-    }
-  }
+  CUDA_TRY(h, event_pool(h, 4 * (size_t)nchunks), "events");
+  cudaEvent_t* ev_in = h->evpool.data();
+  cudaEvent_t* ev_k = ev_in + nchunks;
+  cudaEvent_t* ev_res = ev_k + nchunks;
+  cudaEvent_t* ev_off = ev_res + nchunks;
+  auto destroy = []() {};  // the events stay in the handle's pool
   uint8_t* dseq = h->seq.as<uint8_t>();
   int64_t *dpo = h->poff.as<int64_t>(), *dto = h->toff.as<int64_t>();
   int32_t *dpl = h->plen.as<int32_t>(), *dtl = h->tlen.as<int32_t>();
@@ -1131,6 +1153,7 @@ int wfa_batch_align(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* result
       rslot += 2 * ((int64_t)pl[j] + tl[j]) + 1;
     }
     DevBuf rbuf;
+    rbuf.st = sc;
     size_t need = (size_t)rn * (8 * 3 + 4 * 2 + sizeof(wfa_result_t)) + (size_t)rslot + 64;
     CUDA_TRY(h, rbuf.ensure(need), "retry buffers");
     char* base = rbuf.as<char>();
