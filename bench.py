@@ -65,7 +65,7 @@ WORKLOADS = {
 }
 
 
-def make_workload(num_pairs, rank, kind="short", packed=True):
+def make_workload(num_pairs, rank, kind="short", packed=True, length_range=None):
     """(pkg, synth, pairs, sequence buffer, pattern offsets, text offsets) in
     the batch layout: 2-bit words and word offsets, or bytes and byte offsets."""
     pkg = load_pkg()
@@ -78,6 +78,13 @@ def make_workload(num_pairs, rank, kind="short", packed=True):
         ps = synth.config4(num_pairs, synth.SEED_BASE + 4 + 1000 * rank)
     else:
         ps = synth.config3(num_pairs, synth.SEED_BASE + 3 + 1000 * rank)
+    if length_range:
+        # Only the pairs of one pattern-length class, drawn from a pool eight
+        # times larger (for profiling one class on a capture-sized case).
+        lo, hi = length_range
+        pool = synth.config3(8 * num_pairs, synth.SEED_BASE + 3 + 1000 * rank) if kind == "long" else ps
+        keep = np.where((pool.p_len >= lo) & (pool.p_len <= hi))[0][:num_pairs]
+        ps = pool.subset(keep)
     if not packed:
         return pkg, synth, ps, np.concatenate([ps.buf, np.zeros(16, np.uint8)]), ps.p_off, ps.t_off
     words, pwo, two = synth.pack2bits(ps)
@@ -217,7 +224,8 @@ def run_gpu(args):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     desc, kind, metric, pen, span, omode, heur, packed = WORKLOADS[args.workload]
-    pkg, synth, ps, words, pwo, two = make_workload(args.pairs, rank, kind, packed)
+    pkg, synth, ps, words, pwo, two = make_workload(args.pairs, rank, kind, packed,
+                                                    args.length_range)
     n = len(ps)
     a = pkg.WavefrontAligner(metric, pen, device=local)
     a.set_alignment_scope(True)
@@ -458,6 +466,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="shortread", choices=sorted(WORKLOADS) + ["serve"])
     ap.add_argument("--rates", default="50,200,800", help="serve: arrival rates (requests/s)")
+    ap.add_argument("--length-range", default=None,
+                    type=lambda s: tuple(int(x) for x in s.split(",")),
+                    help="lo,hi: keep only pairs with pattern length in [lo, hi] (profiling)")
     ap.add_argument("--workers", type=int, default=2, help="serve: workers per lane")
     ap.add_argument("--pairs", type=int, default=None)
     ap.add_argument("--plain-pairs", type=int, default=None)
