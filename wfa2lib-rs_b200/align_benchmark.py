@@ -176,7 +176,7 @@ def main(argv=None):
                         f"(P0<=|P|,Pf<=|P|,T0<=|T|,Tf<=|T|) where (|P|,|T|)=({len(p)},{len(t)})")
                 a.set_alignment_free_ends(*ends)
                 s = a.align_endsfree(p, t)
-                es, ek, eo = a.alignment_end_pos()
+                es, ek, eo = a.alignment_end_pos
                 rec = {"score": s, "status": a.status(), "end_score": es, "end_k": ek, "end_offset": eo}
                 ops = "" if score_only else a.cigar().operations.decode()
                 lines.append(cli_format.line(metric, orig, score_only, False, rec, ops, len(p), len(t)))
