@@ -216,6 +216,20 @@ WFA_API int wfa_batch_align(wfa_aligner_t* h, const wfa_batch_t* batch, wfa_resu
 WFA_API int wfa_batch_align_device(wfa_aligner_t* h, const wfa_batch_t* batch, wfa_result_t* results,
                            uint8_t* cigars, void* stream);
 
+/* Asynchronous host-buffer batch: queues the batch of wfa_batch_align and
+ * returns a ticket (>= 0) at once.  The batch's arrays, `results` and
+ * `cigars` are the caller's and must stay valid and untouched until the
+ * ticket completes.  A handle's batches run one after another, in
+ * submission order, on a worker thread the first submit starts; while
+ * tickets are outstanding, use no other call of the handle.
+ * wfa_batch_poll returns 1 (and the batch's return code in *status) once the
+ * ticket is done, 0 before; wfa_batch_wait blocks until then and returns that
+ * code.  A completed ticket is reported once. */
+WFA_API int64_t wfa_batch_submit(wfa_aligner_t* h, const wfa_batch_t* batch, wfa_result_t* results,
+                                 uint8_t* cigars);
+WFA_API int wfa_batch_poll(wfa_aligner_t* h, int64_t ticket, int* status);
+WFA_API int wfa_batch_wait(wfa_aligner_t* h, int64_t ticket);
+
 /* ---- device-buffer batch that allocates nothing -----------------------------
  * No counterpart in the reference: an addition of this library.
  *

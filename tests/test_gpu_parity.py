@@ -250,3 +250,24 @@ def test_device_api_matches_host_api(pkg):
         a_ops = cd[coff[i] + rd["cigar_begin"][i]: coff[i] + rd["cigar_begin"][i] + rd["cigar_length"][i]]
         b_ops = cig_h[res_h["cigar_begin"][i]: res_h["cigar_begin"][i] + res_h["cigar_length"][i]]
         assert a_ops.tobytes() == b_ops.tobytes(), i
+
+
+def test_async_batches_match_the_blocking_call(pkg):
+    """wfa_batch_submit / poll / wait: three batches queued at once give the
+    results of wfa_batch_align, in order."""
+    from wfa_b200 import synth
+    a = pkg.WavefrontAligner(3, [0, 4, 6, 2])
+    a.set_alignment_scope(True)
+    sets = [synth.uniform_pairs(3000, 100, 150, 0.0, 0.04, 500 + i) for i in range(3)]
+    tickets = [a.submit_batch(ps.buf, ps.p_off, ps.p_len, ps.t_off, ps.t_len) for ps in sets]
+    import time
+    t0 = time.time()
+    while not a.poll_batch(tickets[0]):
+        assert time.time() - t0 < 120
+        time.sleep(0.001)
+    got = [a.wait_batch(t) for t in tickets]
+    for ps, (res, cig) in zip(sets, got):
+        ref_res, ref_cig = a.align_batch(ps.buf, ps.p_off, ps.p_len, ps.t_off, ps.t_len)
+        assert np.array_equal(res, ref_res)
+        assert cig[:int(res["cigar_length"].sum())].tobytes() == ref_cig[:int(ref_res["cigar_length"].sum())].tobytes()
+    a.close()

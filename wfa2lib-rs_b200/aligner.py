@@ -101,6 +101,9 @@ def lib():
         "wfa_last_error_string": (ctypes.c_char_p, [vp]),
         "wfa_batch_align": (ctypes.c_int, [vp, ctypes.POINTER(Batch), vp, vp]),
         "wfa_batch_align_device": (ctypes.c_int, [vp, ctypes.POINTER(Batch), vp, vp, vp]),
+        "wfa_batch_submit": (i64, [vp, ctypes.POINTER(Batch), vp, vp]),
+        "wfa_batch_poll": (ctypes.c_int, [vp, i64, ctypes.POINTER(ctypes.c_int)]),
+        "wfa_batch_wait": (ctypes.c_int, [vp, i64]),
         "wfa_batch_align_device_noalloc": (ctypes.c_int, [vp, ctypes.POINTER(Batch), vp, vp, vp]),
         "wfa_server_start": (vp, [ctypes.POINTER(ServerConfig), ctypes.POINTER(ctypes.c_int)]),
         "wfa_server_submit": (i64, [vp, ctypes.c_char_p, i32, ctypes.c_char_p, i32]),
@@ -286,6 +289,43 @@ class WavefrontAligner:
         self._check(self._L.wfa_batch_align(self._h, ctypes.byref(b), res.ctypes.data,
                                             cig.ctypes.data))
         return res, cig
+
+    def submit_batch(self, seq, p_off, p_len, t_off, t_len, packed=False, span=SPAN_END2END):
+        """align_batch without waiting: returns a ticket; wait_batch(ticket)
+        returns (results, dense CIGAR bytes) as align_batch does."""
+        n = len(p_len)
+        seq = np.ascontiguousarray(seq).view(np.uint8)
+        arrs = [np.ascontiguousarray(x, dtype=d) for x, d in
+                ((p_off, np.int64), (p_len, np.int32), (t_off, np.int64), (t_len, np.int32))]
+        res = np.zeros(n, RESULT_DTYPE)
+        caps = 2 * (arrs[1].astype(np.int64) + arrs[3]) + 1
+        cig = np.zeros(int(caps.sum()) + 16, np.uint8)
+        b = Batch(SEQ_PACKED2 if packed else SEQ_ASCII, span, n, seq.ctypes.data, seq.nbytes,
+                  arrs[0].ctypes.data, arrs[1].ctypes.data, arrs[2].ctypes.data,
+                  arrs[3].ctypes.data, None, 0)
+        t = self._L.wfa_batch_submit(self._h, ctypes.byref(b), res.ctypes.data, cig.ctypes.data)
+        self._check(t)
+        if not hasattr(self, "_pending"):
+            self._pending = {}
+        self._pending[t] = (seq, arrs, res, cig)  # alive until the batch is done
+        return t
+
+    def poll_batch(self, ticket):
+        """True once the ticket's batch is done (then wait_batch returns at once)."""
+        st = ctypes.c_int(0)
+        r = self._L.wfa_batch_poll(self._h, ticket, ctypes.byref(st))
+        self._check(r)
+        if r == 1:
+            self._check(st.value)
+            self._pending[ticket] = self._pending[ticket][2:] + ("done",)
+        return r == 1
+
+    def wait_batch(self, ticket):
+        p = self._pending.pop(ticket)
+        if len(p) == 3:  # already reported done by poll_batch
+            return p[0], p[1]
+        self._check(self._L.wfa_batch_wait(self._h, ticket))
+        return p[2], p[3]
 
     def align_batch_device(self, seq_ptr, seq_bytes, p_off, p_len, t_off, t_len, num_pairs,
                            results_ptr, cigars_ptr=None, cigar_off=None, cigar_bytes=0,

@@ -9,9 +9,14 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "wfa_common.h"
@@ -99,6 +104,21 @@ struct wfa_aligner {
   // creating and destroying events waits for work running on the device
   // (other handles' kernels included).
   std::vector<cudaEvent_t> evpool;
+  // Asynchronous host-buffer batches (wfa_batch_submit): one worker thread,
+  // started by the first submit, runs them in submission order.
+  struct Job {
+    int64_t ticket;
+    wfa_batch_t batch;
+    wfa_result_t* results;
+    uint8_t* cigars;
+  };
+  std::thread async_worker;
+  std::mutex async_mu;
+  std::condition_variable async_cv;
+  std::deque<Job> async_jobs;
+  std::map<int64_t, int> async_done;  // ticket -> return code
+  int64_t async_next = 0;
+  bool async_stop = false;
 };
 
 // At least `count` pooled events in h->evpool.
@@ -625,6 +645,14 @@ wfa_aligner_t* wfa_aligner_create(wfa_metric_t metric, const wfa_penalties_t* pe
 
 void wfa_aligner_destroy(wfa_aligner_t* h) {
   if (!h) return;
+  if (h->async_worker.joinable()) {  // finish the submitted batches first
+    {
+      std::lock_guard<std::mutex> lock(h->async_mu);
+      h->async_stop = true;
+    }
+    h->async_cv.notify_all();
+    h->async_worker.join();
+  }
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   for (DevBuf* b : {&h->seq, &h->poff, &h->plen, &h->toff, &h->tlen, &h->coff, &h->results,
@@ -1201,6 +1229,58 @@ int wfa_batch_align(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* result
     }
   }
   return WFA_OK;
+}
+
+static void async_loop(wfa_aligner_t* h) {
+  cudaSetDevice(h->device);
+  for (;;) {
+    wfa_aligner_t::Job job;
+    {
+      std::unique_lock<std::mutex> lock(h->async_mu);
+      h->async_cv.wait(lock, [&] { return h->async_stop || !h->async_jobs.empty(); });
+      if (h->async_jobs.empty()) return;
+      job = h->async_jobs.front();
+      h->async_jobs.pop_front();
+    }
+    const int rc = wfa_batch_align(h, &job.batch, job.results, job.cigars);
+    {
+      std::lock_guard<std::mutex> lock(h->async_mu);
+      h->async_done[job.ticket] = rc;
+    }
+    h->async_cv.notify_all();
+  }
+}
+
+int64_t wfa_batch_submit(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* results,
+                         uint8_t* cigars) {
+  if (!h || !b || !results) return WFA_ERR_ARGUMENT;
+  std::lock_guard<std::mutex> lock(h->async_mu);
+  if (h->async_stop) return WFA_ERR_ARGUMENT;
+  if (!h->async_worker.joinable()) h->async_worker = std::thread(async_loop, h);
+  const int64_t t = h->async_next++;
+  h->async_jobs.push_back(wfa_aligner_t::Job{t, *b, results, cigars});
+  h->async_cv.notify_all();
+  return t;
+}
+
+int wfa_batch_poll(wfa_aligner_t* h, int64_t ticket, int* status) {
+  if (!h || ticket < 0) return WFA_ERR_ARGUMENT;
+  std::lock_guard<std::mutex> lock(h->async_mu);
+  auto it = h->async_done.find(ticket);
+  if (it == h->async_done.end()) return ticket < h->async_next ? 0 : WFA_ERR_ARGUMENT;
+  if (status) *status = it->second;
+  h->async_done.erase(it);
+  return 1;
+}
+
+int wfa_batch_wait(wfa_aligner_t* h, int64_t ticket) {
+  if (!h || ticket < 0) return WFA_ERR_ARGUMENT;
+  std::unique_lock<std::mutex> lock(h->async_mu);
+  if (ticket >= h->async_next) return WFA_ERR_ARGUMENT;
+  h->async_cv.wait(lock, [&] { return h->async_done.count(ticket) > 0; });
+  const int rc = h->async_done[ticket];
+  h->async_done.erase(ticket);
+  return rc;
 }
 
 int32_t wfa_cigar_rle(const uint8_t* ops, int32_t len, char* out, int32_t cap) {
