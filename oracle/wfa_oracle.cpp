@@ -12,7 +12,7 @@
 // reference never initialised aborts (poisoned memory).
 //
 // Not restated here (out of the hot path or later rows): lambda sequences
-// (host callback), Compat::Corrected, med/low piggyback backtrace.
+// (host callback), Compat::Corrected.
 
 #include "wfa_oracle.h"
 
@@ -316,6 +316,18 @@ struct Wavefront {
   int32_t base_k = 0, alloc = 0;
   int32_t lo = 1, hi = -1, init_min = 0, init_max = 0;
   bool null = false;
+  // Med/low (piggyback) bookkeeping, src/wavefront.rs:359-415: the range of
+  // cells whose backtrace was written since init (a union range, as the
+  // reference keeps it) and the begin-free seeds placed in this wavefront.
+  int32_t wr_lo = 1, wr_hi = 0;
+  std::vector<int32_t> seeds;
+  void mark_written(int32_t l, int32_t h) {
+    if (l > h) return;
+    if (wr_lo > wr_hi) { wr_lo = l; wr_hi = h; }
+    else { wr_lo = std::min(wr_lo, l); wr_hi = std::max(wr_hi, h); }
+  }
+  bool written(int32_t k) const { return k >= wr_lo && k <= wr_hi; }
+  bool is_seed(int32_t k) const { return std::find(seeds.begin(), seeds.end(), k) != seeds.end(); }
 
   bool allocated(int32_t k) const { return k >= base_k && k < base_k + alloc; }
   int32_t get(int32_t k) const {
@@ -341,14 +353,18 @@ struct Wavefront {
   }
   void init(int32_t min_lo, int32_t /*max_hi*/) {  // :307
     null = false; lo = 1; hi = -1; base_k = min_lo; init_min = 0; init_max = 0;
+    wr_lo = 1; wr_hi = 0; seeds.clear();
   }
   void init_null(int32_t min_lo, int32_t max_hi) {  // :331
-    null = true; lo = 1; hi = -1; base_k = min_lo;
+    null = true; lo = 1; hi = -1; base_k = min_lo; wr_lo = 1; wr_hi = 0; seeds.clear();
     for (int32_t i = 0; i < max_hi - min_lo + 1; ++i) mem[(size_t)i] = OFFSET_NULL;
     init_min = min_lo; init_max = max_hi;
   }
   void init_victim(int32_t min_lo, int32_t max_hi) { init(min_lo, max_hi); null = true; }
-  void set_limits(int32_t l, int32_t h) { lo = l; hi = h; init_min = l; init_max = h; }  // :360
+  void set_limits(int32_t l, int32_t h) {  // :360
+    lo = l; hi = h; init_min = l; init_max = h;
+    mark_written(l, h);
+  }
   void clear_init_range() { init_min = lo; init_max = hi; }  // :375
   void set_null_cell_if_allocated(int32_t k) { if (allocated(k)) set(k, OFFSET_NULL); }  // :405
   void init_ends_lower(int32_t min_lo) {  // :422
@@ -627,6 +643,16 @@ struct Components {
     return modular ? (size_t)((uint32_t)score % (uint32_t)scope) : (size_t)score;
   }
   bool has_slot(int32_t score) const { return modular || (size_t)score < num_wavefronts; }
+  // Med/low keep every score here (the reference's modular components have
+  // no score cap): the arrays grow on demand.
+  bool grow = false;
+  bool make_slot(int32_t score) {
+    if (grow && !modular && (size_t)score >= num_wavefronts) {
+      num_wavefronts = std::max(2 * num_wavefronts, (size_t)score + 1);
+      for (auto& a : arr) a.resize(num_wavefronts, nullptr);
+    }
+    return has_slot(score);
+  }
   Wavefront* get(int c, int32_t score) const { return arr[c][slot(score)]; }
   void set(int c, int32_t score, Wavefront* w) { arr[c][slot(score)] = w; }
 };
@@ -756,6 +782,7 @@ class Aligner {
   Heuristic heur;
   HeurState hstate;
   int memory_mode = 0;
+  bool piggyback = false;  // med/low memory with an alignment (the piggyback backtrace)
   int32_t max_steps = INT32_MAX;
   std::vector<int32_t> scratch;
   Counters ctr;
@@ -830,7 +857,12 @@ class Aligner {
     return allocate(alo, ahi);
   }
 
-  void endsfree_init_offset(Wavefront& wf, int32_t k, int32_t /*v*/, int32_t h) { wf.set(k, h); }
+  // The seed's backtrace starts at (v, h) = (offset - k, offset) (set_bt_init,
+  // src/aligner.rs:213-225, and :3425-3434).
+  void endsfree_init_offset(Wavefront& wf, int32_t k, int32_t /*v*/, int32_t h) {
+    wf.set(k, h);
+    if (piggyback) { wf.seeds.push_back(k); wf.mark_written(k, k); }
+  }
 
   // endsfree_init, src/aligner.rs:3426-3452
   void endsfree_init(Wavefront& wf, int32_t k) {
@@ -892,13 +924,14 @@ class Aligner {
     int32_t n = plen(), m = tlen();
     if (scope == SCOPE_ALIGNMENT) cigar.resize((size_t)(2 * (n + m)) + 1);
     bool score_only = scope == SCOPE_SCORE;
-    bool piggyback = !score_only && memory_mode != 0;
-    if (piggyback) {
-      // Med/low memory (piggyback backtrace) is not restated in this oracle.
-      std::fprintf(stderr, "oracle: med/low memory modes are not restated\n");
-      std::abort();
-    }
+    // Med/low with an alignment: the piggyback backtrace.  Its CIGAR is the
+    // chain of operations each cell copies from the predecessor its kernel
+    // picked (src/compute/piggyback.rs), so the oracle keeps every score
+    // (no score cap, as the reference's modular components have none) and
+    // walks those choices back from the end cell (backtrace_piggyback).
+    piggyback = !score_only && memory_mode != 0;
     comps.modular = score_only;
+    comps.grow = piggyback;
     comps.resize(n, m, pen);
     pool_reset();
     num_null_steps = 0;
@@ -919,6 +952,7 @@ class Aligner {
       for (int32_t h = 1; h <= t0; ++h) wf->set(h, h);
       for (int32_t v = 1; v <= p0; ++v) wf->set(-v, 0);
       wf->lo = -p0; wf->hi = t0; wf->init_min = -p0; wf->init_max = t0;
+      if (piggyback) wf->mark_written(-p0, t0);
     }
     comps.set(CM, 0, wf);
     ctr = Counters();
@@ -1518,7 +1552,9 @@ class Aligner {
     else backtrace_linear(score, k, off);
   }
   void backtrace_from(int32_t score, int32_t k, int32_t off) {  // :1414-1436
-    if (singletrack()) {
+    if (piggyback) {
+      backtrace_piggyback(score, k, off);
+    } else if (singletrack()) {
       int32_t pbf = span == SPAN_ENDSFREE ? p0 : 0, tbf = span == SPAN_ENDSFREE ? t0 : 0;
       backtrace_singletrack(pbf, tbf, score, k, off);
     } else {
@@ -1526,8 +1562,136 @@ class Aligner {
     }
   }
   void backtrace_zdrop_end(int32_t score) {  // :1397-1411 (C compatibility)
-    int32_t from = end_pos.score >= 0 ? end_pos.score : score;
+    // Med/low read the end cell at the current score (where it may be dead).
+    int32_t from = (!piggyback && end_pos.score >= 0) ? end_pos.score : score;
     backtrace_from(from, end_pos.k, end_pos.offset);
+  }
+
+  // --- med/low: the piggyback backtrace --------------------------------------
+  // Offset of (comp, score, k) as the compute kernels read it (absent and
+  // null wavefronts read as NULL).
+  int32_t pv(int comp, int32_t s, int32_t k) const {
+    if (s < 0) return OFFSET_NULL;
+    const Wavefront* w = comps.get(comp, s);
+    if (is_null_wf(w)) return OFFSET_NULL;
+    return w->get(k);
+  }
+  struct Step {
+    uint8_t op;
+    int comp;
+    int32_t s, k;
+  };
+  // The predecessor a piggyback kernel copied cell (comp, s, k)'s backtrace
+  // from, and the operation it pushed (src/compute/piggyback.rs:172-528):
+  // edit/linear take misms over del over ins (later checks win ties), indel
+  // del over ins; a gap cell takes its extension over the M opening on a tie
+  // (`gap`, :146-170); affine M takes misms, else D2, D1, I2, I1 in that
+  // order, pushing an X on top of the gap's chain (the gap close, dropped
+  // when unpacking).
+  Step piggyback_pred(int comp, int32_t s, int32_t k) const {
+    const int32_t x = pen.mismatch;
+    switch (pen.metric) {
+      case EDIT: case INDEL: case LINEAR: {
+        const int32_t gs = pen.metric == LINEAR ? s - pen.o1 : s - 1;
+        const int32_t ms = pen.metric == LINEAR ? s - x : s - 1;
+        const int32_t ins = wrap_add(pv(CM, gs, k - 1), 1), del = pv(CM, gs, k + 1);
+        if (pen.metric == INDEL) {
+          const int32_t mx = std::max(del, ins);
+          return mx == del ? Step{'D', CM, gs, k + 1} : Step{'I', CM, gs, k - 1};
+        }
+        const int32_t misms = wrap_add(pv(CM, ms, k), 1);
+        const int32_t mx = std::max(del, std::max(ins, misms));
+        if (mx == misms) return Step{'X', CM, ms, k};
+        return mx == del ? Step{'D', CM, gs, k + 1} : Step{'I', CM, gs, k - 1};
+      }
+      default: {
+        const bool two = pen.metric == AFFINE2P;
+        if (comp == CI1 || comp == CD1 || comp == CI2 || comp == CD2) {
+          const bool ins = comp == CI1 || comp == CI2;
+          const bool p2 = comp == CI2 || comp == CD2;
+          const int32_t o = p2 ? pen.o2 : pen.o1, e = p2 ? pen.e2 : pen.e1;
+          const int32_t kk = ins ? k - 1 : k + 1;
+          const int32_t open = pv(CM, s - o - e, kk), ext = pv(comp, s - e, kk);
+          const uint8_t op = ins ? 'I' : 'D';
+          return ext >= open ? Step{op, comp, s - e, kk} : Step{op, CM, s - o - e, kk};
+        }
+        const int32_t i1 = pv(CI1, s, k), d1 = pv(CD1, s, k);
+        const int32_t i2 = two ? pv(CI2, s, k) : OFFSET_NULL, d2 = two ? pv(CD2, s, k) : OFFSET_NULL;
+        const int32_t misms = wrap_add(pv(CM, s - x, k), 1);
+        int32_t mx = std::max(d1, std::max(misms, i1));
+        if (two) mx = std::max(std::max(std::max(i1, i2), std::max(d1, d2)), misms);
+        if (mx == misms) return Step{'X', CM, s - x, k};
+        if (two && mx == d2) return Step{'X', CD2, s, k};
+        if (mx == d1) return Step{'X', CD1, s, k};
+        if (two && mx == i2) return Step{'X', CI2, s, k};
+        return Step{'X', CI1, s, k};
+      }
+    }
+  }
+
+  // backtrace_piggyback + backtrace_piggyback_bt, src/aligner.rs:1443-1485:
+  // the chain of M cell (score, k) back to its begin position, unpacked.
+  void backtrace_piggyback(int32_t score, int32_t k, int32_t offset) {
+    const Wavefront* m = comps.get(CM, score);
+    if (!m || !m->allocated(k)) { cigar.begin = 0; cigar.end = 0; return; }
+    std::vector<uint8_t> back;
+    int32_t bv = 0, bh = 0;  // the chain's begin; (0, 0) for an unwritten cell
+    int comp = CM;
+    int32_t s = score, kk = k;
+    const Wavefront* w = m;
+    // A cell outside the written range (or a dead cell, whose backtrace the
+    // kernels never build from a live predecessor) reads as the zero
+    // backtrace: no operations, from the first initial block (0, 0).
+    while (w && w->written(kk) && w->get(kk) >= 0) {
+      if (comp == CM && (s == 0 || w->is_seed(kk))) {
+        // The seed's position when it was placed (before any extension):
+        // (0, k) on a text diagonal, (-k, 0) on a pattern one, (0, 0) at k 0.
+        bv = kk < 0 ? -kk : 0;
+        bh = kk > 0 ? kk : 0;
+        break;
+      }
+      const Step st = piggyback_pred(comp, s, kk);
+      back.push_back(st.op);
+      comp = st.comp; s = st.s; kk = st.k;
+      w = s >= 0 ? comps.get(comp, s) : nullptr;
+      if (is_null_wf(w)) break;
+    }
+    std::reverse(back.begin(), back.end());
+    unpack_piggyback(back, bv, bh, offset - k, offset);
+    cigar.score = score;
+  }
+
+  // unpack_piggyback, src/aligner.rs:232-311: begin-free I/D, then the
+  // operations, re-extending matches before each one (only in M when
+  // affine, where an X after I/D is the gap close and is dropped), then
+  // matches to the end cell and I/D to the sequence ends.
+  void unpack_piggyback(const std::vector<uint8_t>& ops, int32_t v, int32_t h, int32_t end_v,
+                        int32_t end_h) {
+    const int32_t n = plen(), m = tlen();
+    const bool affine = pen.metric == AFFINE || pen.metric == AFFINE2P;
+    int64_t p = 0;
+    auto put = [&](uint8_t op) { cigar.ops[(size_t)p++] = op; };
+    for (int32_t i = 0; i < h; ++i) put('I');
+    for (int32_t i = 0; i < v; ++i) put('D');
+    bool in_m = true;
+    for (uint8_t op : ops) {
+      if (in_m || !affine) {
+        while (v < n && h < m && seq.cmp(v, h)) { put('M'); ++v; ++h; }
+      }
+      if (affine && !in_m && op == 'X') { in_m = true; continue; }
+      put(op);
+      if (op == 'D') { ++v; in_m = false; }
+      else if (op == 'I') { ++h; in_m = false; }
+      else { ++v; ++h; in_m = true; }
+    }
+    const int32_t nm = std::min(end_v - v, end_h - h);
+    for (int32_t i = 0; i < nm; ++i) put('M');
+    v += nm;
+    h += nm;
+    while (h < m) { put('I'); ++h; }
+    while (v < n) { put('D'); ++v; }
+    cigar.begin = 0;
+    cigar.end = p;
   }
 
   // cigar_wfa_score, src/aligner.rs:2700-2719
@@ -1608,7 +1772,7 @@ class Aligner {
     for (;;) {
       if (extend_end2end(score)) break;
       ++score;
-      if (!comps.has_slot(score)) { status = MAX_STEPS; break; }
+      if (!comps.make_slot(score)) { status = MAX_STEPS; break; }
       compute_step(score);
       if (score >= max_steps) { status = MAX_STEPS; break; }
     }
@@ -1657,7 +1821,7 @@ class Aligner {
     for (;;) {
       if (extend_endsfree(score)) break;
       ++score;
-      if (!comps.has_slot(score)) { status = MAX_STEPS; break; }
+      if (!comps.make_slot(score)) { status = MAX_STEPS; break; }
       compute_step(score);
       if (score >= max_steps) { status = MAX_STEPS; break; }
     }

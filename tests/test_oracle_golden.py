@@ -18,13 +18,10 @@ def _cases():
 
 
 CASES = _cases()
-PIGGYBACK = {"med", "low"}
 
 
 @pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
 def test_cli_golden(case):
-    if case["memory"] in PIGGYBACK:
-        pytest.skip("med/low piggyback backtrace is not restated in the oracle")
     assert O.run_cli_case(case) == case["expected"], case["source"]
 
 
