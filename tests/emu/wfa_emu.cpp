@@ -76,7 +76,7 @@ extern "C" int64_t wfa_emu_batch(int metric, const int32_t* pen6, int compute_al
                                  const int64_t* p_off, const int32_t* p_len, const int64_t* t_off,
                                  const int32_t* t_len, int64_t num_pairs, const int64_t* cigar_off,
                                  uint8_t* cigars, wfa_result_t* results, int32_t wmax,
-                                 int32_t hist_scores, int64_t hist_words) {
+                                 int32_t hist_scores, int64_t hist_words, int piggyback) {
   AlignParams P;
   std::memset(&P, 0, sizeof P);
   wfa_penalties_t u = {pen6[0], pen6[1], pen6[2], pen6[3], pen6[4], pen6[5]};
@@ -87,6 +87,7 @@ extern "C" int64_t wfa_emu_batch(int metric, const int32_t* pen6, int compute_al
   P.hkind = hkind;
   if (hp3) { P.hp0 = hp3[0]; P.hp1 = hp3[1]; P.hp2 = hp3[2]; }
   P.compute_alignment = compute_alignment;
+  P.piggyback = piggyback;
   P.max_steps = max_steps;
   P.format = format;
   P.seq = seq;

@@ -19,9 +19,10 @@ PENS = [(1, None), (0, None), (2, [0, 4, 2]), (2, [-1, 3, 2]), (3, [0, 4, 6, 2])
 HEUR = {"wfa-adaptive": 1, "xdrop": 2, "zdrop": 3, "banded-static": 4, "banded-adaptive": 5}
 
 
-def oracle_run(metric, pen, p, t, compute, span, free, hk, hp, extension=False):
+def oracle_run(metric, pen, p, t, compute, span, free, hk, hp, extension=False, memory="high"):
     a = O.OracleAligner(metric, pen)
     a.set_alignment_scope(compute)
+    a.set_memory_mode(memory)
     if hk:
         a.set_heuristic(hk, *hp)
     if extension:
@@ -37,13 +38,13 @@ def oracle_run(metric, pen, p, t, compute, span, free, hk, hp, extension=False):
 
 
 def compare(metric, pen, pairs, compute=True, span=0, free=None, hk=0, hp=(0, 0, 0),
-            extension=False, packed=False):
+            extension=False, packed=False, memory="high"):
     res, cig = emu_lib.run(metric, pen, pairs, compute_alignment=compute, span=span or int(extension),
                            extension=int(extension), free=free, heuristic=hk, hparams=hp,
-                           packed=packed)
+                           packed=packed, piggyback=compute and memory != "high")
     for i, (p, t) in enumerate(pairs):
         s, st, ops, ep, (cs, ev, eh) = oracle_run(metric, pen, p, t, compute, span, free, hk, hp,
-                                                  extension)
+                                                  extension, memory)
         r = res[i]
         got = (int(r["score"]), int(r["status"]), cig[i] if compute else "",
                (int(r["end_score"]), int(r["end_k"]), int(r["end_offset"])))
@@ -102,11 +103,52 @@ def test_packed_and_edges(packed):
         compare(metric, pen, edge, packed=packed)
 
 
+# Med/low memory with an alignment: the piggyback backtrace.
+@pytest.mark.parametrize("metric,pen", PENS)
+@pytest.mark.parametrize("memory", ["med", "low"])
+def test_piggyback_end2end(metric, pen, memory):
+    compare(metric, pen, lcg_pairs(61 + metric, 30, 250), memory=memory)
+
+
+@pytest.mark.parametrize("metric,pen", PENS)
+def test_piggyback_endsfree(metric, pen):
+    r = random.Random(metric * 11 + 3)
+    for p, t in lcg_pairs(67 + metric, 20, 200):
+        free = [r.randrange(0, len(p) // 3 + 1), r.randrange(0, len(p) // 3 + 1),
+                r.randrange(0, len(t) // 3 + 1), r.randrange(0, len(t) // 3 + 1)]
+        compare(metric, pen, [(p, t)], span=1, free=free, memory="med")
+
+
+@pytest.mark.parametrize("metric,pen", [x for x in PENS if x[0] >= 2])
+def test_piggyback_extension(metric, pen):
+    compare(metric, pen, lcg_pairs(71 + metric, 20, 200), extension=True, memory="low")
+
+
+@pytest.mark.parametrize("metric,pen", PENS)
+@pytest.mark.parametrize("h,hp", [("wfa-adaptive", (10, 50, 1)), ("xdrop", (20, 1)),
+                                  ("banded-static", (-5, 5)), ("banded-adaptive", (-3, 3, 1))])
+def test_piggyback_heuristics(metric, pen, h, hp):
+    if h in ("xdrop", "zdrop") and metric in (0, 1):
+        pytest.skip("drops are rejected with edit/indel")
+    hp = list(hp) + [0] * (3 - len(hp))
+    compare(metric, pen, lcg_pairs(73 + metric, 20, 250), hk=HEUR[h], hp=hp, memory="med")
+
+
+def test_piggyback_edges():
+    edge = [(b"", b""), (b"A", b""), (b"", b"ACGT"), (b"A", b"C"), (b"A", b"A"),
+            (b"ACGT" * 40, b"ACGT" * 40), (b"AAAAAAAA", b"CCCCCCCC"), (b"ACGTTTTTTTTTTACGT", b"ACGTACGT")]
+    for metric, pen in PENS:
+        compare(metric, pen, edge, memory="med")
+        for p, t in edge:  # free ends within the lengths, as the aligner requires
+            free = [min(2, len(p)), min(1, len(p)), min(2, len(t)), min(1, len(t))]
+            compare(metric, pen, [(p, t)], span=1, free=free, memory="low")
+
+
 def test_golden_cli_cases(golden):
     """The reference's CLI golden lines, reproduced by the device logic."""
     checked = 0
     for case in golden["cases"]:
-        if case["memory"] != "high":
+        if case["memory"] not in ("high", "med", "low"):
             continue
         metric = O.METRICS[case["algo"]]
         pen = [int(x) for x in case["penalties"].split(",")] if case["penalties"] else O.DEFAULT_PEN[metric]
@@ -128,7 +170,8 @@ def test_golden_cli_cases(golden):
                         O.nominal_prop(len(tb), fr[2]), O.nominal_prop(len(tb), fr[3])]
                 span = 1
             res, cig = emu_lib.run(metric, pen, [(pb, tb)], compute_alignment=not so, span=span,
-                                   extension=ext, free=free, heuristic=hk, hparams=hp[:3])
+                                   extension=ext, free=free, heuristic=hk, hparams=hp[:3],
+                                   piggyback=not so and case["memory"] != "high")
             orig = (pen + [0] * 6)[:6]
             lines.append(cli_format.line(metric, orig, so, False, res[0], cig[0], len(pb), len(tb)))
         assert lines == case["expected"], case["name"]

@@ -35,9 +35,10 @@ def pack(pairs):
 
 
 def gpu_batch(pkg, metric, pen, pairs, compute=True, span=0, free=None, hk=0, hp=(0, 0, 0),
-              extension=False, packed=False):
+              extension=False, packed=False, memory="high"):
     a = pkg.WavefrontAligner(metric, pen)
     a.set_alignment_scope(compute)
+    a.set_memory_mode(memory)
     if hk:
         a.set_heuristic(hk, *hp)
     if extension:
@@ -58,9 +59,10 @@ def gpu_batch(pkg, metric, pen, pairs, compute=True, span=0, free=None, hk=0, hp
     return res, cigars
 
 
-def oracle_one(metric, pen, p, t, compute, span, free, hk, hp, extension):
+def oracle_one(metric, pen, p, t, compute, span, free, hk, hp, extension, memory="high"):
     a = O.OracleAligner(metric, pen)
     a.set_alignment_scope(compute)
+    a.set_memory_mode(memory)
     if hk:
         a.set_heuristic(hk, *hp)
     if extension:
@@ -76,11 +78,12 @@ def oracle_one(metric, pen, p, t, compute, span, free, hk, hp, extension):
 
 
 def compare(pkg, metric, pen, pairs, compute=True, span=0, free=None, hk=0, hp=(0, 0, 0),
-            extension=False, packed=False):
-    res, cig = gpu_batch(pkg, metric, pen, pairs, compute, span, free, hk, hp, extension, packed)
+            extension=False, packed=False, memory="high"):
+    res, cig = gpu_batch(pkg, metric, pen, pairs, compute, span, free, hk, hp, extension, packed,
+                         memory)
     for i, (p, t) in enumerate(pairs):
         s, st, ops, ep, (cs, ev, eh) = oracle_one(metric, pen, p, t, compute, span, free, hk, hp,
-                                                  extension)
+                                                  extension, memory)
         r = res[i]
         got = (int(r["score"]), int(r["status"]), cig[i] if compute else "",
                (int(r["end_score"]), int(r["end_k"]), int(r["end_offset"])))
@@ -140,16 +143,76 @@ def test_retry_escalation(pkg):
     compare(pkg, 1, None, pairs)
 
 
+@pytest.mark.parametrize("metric,pen", PENS)
+@pytest.mark.parametrize("memory", ["med", "low"])
+def test_med_low_piggyback(pkg, metric, pen, memory):
+    """Med/low memory with an alignment: the piggyback backtrace's CIGARs."""
+    compare(pkg, metric, pen, lcg_pairs(261 + metric, 60, 300), memory=memory)
+    compare(pkg, metric, pen, lcg_pairs(263 + metric, 30, 200), packed=True, memory=memory)
+
+
+@pytest.mark.parametrize("metric,pen", PENS)
+def test_med_low_piggyback_spans_and_heuristics(pkg, metric, pen):
+    r = random.Random(metric + 17)
+    for p, t in lcg_pairs(267 + metric, 12, 200):
+        free = [r.randrange(0, len(p) // 3 + 1), r.randrange(0, len(p) // 3 + 1),
+                r.randrange(0, len(t) // 3 + 1), r.randrange(0, len(t) // 3 + 1)]
+        compare(pkg, metric, pen, [(p, t)], span=1, free=free, memory="med")
+    if metric >= 2:
+        compare(pkg, metric, pen, lcg_pairs(269 + metric, 30, 200), extension=True, memory="low")
+        compare(pkg, metric, pen, lcg_pairs(271 + metric, 30, 250), hk=2, hp=(20, 1, 0), memory="med")
+    compare(pkg, metric, pen, lcg_pairs(273 + metric, 30, 250), hk=1, hp=(10, 50, 1), memory="med")
+    compare(pkg, metric, pen, lcg_pairs(275 + metric, 30, 250), hk=5, hp=(-3, 3, 1), memory="low")
+
+
+@pytest.mark.parametrize("memory", ["high", "med", "low"])
+def test_reference_unit_cases_in_every_memory_mode(pkg, memory):
+    """src/aligner.rs:3890-3943: empty sequences give score 0 and an empty
+    CIGAR; a begin-free seed at score 0 starts the CIGAR at its position."""
+    for metric, pen in [(1, None), (3, [0, 4, 6, 2])]:
+        for endsfree in (False, True):
+            a = pkg.WavefrontAligner(metric, pen)
+            a.set_memory_mode(memory)
+            a.set_alignment_scope(True)
+            if endsfree:
+                a.set_alignment_free_ends(0, 0, 0, 0)
+                s = a.align_endsfree(b"", b"")
+            else:
+                s = a.align_end2end(b"", b"")
+            assert s == 0 and a.status() == 5 and a.cigar().operations == b""  # Completed
+    a = pkg.WavefrontAligner(2, [0, 3, 3])
+    a.set_memory_mode(memory)
+    a.set_alignment_scope(True)
+    a.set_alignment_free_ends(0, 0, 4, 11)
+    a.align_endsfree(b"G", b"TCGGGACATCGAG")
+    assert a.cigar().to_string_rle() == "2I1M10I"
+
+
+def test_med_low_long_pairs(pkg):
+    """Pairs long enough to outgrow the first history size re-run and match."""
+    r = random.Random(29)
+    pairs = []
+    for n in (1500, 3000):
+        p = bytes(r.choice(b"ACGT") for _ in range(n))
+        t = bytearray(p)
+        for _ in range(n // 12):
+            t[r.randrange(len(t))] = r.choice(b"ACGT")
+        pairs.append((p, bytes(t)))
+    for metric, pen in [(1, None), (3, [0, 4, 6, 2]), (4, [0, 4, 6, 2, 24, 1])]:
+        compare(pkg, metric, pen, pairs + lcg_pairs(277, 20, 200), memory="med")
+
+
 def test_plain_calls_and_golden_cli(pkg, golden):
     """The plain per-call form reproduces the reference's CLI golden lines."""
     for case in golden["cases"]:
-        if case["memory"] != "high":
+        if case["memory"] not in ("high", "med", "low"):
             continue
         metric = O.METRICS[case["algo"]]
         pen = [int(x) for x in case["penalties"].split(",")] if case["penalties"] else O.DEFAULT_PEN[metric]
         so = case["score_only"]
         a = pkg.WavefrontAligner(metric, pen)
         a.set_alignment_scope(not so)
+        a.set_memory_mode(case["memory"])
         if case["heuristic"]:
             a.set_heuristic(case["heuristic"], *[int(x) for x in case["hparams"].split(",")])
         span_s = case["span"]

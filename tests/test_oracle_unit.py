@@ -141,9 +141,11 @@ def test_endsfree_begin_free_match_zero():
 
 @pytest.mark.parametrize("metric,pen", [(EDIT, None), (AFFINE, AFF)])
 @pytest.mark.parametrize("endsfree", [False, True])
-def test_empty_sequences(metric, pen, endsfree):
-    """src/aligner.rs:3890-3921 (high memory; med/low are a later row)."""
+@pytest.mark.parametrize("memory", ["high", "med", "low"])
+def test_empty_sequences(metric, pen, endsfree, memory):
+    """src/aligner.rs:3890-3921."""
     a = O.OracleAligner(metric, pen)
+    a.set_memory_mode(memory)
     a.set_alignment_scope(True)
     if endsfree:
         a.set_alignment_free_ends(0, 0, 0, 0)
@@ -155,9 +157,11 @@ def test_empty_sequences(metric, pen, endsfree):
     assert b.align_biwfa(b"", b"") == 0 and b.cigar()[0] == b""
 
 
-def test_endsfree_begin_free_seed_backtrace():
-    """src/aligner.rs:3924-3943 (high memory)."""
+@pytest.mark.parametrize("memory", ["high", "med", "low"])
+def test_endsfree_begin_free_seed_backtrace(memory):
+    """src/aligner.rs:3924-3943."""
     a = O.OracleAligner(LINEAR, [0, 3, 3])
+    a.set_memory_mode(memory)
     a.set_alignment_scope(True)
     a.set_alignment_free_ends(0, 0, 4, 11)
     a.align_endsfree(b"G", b"TCGGGACATCGAG")

@@ -272,6 +272,11 @@ struct PairAligner {
   // steps store null slots (BiWFA's overlap scans read every ring slot).
   int32_t hist_nc;
   bool keep_null_slots;
+  // Med/low memory with an alignment (the piggyback backtrace), and the
+  // begin-free seeds endsfree_init placed at the current score (bit 0 text
+  // seed at +k, bit 1 pattern seed at -k), stored with M's history record.
+  bool pgb = false;
+  int32_t seed_flags = 0;
   int32_t comp_end;  // component whose end diagonal terminates (BiWFA), else M
   int32_t cscore, cidx;  // current score and its ring index
   // Scores that are not multiples of gstep can have no wavefront: every input
@@ -343,11 +348,12 @@ struct PairAligner {
         if (hused + w > P.hist_words) { retry = true; return; }
         for (int64_t i = lane; i < w; i += WFA_WARP) ws.harena[hused + i] = d.vals[i];
         r.z = (int32_t)hused;
-        r.w = 1;
+        r.w = c == CM ? 1 | (seed_flags << 1) : 1;
         hused += w;
       }
       if (lane == 0) ws.hist[(int64_t)s * hist_nc + c] = r;
     }
+    seed_flags = 0;
     // No sync: the history is read only by the backtrace, which starts with one.
   }
 
@@ -420,19 +426,21 @@ struct PairAligner {
     Warp::sync();
     if (t0 >= k) {
       if (hi >= k) {
-        if (base[k - L] <= k) { Warp::sync(); if (lane == 0) base[k - L] = k; }
+        if (base[k - L] <= k) { Warp::sync(); if (lane == 0) base[k - L] = k; seed_flags |= 1; }
       } else {
         for (int kk = hi + 1 + lane; kk < k; kk += WFA_WARP) base[kk - L] = kOffsetNull;
         if (lane == 0) base[k - L] = k;
+        seed_flags |= 1;
         hi = k;
       }
     }
     Warp::sync();
     if (p0 >= k) {
       if (lo <= -k) {
-        if (base[-k - L] <= 0) { Warp::sync(); if (lane == 0) base[-k - L] = 0; }
+        if (base[-k - L] <= 0) { Warp::sync(); if (lane == 0) base[-k - L] = 0; seed_flags |= 2; }
       } else {
         if (lane == 0) base[-k - L] = 0;
+        seed_flags |= 2;
         for (int kk = -k + 1 + lane; kk < lo; kk += WFA_WARP) base[kk - L] = kOffsetNull;
         lo = -k;
       }
@@ -456,6 +464,7 @@ struct PairAligner {
       if (text) v[k - lo] = k;
       if (pattern) v[-k - lo] = 0;
     }
+    seed_flags |= (text ? 1 : 0) | (pattern ? 2 : 0);
     Warp::sync();
     WfD d;
     d.vals = v; d.lo = lo; d.hi = hi; d.a = lo; d.b = hi; d.flags = kPresent; d.adub = kAdUnknown;
@@ -1442,8 +1451,146 @@ struct PairAligner {
     run('I', h);
   }
 
+  // ---- med/low: the piggyback backtrace ----------------------------------------
+  // The reference's med/low kernels (src/compute/piggyback.rs) carry each
+  // cell's backtrace along, copied from the predecessor the kernel picked;
+  // here every component's history is kept and the same picks are re-made
+  // from it, walking back from the end cell.
+  //
+  // Offset of (c, s, k) as the compute kernels read it (absent wavefronts
+  // and cells outside the stored range read as NULL).
+  WFA_D int32_t pv(int c, int s, int k) const {
+    if (s < 0) return kOffsetNull;
+    int4 r = ws.hist[(int64_t)s * hist_nc + c];
+    if (!(r.w & 1) || k < r.x || k > r.y) return kOffsetNull;
+    return ws.harena[r.z + (k - r.x)];
+  }
+  // The begin-free seed endsfree_init placed at M cell (s, k).
+  WFA_D bool pb_seed(int s, int k) const {
+    if (P.match >= 0 || s <= 0) return false;
+    int fl = ws.hist[(int64_t)s * hist_nc + CM].w >> 1;
+    if (!fl) return false;
+    int bk = s / (-P.match);
+    return ((fl & 1) && k == bk) || ((fl & 2) && k == -bk);
+  }
+  struct PbStep {
+    uint8_t op;
+    int c, s, k;
+  };
+  // The predecessor cell (c, s, k)'s kernel copied its backtrace from, and
+  // the operation it pushed (src/compute/piggyback.rs:172-528): edit and
+  // linear take misms over del over ins, indel del over ins; a gap cell
+  // takes its extension over the M opening on a tie (:146-170); affine M
+  // takes misms, else D2, D1, I2, I1, pushing an X (the gap close) on top of
+  // the gap's chain.
+  WFA_D PbStep pb_pred(int c, int s, int k) const {
+    if (!AFF) {
+      const int gs = s - P.o1;
+      const int32_t ins = pv(CM, gs, k - 1) + 1, del = pv(CM, gs, k + 1);
+      if (P.metric == WFA_METRIC_INDEL)
+        return imax(del, ins) == del ? PbStep{'D', CM, gs, k + 1} : PbStep{'I', CM, gs, k - 1};
+      const int ms = s - P.mismatch;
+      const int32_t misms = pv(CM, ms, k) + 1;
+      const int32_t mx = imax(del, imax(ins, misms));
+      if (mx == misms) return PbStep{'X', CM, ms, k};
+      return mx == del ? PbStep{'D', CM, gs, k + 1} : PbStep{'I', CM, gs, k - 1};
+    }
+    if (c != CM) {
+      const bool ins = c == CI1 || c == CI2, p2 = c == CI2 || c == CD2;
+      const int o = p2 ? P.o2 : P.o1, e = p2 ? P.e2 : P.e1;
+      const int kk = ins ? k - 1 : k + 1;
+      const uint8_t op = ins ? 'I' : 'D';
+      const int32_t open = pv(CM, s - o - e, kk), ext = pv(c, s - e, kk);
+      return ext >= open ? PbStep{op, c, s - e, kk} : PbStep{op, CM, s - o - e, kk};
+    }
+    const int32_t i1 = pv(CI1, s, k), d1 = pv(CD1, s, k);
+    const int32_t i2 = TWO ? pv(CI2, s, k) : kOffsetNull, d2 = TWO ? pv(CD2, s, k) : kOffsetNull;
+    const int32_t misms = pv(CM, s - P.mismatch, k) + 1;
+    const int32_t mx = imax(imax(misms, imax(i1, d1)), imax(i2, d2));
+    if (mx == misms) return PbStep{'X', CM, s - P.mismatch, k};
+    if (TWO && mx == d2) return PbStep{'X', CD2, s, k};
+    if (mx == d1) return PbStep{'X', CD1, s, k};
+    if (TWO && mx == i2) return PbStep{'X', CI2, s, k};
+    return PbStep{'X', CI1, s, k};
+  }
+  // Forward CIGAR writes of the unpack: at most `limit` (exclusive) -- the
+  // chain operations not yet read sit above it in the same slot.
+  WFA_D bool fwd(int64_t& p, int64_t limit, uint8_t op, int cnt) {
+    if (cnt <= 0) return true;
+    if (p + cnt > limit) { status = WFA_STATUS_OOM; return false; }
+    for (int i = lane; i < cnt; i += WFA_WARP) cg[p + i] = op;
+    p += cnt;
+    return true;
+  }
+  // backtrace_piggyback + backtrace_piggyback_bt (src/aligner.rs:1443-1485)
+  // and unpack_piggyback (:232-311): the chain of M cell (score, k) back to
+  // its begin -- score 0, or a begin-free seed at (0, k) / (-k, 0) -- then
+  // unpacked forwards: begin-free I/D, the operations with matches
+  // re-extended before each one (only in M when affine, where an X after I/D
+  // is the gap close and is dropped), matches to the end cell, I/D to the
+  // sequence ends.  The chain is stored backwards from the slot's end and
+  // read in order while the CIGAR is written from the slot's start.
+  WFA_D void backtrace_piggyback(int score, int k, int offset) {
+    cg_begin = 0;
+    cg_end = 0;
+    if (score < 0) return;
+    {
+      int4 r = ws.hist[(int64_t)score * hist_nc + CM];
+      if (!(r.w & 1) || k < r.x || k > r.y) return;  // no such end cell: no CIGAR
+    }
+    int64_t rd = cg_cap;
+    int c = CM, s = score, kk = k, bv = 0, bh = 0;
+    // A dead cell ends the chain with the zero backtrace (no operations, from
+    // (0, 0)): the kernels never build it from a live predecessor.
+    while (pv(c, s, kk) >= 0) {
+      if (c == CM && (s == 0 || pb_seed(s, kk))) {
+        bv = kk < 0 ? -kk : 0;
+        bh = kk > 0 ? kk : 0;
+        break;
+      }
+      const PbStep st = pb_pred(c, s, kk);
+      if (rd == 0) { status = WFA_STATUS_OOM; return; }
+      --rd;
+      if (lane == 0) cg[rd] = st.op;
+      c = st.c; s = st.s; kk = st.k;
+    }
+    Warp::sync();
+    const bool affine = AFF;
+    int64_t p = 0;
+    int v = bv, h = bh;
+    if (!fwd(p, rd, 'I', h) || !fwd(p, rd, 'D', v)) return;
+    bool in_m = true;
+    for (int64_t i = rd; i < cg_cap; ++i) {
+      const uint8_t op = cg[i];
+      Warp::sync();  // every lane has read cg[i] before it may be overwritten
+      if (in_m || !affine) {
+        const int nm = lcp_fwd(pat, v, txt, h, imax(0, imin(n - v, m - h)));
+        if (!fwd(p, i + 1, 'M', nm)) return;
+        v += nm;
+        h += nm;
+      }
+      if (affine && !in_m && op == 'X') { in_m = true; continue; }
+      if (!fwd(p, i + 1, op, 1)) return;
+      if (op == 'D') { ++v; in_m = false; }
+      else if (op == 'I') { ++h; in_m = false; }
+      else { ++v; ++h; in_m = true; }
+    }
+    const int nm = imin(offset - k - v, offset - h);
+    if (!fwd(p, cg_cap, 'M', nm)) return;
+    v += nm;  // as the reference: a negative count moves back
+    h += nm;
+    if (!fwd(p, cg_cap, 'I', m - h) || !fwd(p, cg_cap, 'D', n - v)) return;
+    cg_end = p;
+  }
+
   WFA_D void backtrace_from(int score, int k, int offset) {  // src/aligner.rs:1414-1436
     Warp::sync();
+    if (pgb) {
+      backtrace_piggyback(score, k, offset);
+      cg_score = score;
+      Warp::sync();
+      return;
+    }
     cg_end = cg_cap;
     cg_begin = cg_cap - 1;
     if (AFF) backtrace_singletrack(score, k, offset);
@@ -1646,7 +1793,7 @@ struct PairAligner {
         if (status != WFA_STATUS_OOM) status = WFA_STATUS_COMPLETED;
       } else if (status == WFA_STATUS_END_UNREACHABLE && end_off != kOffsetNull) {
         if (cigar) {
-          backtrace_from(end_score >= 0 ? end_score : score, end_k, end_off);
+          backtrace_from(end_score >= 0 && !pgb ? end_score : score, end_k, end_off);
           maxtrim_cigar();
         }
         if (status != WFA_STATUS_OOM) status = WFA_STATUS_PARTIAL;
@@ -1654,7 +1801,7 @@ struct PairAligner {
     } else if (status == WFA_STATUS_END_REACHED || status == WFA_STATUS_END_UNREACHABLE) {
       bool unreachable = status == WFA_STATUS_END_UNREACHABLE;
       if (cigar && (status == WFA_STATUS_END_REACHED || end_off != kOffsetNull)) {
-        if (unreachable) backtrace_from(end_score >= 0 ? end_score : score, end_k, end_off);
+        if (unreachable) backtrace_from(end_score >= 0 && !pgb ? end_score : score, end_k, end_off);
         else backtrace_from(score, end_k, end_off);
         if (status == WFA_STATUS_OOM) return result;
         if (P.extension || unreachable) {
@@ -1688,10 +1835,12 @@ WFA_D bool align_one(const AlignParams& P, const Workspace& ws, int64_t pair, S 
   A.scope = P.scope;
   A.wmax = P.wmax;
   A.modular = P.compute_alignment == 0;
-  A.cap = A.modular ? INT_MAX : imax(A.dims_num(1000, 1000), A.dims_num(A.n, A.m));
+  A.pgb = !A.modular && P.piggyback != 0;
+  // Med/low components are modular: no score cap.
+  A.cap = A.modular || A.pgb ? INT_MAX : imax(A.dims_num(1000, 1000), A.dims_num(A.n, A.m));
   A.endsfree = P.span == WFA_SPAN_ENDSFREE;
   A.hkind = P.hkind; A.hp0 = P.hp0; A.hp1 = P.hp1; A.hp2 = P.hp2;
-  A.hist_nc = 1;
+  A.hist_nc = A.pgb ? PairAligner<CLS, S, GEN>::NC : 1;
   A.keep_null_slots = false;
   A.comp_end = CM;
   if (P.extension) { A.p0 = 0; A.pf = A.n; A.t0 = 0; A.tf = A.m; }

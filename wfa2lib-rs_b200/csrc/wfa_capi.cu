@@ -192,9 +192,6 @@ __global__ void max_lengths(const int32_t* pl, const int32_t* tl, int64_t n, int
 // Configuration checks
 // ---------------------------------------------------------------------------
 static int check_supported(wfa_aligner_t* h, bool biwfa) {
-  if (!biwfa && h->scope == WFA_SCOPE_ALIGNMENT && h->memory_mode != WFA_MEMORY_HIGH)
-    return fail(h, WFA_ERR_UNSUPPORTED,
-                "med/low memory (piggyback backtrace) is not available in this build");
   if (!biwfa && h->compat == WFA_COMPAT_CORRECTED && h->pen.match < 0 && h->span == WFA_SPAN_ENDSFREE)
     return fail(h, WFA_ERR_UNSUPPORTED, "Compat::Corrected ends-free with a match reward");
   if (h->pen.scope > 1024) return fail(h, WFA_ERR_UNSUPPORTED, "max_score_scope above 1024");
@@ -208,6 +205,9 @@ static void fill_params(const wfa_aligner_t* h, const wfa_batch_t* b, AlignParam
   P.p0 = h->p0; P.pf = h->pf; P.t0 = h->t0; P.tf = h->tf;
   P.hkind = h->hkind; P.hp0 = h->hp0; P.hp1 = h->hp1; P.hp2 = h->hp2;
   P.compute_alignment = h->scope == WFA_SCOPE_ALIGNMENT;
+  // Med/low with an alignment: the piggyback backtrace (BiWFA ignores the mode).
+  P.piggyback = P.compute_alignment && h->memory_mode != WFA_MEMORY_HIGH &&
+                b->span != WFA_SPAN_BIWFA;
   P.max_steps = h->max_steps;
   P.format = b->format;
   P.seq = static_cast<const uint8_t*>(b->seq);
@@ -252,9 +252,11 @@ static Round first_round(const AlignParams& P, int nc, int32_t max_len_sum) {
   Round r;
   const bool longp = max_len_sum > kLongPair;
   r.cfg.wmax = std::max(8, std::min(max_len_sum + 3, 8192));
-  r.cfg.hist_scores = P.compute_alignment ? (longp ? max_len_sum + 3 : 1024) : 0;
+  // The piggyback backtrace keeps every component's history.
+  const int hnc = P.piggyback ? nc : 1;
+  r.cfg.hist_scores = P.compute_alignment ? hnc * (longp ? max_len_sum + 3 : 1024) : 0;
   r.cfg.hist_words = P.compute_alignment
-                         ? (int64_t)std::max(32768, (longp ? 64 : 16) * (max_len_sum + 3))
+                         ? hnc * (int64_t)std::max(32768, (longp ? 64 : 16) * (max_len_sum + 3))
                          : 0;
   r.ring_smem = !longp && (size_t)P.scope * nc * kRingSmemWidth * 4 <= kRingSmemBudget;
   if (r.ring_smem) r.cfg.wmax = std::min(r.cfg.wmax, kRingSmemWidth);
@@ -520,8 +522,9 @@ static int run_noalloc_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_
   int64_t* list = reinterpret_cast<int64_t*>(base + kNaHeaderWords);
   Round r = first_round(P, nc, max_len_sum);
   if (P.compute_alignment) {
-    r.cfg.hist_scores = 256;
-    r.cfg.hist_words = 4096;
+    const int hnc = P.piggyback ? nc : 1;
+    r.cfg.hist_scores = 256 * hnc;
+    r.cfg.hist_words = 4096 * hnc;
   }
   int64_t todo = b->num_pairs, pending = 0;
   int grown = 0;

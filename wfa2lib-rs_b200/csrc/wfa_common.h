@@ -31,6 +31,9 @@ struct AlignParams {
   // Heuristic (wfa_heuristic_kind_t and its three parameters).
   int32_t hkind, hp0, hp1, hp2;
   int32_t compute_alignment;
+  // 1: med/low memory with an alignment -- the piggyback backtrace (every
+  // component's history, no score cap).
+  int32_t piggyback;
   int32_t max_steps;
   // Input.
   int32_t format;  // wfa_seq_format_t
