@@ -34,6 +34,7 @@ def lib(fast=False):
     L.wfo_destroy.argtypes = [vp]
     L.wfo_set_alignment_scope.argtypes = [vp, ctypes.c_int]
     L.wfo_set_memory_mode.argtypes = [vp, ctypes.c_int]
+    L.wfo_set_compat.argtypes = [vp, ctypes.c_int]
     L.wfo_set_heuristic.argtypes = [vp, ctypes.c_int, i32, i32, i32]
     L.wfo_set_max_alignment_steps.argtypes = [vp, i32]
     L.wfo_set_alignment_free_ends.argtypes = [vp, i32, i32, i32, i32]
@@ -85,6 +86,10 @@ class OracleAligner:
 
     def set_memory_mode(self, mode):
         self.L.wfo_set_memory_mode(self.h, {"high": 0, "med": 1, "low": 2}.get(mode, mode))
+
+    def set_compat(self, compat):
+        """'c' (reproduce C's known bugs, the default) or 'corrected'."""
+        self.L.wfo_set_compat(self.h, {"c": 0, "corrected": 1}.get(compat, compat))
 
     def set_heuristic(self, kind, *params):
         k = HEURISTICS[kind] if isinstance(kind, str) or kind is None else kind
@@ -167,6 +172,8 @@ def run_cli_case(case, fast=False):
     score_only = bool(case.get("score_only"))
     if not score_only:
         a.set_alignment_scope(True)
+    if case.get("no_c_compat"):
+        a.set_compat("corrected")
     mem = case.get("memory", "high")
     biwfa = mem == "ultralow"
     a.set_memory_mode("high" if biwfa else mem)

@@ -783,6 +783,20 @@ class Aligner {
   HeurState hstate;
   int memory_mode = 0;
   bool piggyback = false;  // med/low memory with an alignment (the piggyback backtrace)
+  // Compat (src/aligner.rs:53-94): 0 C (reproduce C's known bugs), 1 Corrected.
+  int compat = 0;
+  // Corrected-mode ends-free end candidate (EndsfreeCandidate, :96-107): the
+  // best cell reaching a free end so far and its total score.
+  struct Candidate {
+    bool has = false;
+    int32_t total = 0;
+    Pos pos;
+  };
+  Candidate best;
+  // Corrected-mode begin-free dominance pruning (:172-186): per component,
+  // the furthest offset each diagonal reached at an earlier score.
+  std::vector<int32_t> dom_best;
+  int32_t dom_base = 0, dom_len = 0;
   int32_t max_steps = INT32_MAX;
   std::vector<int32_t> scratch;
   Counters ctr;
@@ -941,6 +955,19 @@ class Aligner {
     int32_t sc = (int32_t)comps.scope;
     comps.hist_lo = -(n + sc + 2);
     comps.hist_hi = m + sc + 2;
+    // Corrected mode (:912-947): no candidate yet; dominance pruning only
+    // with begin-free seeds (at most 4 bases unless gap-linear) and no
+    // heuristic that reads the wavefronts.
+    best = Candidate();
+    dom_best.clear();
+    const int32_t bfree = std::max(p0, t0);
+    if (endsfree_corrected() && span == SPAN_ENDSFREE && bfree > 0 &&
+        (pen.metric == LINEAR || bfree <= 4) &&
+        (heur.kind == H_NONE || heur.kind == H_BANDED_STATIC)) {
+      dom_base = comps.hist_lo;
+      dom_len = comps.hist_hi - comps.hist_lo + 1;
+      dom_best.assign((size_t)ncomp() * (size_t)dom_len, -1);
+    }
     int32_t lo0 = 0, hi0 = 0;
     if (pen.match_ == 0 && span == SPAN_ENDSFREE) { lo0 = -p0; hi0 = t0; }
     int32_t alo, ahi;
@@ -1090,6 +1117,7 @@ class Aligner {
 
   // extend_endsfree, src/aligner.rs:1053-1101 (C compatibility)
   bool extend_endsfree(int32_t score) {
+    if (endsfree_corrected()) return extend_endsfree_corrected(score);
     Wavefront* m = comps.get(CM, score);
     if (!m) {
       if (num_null_steps > (int32_t)comps.scope) { status = END_UNREACHABLE; return true; }
@@ -1103,6 +1131,127 @@ class Aligner {
     }
     if (heur.kind != H_NONE && apply_heuristic_cutoff(score, m)) {
       status = END_UNREACHABLE;
+      return true;
+    }
+    return false;
+  }
+
+  // --- Compat::Corrected ends-free (src/aligner.rs:1104-1345) ----------------
+  bool endsfree_corrected() const { return compat == 1 && pen.match_ < 0; }  // :1107
+
+  // endsfree_left, src/termination.rs:65-86: the bases a cell at a free end
+  // leaves to the free end gap (the smaller of the two ends it reaches).
+  bool endsfree_left(int32_t k, int32_t off, int32_t& left) const {
+    const int32_t n = plen(), m = tlen(), h = off, v = off - k;
+    const bool by_t = h >= m && n - v <= pf, by_p = v >= n && m - h <= tf;
+    if (!by_t && !by_p) return false;
+    left = by_t && by_p ? std::min(n - v, m - h) : by_t ? n - v : m - h;
+    return true;
+  }
+  // extend_matches_packed_endsfree_best, src/extend.rs:179-232: extend every
+  // cell (no early stop) and return the free-end cell leaving the fewest
+  // bases (the lowest diagonal on ties).
+  bool extend_endsfree_best_wf(Wavefront& wf, int32_t& rk, int32_t& roff, int32_t& rleft) {
+    bool found = false;
+    for (int32_t k = wf.lo; k <= wf.hi; ++k) {
+      int32_t off = wf.get(k);
+      if (off == OFFSET_NULL) continue;
+      off = extend_one(k, off);
+      wf.set(k, off);
+      int32_t left;
+      if (term_endsfree(k, off) && endsfree_left(k, off, left) && (!found || left < rleft)) {
+        found = true; rk = k; roff = off; rleft = left;
+      }
+    }
+    return found;
+  }
+  // Wavefront::trim_nulled, src/wavefront.rs:463-490
+  static void trim_nulled(Wavefront& wf, int32_t lo, int32_t hi) {
+    if (wf.null || wf.lo > wf.hi || (lo <= wf.lo && hi >= wf.hi)) return;
+    const int32_t olo = wf.lo, ohi = wf.hi;
+    const int32_t nlo = std::max(lo, olo), nhi = std::min(hi, ohi);
+    if (nlo > nhi) {
+      for (int32_t k = olo; k <= ohi; ++k) wf.set(k, OFFSET_NULL);
+      wf.null = true;
+    } else {
+      for (int32_t k = olo; k < nlo; ++k) wf.set(k, OFFSET_NULL);
+      for (int32_t k = nhi + 1; k <= ohi; ++k) wf.set(k, OFFSET_NULL);
+    }
+    wf.lo = nlo;
+    wf.hi = nhi;
+  }
+  // endsfree_prune, :1214-1255: null the diagonals farther than
+  // (total - score) / -match from the end diagonal, in every component.
+  void endsfree_prune(int32_t score, int32_t total) {
+    const int32_t radius = (total - score) / -pen.match_;
+    const int32_t kend = tlen() - plen();
+    for (int c = 0; c < ncomp(); ++c) {
+      Wavefront* w = comps.get(c, score);
+      if (w) trim_nulled(*w, kend - radius, kend + radius);
+    }
+  }
+  // endsfree_dominance_prune, :1257-1320: trim from the ends the cells of a
+  // just-computed component that reach no further than a cell of that
+  // component did at an earlier score; with `record`, keep the kept offsets.
+  void dominance_prune(Wavefront& wf, int c, bool record) {
+    if (wf.lo > wf.hi) return;
+    const int32_t lo = wf.lo, n = wf.hi - wf.lo + 1;
+    int32_t* b = &dom_best[(size_t)c * dom_len + (size_t)(lo - dom_base)];
+    int32_t first = 0, last = n;
+    while (first < n && wf.get(lo + first) <= b[first]) ++first;
+    while (last > first && wf.get(lo + last - 1) <= b[last - 1]) --last;
+    if (record)
+      for (int32_t i = first; i < last; ++i) b[i] = std::max(b[i], wf.get(lo + i));
+    for (int32_t i = 0; i < first; ++i) wf.set(lo + i, OFFSET_NULL);
+    for (int32_t i = last; i < n; ++i) wf.set(lo + i, OFFSET_NULL);
+    if (first == last) { wf.lo = 1; wf.hi = 0; wf.null = true; }
+    else { wf.lo = lo + first; wf.hi = lo + last - 1; }
+  }
+  // endsfree_dominance_update, :1322-1338 (M, after extend)
+  void dominance_update(const Wavefront& wf, int c) {
+    if (wf.null || wf.lo > wf.hi) return;
+    int32_t* b = &dom_best[(size_t)c * dom_len + (size_t)(wf.lo - dom_base)];
+    for (int32_t k = wf.lo; k <= wf.hi; ++k) b[k - wf.lo] = std::max(b[k - wf.lo], wf.get(k));
+  }
+  // The dominance pruning of a compute step's outputs, after trim_ends
+  // (:1999-2001, :2187-2191, :2541-2550): M without recording, the gap
+  // components recording their kept offsets.
+  void dominance_outputs(int32_t score) {
+    if (dom_best.empty()) return;
+    for (int c = 0; c < ncomp(); ++c) {
+      Wavefront* w = comps.get(c, score);
+      if (w) dominance_prune(*w, c, c != CM);
+    }
+  }
+  // extend_endsfree_corrected, :1123-1211
+  bool extend_endsfree_corrected(int32_t score) {
+    Wavefront* m = comps.get(CM, score);
+    const bool prune = heur.kind == H_NONE || heur.kind == H_BANDED_STATIC;
+    if (prune && best.has && best.total > score) endsfree_prune(score, best.total);
+    if (m) {
+      int32_t k, off, left;
+      if (extend_endsfree_best_wf(*m, k, off, left)) {
+        const int32_t total = score + (-pen.match_) * left;
+        if (!best.has || total < best.total) {
+          best.has = true;
+          best.total = total;
+          best.pos = Pos{score, k, off};
+          if (prune && total > score) endsfree_prune(score, total);
+        }
+      }
+    }
+    if (!dom_best.empty() && !is_null_wf(m)) dominance_update(*m, CM);
+    if (best.has && best.total <= score) {  // no later cell can beat it
+      end_pos = best.pos;
+      status = END_REACHED;
+      return true;
+    }
+    bool done;
+    if (!m) done = !best.has && num_null_steps > (int32_t)comps.scope;
+    else done = heur.kind != H_NONE && apply_heuristic_cutoff(score, m);
+    if (done) {
+      if (best.has) { end_pos = best.pos; status = END_REACHED; }
+      else status = END_UNREACHABLE;
       return true;
     }
     return false;
@@ -1137,6 +1286,7 @@ class Aligner {
     }
     comps.set(CM, score, cur);
     trim_ends(n, m, *cur);
+    dominance_outputs(score);
   }
 
   // compute_linear_step, src/aligner.rs:1867-2003 (+ compute_linear_idm,
@@ -1183,6 +1333,7 @@ class Aligner {
     comps.set(CM, score, cur);
     if (endsfree_begin_k(score, bk)) endsfree_init(*cur, bk);
     trim_ends(n, m, *cur);
+    dominance_outputs(score);
   }
 
   // compute_affine_step, src/aligner.rs:2006-2193 and compute_affine2p_step,
@@ -1297,6 +1448,7 @@ class Aligner {
     trim_ends(n, m, *dc);
     if (i2c) trim_ends(n, m, *i2c);
     if (d2c) trim_ends(n, m, *d2c);
+    dominance_outputs(score);
   }
 
   void compute_step(int32_t score) {  // :3502-3509
@@ -1561,9 +1713,13 @@ class Aligner {
       backtrace_components(score, k, off, CM, CM);
     }
   }
-  void backtrace_zdrop_end(int32_t score) {  // :1397-1411 (C compatibility)
-    // Med/low read the end cell at the current score (where it may be dead).
-    int32_t from = (!piggyback && end_pos.score >= 0) ? end_pos.score : score;
+  void backtrace_zdrop_end(int32_t score) {  // :1393-1411
+    // C: med/low read the end cell at the current score (where it may be
+    // dead).  Corrected: every mode backtraces the best cell at the score it
+    // was found at (med/low from the backtrace kept then; every score's
+    // cells are kept here, so that is the cell's own chain).
+    int32_t from = compat == 1 ? end_pos.score
+                   : (!piggyback && end_pos.score >= 0) ? end_pos.score : score;
     backtrace_from(from, end_pos.k, end_pos.offset);
   }
 
@@ -1828,16 +1984,26 @@ class Aligner {
     int32_t result = score;
     if (status == END_REACHED || status == END_UNREACHABLE) {
       bool unreachable = status == END_UNREACHABLE;
+      // Corrected mode: the candidate's cell can be from an earlier score,
+      // and its total is the alignment's score (:772-777).
+      const bool cand = best.has && !unreachable;
+      if (cand) result = best.total;
       if (scope == SCOPE_ALIGNMENT && (status == END_REACHED || end_pos.offset != OFFSET_NULL)) {
-        if (unreachable) backtrace_zdrop_end(score);
-        else backtrace_from(score, end_pos.k, end_pos.offset);
+        if (cand) {
+          backtrace_from(best.pos.score, best.pos.k, best.pos.offset);
+          cigar.score = best.total;
+        } else if (unreachable) {
+          backtrace_zdrop_end(score);
+        } else {
+          backtrace_from(score, end_pos.k, end_pos.offset);
+        }
         if (extension || unreachable) {
           bool trimmed = maxtrim_cigar();
           status = (trimmed || unreachable) ? PARTIAL : COMPLETED;
         } else {
           cigar.end_v = end_pos.offset - end_pos.k;
           cigar.end_h = end_pos.offset;
-          result = rescore_heuristic_cigar(score);
+          if (!cand) result = rescore_heuristic_cigar(score);
           status = COMPLETED;
         }
       } else {
@@ -2095,6 +2261,7 @@ void* wfo_create(int metric, const int32_t* pen) {
 void wfo_destroy(void* h) { delete static_cast<Aligner*>(h); }
 void wfo_set_alignment_scope(void* h, int a) { static_cast<Aligner*>(h)->scope = a ? SCOPE_ALIGNMENT : SCOPE_SCORE; }
 void wfo_set_memory_mode(void* h, int mode) { static_cast<Aligner*>(h)->memory_mode = mode; }
+void wfo_set_compat(void* h, int compat) { static_cast<Aligner*>(h)->compat = compat; }
 void wfo_set_heuristic(void* h, int kind, int32_t p0, int32_t p1, int32_t p2) {
   Heuristic& hs = static_cast<Aligner*>(h)->heur;
   hs.kind = kind; hs.p0 = p0; hs.p1 = p1; hs.p2 = p2;
@@ -2182,7 +2349,13 @@ int32_t wfo_cli_line(void* h, int span, const int32_t* free4, int biwfa, int sco
   if (have_end_score) wfa_score = end_score;
   int32_t outscore;
   const Penalties& pen = a->pen;
-  if (failed_bi) {
+  // --no-c-compat: score-only output with no alignment behind it is -1
+  // (src/bin/align_benchmark.rs:396-405, 641-652).
+  const bool no_alignment =
+      failed_bi || (!biwfa && unreached && a->end_pos.offset == OFFSET_NULL);
+  if (score_only && a->compat == 1 && no_alignment) {
+    outscore = -1;
+  } else if (failed_bi) {
     outscore = INT32_MIN;
   } else if (!score_only) {
     const Cigar& c = a->cigar;
