@@ -2028,6 +2028,7 @@ class Aligner {
       bi_base.reset(new Aligner(pen));
       bi_base->scope = SCOPE_ALIGNMENT;
     }
+    bi_base->compat = compat;
   }
   // check_component_termination, :3268-3302
   bool check_component_termination(int32_t score, int comp) {
@@ -2144,8 +2145,14 @@ class Aligner {
       base.backtrace_components(score, pos.k, pos.offset, cb, ce);
       result = score;
     } else if (base.status == END_UNREACHABLE && pos.offset != OFFSET_NULL) {
-      int32_t from = pos.score >= 0 ? pos.score : score;
-      base.backtrace_components(from, pos.k, pos.offset, cb, ce);
+      // C: from component_end at the best cell's score; Corrected: from M
+      // (the best cell is an M cell), :3181-3192.
+      if (base.compat == 1) {
+        base.backtrace_components(pos.score, pos.k, pos.offset, cb, CM);
+      } else {
+        int32_t from = pos.score >= 0 ? pos.score : score;
+        base.backtrace_components(from, pos.k, pos.offset, cb, ce);
+      }
       base.maxtrim_cigar();
       st.kind = BI_UNATTAINABLE;
     } else {

@@ -4,6 +4,7 @@
 // them with the oracle so the kernel's logic is checked before it runs on a
 // GPU.  Not part of the product.
 #define WFA_EMU 1
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 #include <thread>
@@ -50,7 +51,9 @@ static bool run_pair(const AlignParams& P, int64_t i) {
   std::vector<int32_t> ringv((size_t)P.scope * NC * P.wmax, 0x5A5A5A5A);
   std::vector<int4> hist((size_t)P.hist_scores, int4{0, -1, 0, 0});
   std::vector<int32_t> harena((size_t)P.hist_words, 0x5A5A5A5A);
-  Workspace ws{ring.data(), ringv.data(), hist.data(), harena.data()};
+  std::vector<int32_t> dom((size_t)P.dom_words, 0x5A5A5A5A);
+  Workspace ws{ring.data(), ringv.data(), hist.data(), harena.data(),
+               P.dom_words ? dom.data() : nullptr};
 #ifdef WFA_EMU_THREADS
   EmuWarp warp;
   g_emu_warp = &warp;
@@ -76,7 +79,8 @@ extern "C" int64_t wfa_emu_batch(int metric, const int32_t* pen6, int compute_al
                                  const int64_t* p_off, const int32_t* p_len, const int64_t* t_off,
                                  const int32_t* t_len, int64_t num_pairs, const int64_t* cigar_off,
                                  uint8_t* cigars, wfa_result_t* results, int32_t wmax,
-                                 int32_t hist_scores, int64_t hist_words, int piggyback) {
+                                 int32_t hist_scores, int64_t hist_words, int piggyback,
+                                 int compat) {
   AlignParams P;
   std::memset(&P, 0, sizeof P);
   wfa_penalties_t u = {pen6[0], pen6[1], pen6[2], pen6[3], pen6[4], pen6[5]};
@@ -88,6 +92,7 @@ extern "C" int64_t wfa_emu_batch(int metric, const int32_t* pen6, int compute_al
   if (hp3) { P.hp0 = hp3[0]; P.hp1 = hp3[1]; P.hp2 = hp3[2]; }
   P.compute_alignment = compute_alignment;
   P.piggyback = piggyback;
+  P.compat = compat;
   P.max_steps = max_steps;
   P.format = format;
   P.seq = seq;
@@ -100,6 +105,10 @@ extern "C" int64_t wfa_emu_batch(int metric, const int32_t* pen6, int compute_al
   P.wmax = wmax;
   P.hist_scores = hist_scores;
   P.hist_words = hist_words;
+  int32_t max_len_sum = 0;
+  for (int64_t i = 0; i < num_pairs; ++i) max_len_sum = std::max(max_len_sum, p_len[i] + t_len[i]);
+  const int nc = metric == WFA_METRIC_GAP_AFFINE_2P ? 5 : metric == WFA_METRIC_GAP_AFFINE ? 3 : 1;
+  P.dom_words = (int64_t)nc * (max_len_sum + 2 * P.scope + 5);
   int64_t retries = 0;
   int cls = metric_class(metric);
   for (int64_t i = 0; i < num_pairs; ++i) {

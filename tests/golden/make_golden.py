@@ -57,10 +57,13 @@ cases = []
 
 
 def add(name, src, pairs, expected, algo="gap-affine-wfa", penalties=None, span="global",
-        score_only=False, memory="high", heuristic=None, hparams=None):
-    cases.append(dict(name=name, source=src, algo=algo, penalties=penalties, span=span,
-                      score_only=score_only, memory=memory, heuristic=heuristic,
-                      hparams=hparams, pairs=pairs, expected=expected))
+        score_only=False, memory="high", heuristic=None, hparams=None, no_c_compat=False):
+    case = dict(name=name, source=src, algo=algo, penalties=penalties, span=span,
+                score_only=score_only, memory=memory, heuristic=heuristic,
+                hparams=hparams, pairs=pairs, expected=expected)
+    if no_c_compat:  # the driver's --no-c-compat (Compat::Corrected)
+        case["no_c_compat"] = True
+    cases.append(case)
 
 
 cli = read("tests/cli_output.rs")
@@ -160,6 +163,11 @@ exp = re.search(r'assert_eq!\(run_file\("issue23_unreachable\.seq", &args\), "([
 add("issue23_unreachable", f"{CLI}:{a}-{b}", seq_file("tests/data/issue23_unreachable.seq"),
     [exp.group(1).encode().decode("unicode_escape").rstrip("\n")], penalties=pen,
     heuristic="xdrop", hparams=hp, score_only=True)
+exp = re.search(r'args\.push\("--no-c-compat"\);\s*assert_eq!\(run_file\("issue23_unreachable\.seq", '
+                r'&args\), "([^"]*)"\);', body)
+add("issue23_unreachable_corrected", f"{CLI}:{a}-{b}", seq_file("tests/data/issue23_unreachable.seq"),
+    [exp.group(1).encode().decode("unicode_escape").rstrip("\n")], penalties=pen,
+    heuristic="xdrop", hparams=hp, score_only=True, no_c_compat=True)
 m = re.search(r'assert_eq!\(run\("unreachable_bi", &pair, &args\), \["([^"]*)"\]\);', body)
 add("unreachable_biwfa_score", f"{CLI}:{a}-{b}", band_pair,
     [m.group(1).encode().decode("unicode_escape")], penalties=pen, memory="ultralow",

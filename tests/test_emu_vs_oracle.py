@@ -19,10 +19,12 @@ PENS = [(1, None), (0, None), (2, [0, 4, 2]), (2, [-1, 3, 2]), (3, [0, 4, 6, 2])
 HEUR = {"wfa-adaptive": 1, "xdrop": 2, "zdrop": 3, "banded-static": 4, "banded-adaptive": 5}
 
 
-def oracle_run(metric, pen, p, t, compute, span, free, hk, hp, extension=False, memory="high"):
+def oracle_run(metric, pen, p, t, compute, span, free, hk, hp, extension=False, memory="high",
+               compat=0):
     a = O.OracleAligner(metric, pen)
     a.set_alignment_scope(compute)
     a.set_memory_mode(memory)
+    a.set_compat(compat)
     if hk:
         a.set_heuristic(hk, *hp)
     if extension:
@@ -38,13 +40,13 @@ def oracle_run(metric, pen, p, t, compute, span, free, hk, hp, extension=False, 
 
 
 def compare(metric, pen, pairs, compute=True, span=0, free=None, hk=0, hp=(0, 0, 0),
-            extension=False, packed=False, memory="high"):
+            extension=False, packed=False, memory="high", compat=0):
     res, cig = emu_lib.run(metric, pen, pairs, compute_alignment=compute, span=span or int(extension),
                            extension=int(extension), free=free, heuristic=hk, hparams=hp,
-                           packed=packed, piggyback=compute and memory != "high")
+                           packed=packed, piggyback=compute and memory != "high", compat=compat)
     for i, (p, t) in enumerate(pairs):
         s, st, ops, ep, (cs, ev, eh) = oracle_run(metric, pen, p, t, compute, span, free, hk, hp,
-                                                  extension, memory)
+                                                  extension, memory, compat)
         r = res[i]
         got = (int(r["score"]), int(r["status"]), cig[i] if compute else "",
                (int(r["end_score"]), int(r["end_k"]), int(r["end_offset"])))
@@ -144,6 +146,45 @@ def test_piggyback_edges():
             compare(metric, pen, [(p, t)], span=1, free=free, memory="low")
 
 
+# Compat::Corrected: ends-free with a match reward (candidate, diagonal and
+# dominance pruning) and Z-drop ends.
+CORR_PENS = [(2, [-1, 3, 2]), (2, [-3, 4, 5]), (3, [-3, 5, 3, 2]), (3, [-5, 4, 0, 8]),
+             (4, [-1, 4, 6, 2, 24, 1]), (4, [-2, 4, 0, 6, 10, 2])]
+
+
+@pytest.mark.parametrize("metric,pen", CORR_PENS)
+@pytest.mark.parametrize("memory", ["high", "med"])
+def test_corrected_endsfree(metric, pen, memory):
+    r = random.Random(metric * 5 + len(memory))
+    for p, t in lcg_pairs(81 + metric, 24, 160):
+        n, m = len(p), len(t)
+        free = [r.choice([0, n, r.randrange(n + 1)]), r.choice([0, n, r.randrange(n + 1)]),
+                r.choice([0, m, r.randrange(m + 1)]), r.choice([0, m, r.randrange(m + 1)])]
+        compare(metric, pen, [(p, t)], span=1, free=free, memory=memory, compat=1)
+        compare(metric, pen, [(p, t)], compute=False, span=1, free=free, compat=1)
+
+
+@pytest.mark.parametrize("metric,pen", CORR_PENS)
+def test_corrected_dominance(metric, pen):
+    """Small begin-free tolerances: the dominance pruning is active."""
+    for i, (p, t) in enumerate(lcg_pairs(87 + metric, 30, 200)):
+        b = 1 + i % 5
+        e = 0 if i % 2 else min(16, len(p), len(t))
+        free = [min(b, len(p)), min(e, len(p)), min(b, len(t)), min(e, len(t))]
+        compare(metric, pen, [(p, t)], span=1, free=free, memory=["high", "low"][i % 2], compat=1)
+
+
+@pytest.mark.parametrize("metric,pen", CORR_PENS)
+def test_corrected_extension_and_heuristics(metric, pen):
+    pairs = lcg_pairs(91 + metric, 20, 200)
+    compare(metric, pen, pairs, extension=True, compat=1)
+    compare(metric, pen, pairs, extension=True, memory="med", compat=1)
+    for hk, hp in ((4, (-20, 20, 0)), (2, (30, 1, 0)), (3, (30, 1, 0)), (1, (10, 50, 1))):
+        compare(metric, pen, pairs, hk=hk, hp=hp, compat=1)
+        compare(metric, pen, pairs, hk=hk, hp=hp, memory="med", compat=1)
+        compare(metric, pen, pairs[:8], span=1, free=[5, 5, 5, 5], hk=hk, hp=hp, compat=1)
+
+
 def test_golden_cli_cases(golden):
     """The reference's CLI golden lines, reproduced by the device logic."""
     checked = 0
@@ -171,9 +212,11 @@ def test_golden_cli_cases(golden):
                 span = 1
             res, cig = emu_lib.run(metric, pen, [(pb, tb)], compute_alignment=not so, span=span,
                                    extension=ext, free=free, heuristic=hk, hparams=hp[:3],
-                                   piggyback=not so and case["memory"] != "high")
+                                   piggyback=not so and case["memory"] != "high",
+                                   compat=int(case.get("no_c_compat", False)))
             orig = (pen + [0] * 6)[:6]
-            lines.append(cli_format.line(metric, orig, so, False, res[0], cig[0], len(pb), len(tb)))
+            lines.append(cli_format.line(metric, orig, so, False, res[0], cig[0], len(pb), len(tb),
+                                         case.get("no_c_compat", False)))
         assert lines == case["expected"], case["name"]
         checked += 1
     assert checked >= 20

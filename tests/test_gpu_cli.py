@@ -28,6 +28,8 @@ def argv_for(case, seq, out):
     if case["score_only"]:
         argv.append("--wfa-score-only")
     argv += ["--wfa-memory", case["memory"], "--wfa-span", case["span"]]
+    if case.get("no_c_compat"):
+        argv.append("--no-c-compat")
     if case["heuristic"]:
         argv += ["--wfa-heuristic", case["heuristic"], f"--wfa-heuristic-parameters={case['hparams']}"]
     return argv

@@ -11,7 +11,7 @@ import pytest
 import cli_format
 import oracle as O
 from _pkg import load
-from test_emu_vs_oracle import HEUR, PENS
+from test_emu_vs_oracle import CORR_PENS, HEUR, PENS
 from test_oracle_unit import lcg_pairs
 
 pytestmark = pytest.mark.gpu
@@ -35,10 +35,11 @@ def pack(pairs):
 
 
 def gpu_batch(pkg, metric, pen, pairs, compute=True, span=0, free=None, hk=0, hp=(0, 0, 0),
-              extension=False, packed=False, memory="high"):
+              extension=False, packed=False, memory="high", compat=0):
     a = pkg.WavefrontAligner(metric, pen)
     a.set_alignment_scope(compute)
     a.set_memory_mode(memory)
+    a.set_compat(compat == 1)
     if hk:
         a.set_heuristic(hk, *hp)
     if extension:
@@ -59,10 +60,11 @@ def gpu_batch(pkg, metric, pen, pairs, compute=True, span=0, free=None, hk=0, hp
     return res, cigars
 
 
-def oracle_one(metric, pen, p, t, compute, span, free, hk, hp, extension, memory="high"):
+def oracle_one(metric, pen, p, t, compute, span, free, hk, hp, extension, memory="high", compat=0):
     a = O.OracleAligner(metric, pen)
     a.set_alignment_scope(compute)
     a.set_memory_mode(memory)
+    a.set_compat(compat)
     if hk:
         a.set_heuristic(hk, *hp)
     if extension:
@@ -78,12 +80,12 @@ def oracle_one(metric, pen, p, t, compute, span, free, hk, hp, extension, memory
 
 
 def compare(pkg, metric, pen, pairs, compute=True, span=0, free=None, hk=0, hp=(0, 0, 0),
-            extension=False, packed=False, memory="high"):
+            extension=False, packed=False, memory="high", compat=0):
     res, cig = gpu_batch(pkg, metric, pen, pairs, compute, span, free, hk, hp, extension, packed,
-                         memory)
+                         memory, compat)
     for i, (p, t) in enumerate(pairs):
         s, st, ops, ep, (cs, ev, eh) = oracle_one(metric, pen, p, t, compute, span, free, hk, hp,
-                                                  extension, memory)
+                                                  extension, memory, compat)
         r = res[i]
         got = (int(r["score"]), int(r["status"]), cig[i] if compute else "",
                (int(r["end_score"]), int(r["end_k"]), int(r["end_offset"])))
@@ -188,6 +190,55 @@ def test_reference_unit_cases_in_every_memory_mode(pkg, memory):
     assert a.cigar().to_string_rle() == "2I1M10I"
 
 
+@pytest.mark.parametrize("metric,pen", CORR_PENS)
+def test_corrected_endsfree(pkg, metric, pen):
+    """Compat::Corrected ends-free with a match reward (the end candidate and
+    the diagonal pruning), one batch per free-end setting."""
+    pairs = lcg_pairs(281 + metric, 40, 200)
+    for free in ([0, 40, 0, 40], [200, 200, 200, 200], [10, 60, 0, 200]):
+        fr = [[min(f, len(p) if i < 2 else len(t)) for i, f in enumerate(free)] for p, t in pairs]
+        for (p, t), f in zip(pairs, fr):
+            compare(pkg, metric, pen, [(p, t)], span=1, free=f, compat=1)
+    compare(pkg, metric, pen, pairs, extension=True, compat=1)
+    compare(pkg, metric, pen, pairs, extension=True, memory="med", compat=1)
+    compare(pkg, metric, pen, pairs, compute=False, extension=True, compat=1)
+
+
+@pytest.mark.parametrize("metric,pen", CORR_PENS)
+def test_corrected_dominance_and_heuristics(pkg, metric, pen):
+    pairs = lcg_pairs(283 + metric, 40, 200)
+    for i, (p, t) in enumerate(pairs[:16]):
+        b, e = 1 + i % 5, 0 if i % 2 else 16
+        free = [min(b, len(p)), min(e, len(p)), min(b, len(t)), min(e, len(t))]
+        compare(pkg, metric, pen, [(p, t)], span=1, free=free, memory=["high", "low"][i % 2], compat=1)
+    for hk, hp in ((4, (-20, 20, 0)), (2, (30, 1, 0)), (3, (30, 1, 0)), (1, (10, 50, 1))):
+        compare(pkg, metric, pen, pairs, hk=hk, hp=hp, compat=1)
+        compare(pkg, metric, pen, pairs, hk=hk, hp=hp, memory="med", compat=1)
+
+
+def test_corrected_reference_cases(pkg, golden):
+    """tests/corrected_endsfree.rs issue_37_repeat_shift (the corrected CIGAR
+    and real score) and tests/corrected_zdrop.rs issue_22_corrected_modes_agree."""
+    a = pkg.WavefrontAligner(3, [-5, 4, 0, 8])
+    a.set_compat(True)
+    a.set_alignment_scope(True)
+    a.set_alignment_free_ends(12, 12, 11, 11)
+    w = a.align_endsfree(b"ACGTACGTACGT", b"ACGACGTACGT")
+    assert (5 * 23 - w) // 2 == 47 and a.cigar().operations == b"MMMDMMMMMMMM"
+    x = golden["extra"]["issue22_zdrop_high"]
+    (p, t), = x["pairs"]
+    got = set()
+    for memory in ("high", "med", "low"):
+        a = pkg.WavefrontAligner(3, x["penalties"])
+        a.set_compat(True)
+        a.set_memory_mode(memory)
+        a.set_alignment_scope(True)
+        a.set_heuristic("zdrop", *x["zdrop"])
+        a.align_end2end(p.encode(), t.encode())
+        got.add(cli_format.classic_score(3, x["penalties"] + [0, 0], a.cigar().operations.decode()))
+    assert got == {x["cigar_affine_score"]}
+
+
 def test_med_low_long_pairs(pkg):
     """Pairs long enough to outgrow the first history size re-run and match."""
     r = random.Random(29)
@@ -213,6 +264,7 @@ def test_plain_calls_and_golden_cli(pkg, golden):
         a = pkg.WavefrontAligner(metric, pen)
         a.set_alignment_scope(not so)
         a.set_memory_mode(case["memory"])
+        a.set_compat(case.get("no_c_compat", False))
         if case["heuristic"]:
             a.set_heuristic(case["heuristic"], *[int(x) for x in case["hparams"].split(",")])
         span_s = case["span"]
@@ -233,7 +285,8 @@ def test_plain_calls_and_golden_cli(pkg, golden):
             es, ek, eo = a.alignment_end_pos
             rec = {"score": s, "status": a.status(), "end_score": es, "end_k": ek, "end_offset": eo}
             orig = (pen + [0] * 6)[:6]
-            lines.append(cli_format.line(metric, orig, so, False, rec, c.operations.decode(), len(pb), len(tb)))
+            lines.append(cli_format.line(metric, orig, so, False, rec, c.operations.decode(), len(pb), len(tb),
+                                         case.get("no_c_compat", False)))
         assert lines == case["expected"], case["name"]
 
 

@@ -121,6 +121,8 @@ def main(argv=None):
     ap.add_argument("--wfa-heuristic")
     ap.add_argument("--wfa-heuristic-parameters")
     ap.add_argument("--wfa-max-steps", type=int)
+    ap.add_argument("--no-c-compat", action="store_true",
+                    help="fix known C WFA2-lib bugs instead of reproducing them (Compat::Corrected)")
     ap.add_argument("--device", type=int, default=0, help="CUDA device")
     args = ap.parse_args(argv)
 
@@ -149,6 +151,8 @@ def main(argv=None):
     except ValueError as e:
         die(f"[WFA] {e}")
     a.set_alignment_scope(not score_only)
+    if args.no_c_compat:
+        a.set_compat(True)
     if heur is not None and heur[0] != "none":
         a.set_heuristic(heur[0], *heur[1])
     if not biwfa:
@@ -179,7 +183,8 @@ def main(argv=None):
                 es, ek, eo = a.alignment_end_pos
                 rec = {"score": s, "status": a.status(), "end_score": es, "end_k": ek, "end_offset": eo}
                 ops = "" if score_only else a.cigar().operations.decode()
-                lines.append(cli_format.line(metric, orig, score_only, False, rec, ops, len(p), len(t)))
+                lines.append(cli_format.line(metric, orig, score_only, False, rec, ops, len(p), len(t),
+                                             args.no_c_compat))
         elif pairs:
             buf, po, pl, to, tl = bytearray(), [], [], [], []
             for p, t in pairs:
@@ -193,7 +198,8 @@ def main(argv=None):
                 r = res[i]
                 ops = "" if score_only else \
                     cig[r["cigar_begin"]:r["cigar_begin"] + r["cigar_length"]].tobytes().decode()
-                lines.append(cli_format.line(metric, orig, score_only, biwfa, r, ops, len(p), len(t)))
+                lines.append(cli_format.line(metric, orig, score_only, biwfa, r, ops, len(p), len(t),
+                                             args.no_c_compat))
     except NotImplementedError as e:
         die(f"[WFA] not available on the GPU build: {e}")
     ms = (time.perf_counter() - t0) * 1000.0

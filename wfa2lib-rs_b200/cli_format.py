@@ -7,6 +7,8 @@ match reward, Eizenga-corrected) WFA score in score-only mode, INT_MIN for a
 failed BiWFA score-only run and -1 with an empty CIGAR; the CIGAR column is
 the run-length string (Cigar::to_string_rle) or "-".  `r` is a mapping with
 the fields of wfa_result_t (score, status, end_score, end_k, end_offset).
+With `corrected` (the driver's --no-c-compat), a score-only run with no
+alignment behind it prints -1 (:396-405, :641-652).
 """
 INT_MIN = -2**31
 NULL = -(2**30)
@@ -49,16 +51,19 @@ def classic_score(metric, orig, ops):
     return s
 
 
-def line(metric, orig, score_only, biwfa, r, ops, n, m):
+def line(metric, orig, score_only, biwfa, r, ops, n, m, corrected=False):
     status = int(r["status"])
     completed = status == 5
     failed_bi = biwfa and score_only and not completed
+    no_alignment = failed_bi or (not biwfa and status in (6, 2) and int(r["end_offset"]) == NULL)
     ev, eh, wfa_score = n, m, int(r["score"])
     if not biwfa and status in (6, 2):
         ev, eh = _wrap(int(r["end_offset"]) - int(r["end_k"])), int(r["end_offset"])
         if int(r["end_score"]) >= 0:
             wfa_score = int(r["end_score"])
-    if failed_bi:
+    if score_only and corrected and no_alignment:
+        out = -1
+    elif failed_bi:
         out = INT_MIN
     elif not score_only:
         out = -1 if not ops else classic_score(metric, orig, ops)

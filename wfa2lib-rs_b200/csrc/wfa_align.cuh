@@ -35,6 +35,7 @@
 #else
 #include <algorithm>
 #include <climits>
+#include <cstdlib>
 #ifndef __CUDACC__
 struct int4 { int x, y, z, w; };
 #endif
@@ -240,6 +241,7 @@ struct Workspace {
   int32_t* ringv;   // [scope][NC][wmax] cells
   int4* hist;       // [hist_scores] M history records {a, b, cell offset of a, present}
   int32_t* harena;  // M history cells
+  int32_t* dom;     // Corrected-mode dominance array (NC x diagonals), or null
 };
 
 // GEN = false compiles the common configuration only (end-to-end, no
@@ -277,6 +279,14 @@ struct PairAligner {
   // seed at +k, bit 1 pattern seed at -k), stored with M's history record.
   bool pgb = false;
   int32_t seed_flags = 0;
+  // Compat::Corrected ends-free with a match reward (src/aligner.rs:1104-1345):
+  // the end candidate (the best cell reaching a free end so far, its total
+  // score) and the begin-free dominance array (ws.dom, NC x diagonals from
+  // hist_lo, the furthest offset each diagonal reached at an earlier score).
+  bool corr = false, dom_on = false;
+  bool c_has = false;
+  int32_t c_total = 0, c_score = 0, c_k = 0, c_off = 0;
+  int32_t dom_len = 0;
   int32_t comp_end;  // component whose end diagonal terminates (BiWFA), else M
   int32_t cscore, cidx;  // current score and its ring index
   // Scores that are not multiples of gstep can have no wavefront: every input
@@ -512,6 +522,20 @@ struct PairAligner {
                     : (hk() == WFA_HEURISTIC_XDROP || hk() == WFA_HEURISTIC_ZDROP) ? hp1 : 0;
     hs.max_sw_score = 0; hs.max_wf_score = 0; hs.max_sw_k = kDiagNull;
     hs.max_sw_off = kOffsetNull; hs.zdrop_last = 0;
+    // Corrected mode (src/aligner.rs:912-947): no candidate yet; dominance
+    // pruning only with begin-free seeds (at most 4 bases unless gap-linear)
+    // and no heuristic that reads the wavefronts.
+    corr = ef() && P.compat == WFA_COMPAT_CORRECTED && P.match < 0;
+    c_has = false;
+    const int bfree = imax(p0, t0);
+    dom_on = corr && bfree > 0 && (CLS == kLinearClass || bfree <= 4) &&
+             (hk() == WFA_HEURISTIC_NONE || hk() == WFA_HEURISTIC_BANDED_STATIC);
+    if (dom_on) {
+      dom_len = hist_hi - hist_lo + 1;
+      if (!ws.dom || (int64_t)NC * dom_len > P.dom_words) { retry = true; return; }
+      for (int64_t i = lane; i < (int64_t)NC * dom_len; i += WFA_WARP) ws.dom[i] = -1;
+      Warp::sync();
+    }
     int lo0 = 0, hi0 = 0;
     bool seeds = ef() && P.match == 0;
     if (seeds) { lo0 = -p0; hi0 = t0; }
@@ -887,6 +911,151 @@ struct PairAligner {
     if (CLS == kEditClass) compute_edit(s);
     else if (CLS == kLinearClass) compute_linear(s);
     else compute_affine(s);
+    // Dominance pruning of the outputs, after their trims (src/aligner.rs:
+    // 1999-2001, 2187-2191, 2541-2550): M without recording, the gap
+    // components recording the offsets they keep.
+    if (dom_on && !retry)
+      for (int c = 0; c < NC; ++c) dom_prune(s, c, c != CM);
+  }
+
+  // ---- Compat::Corrected ends-free ---------------------------------------------
+  // NULL cells [from, to] of a stored wavefront (inside its initialised range).
+  WFA_D void null_cells(const WfD& d, int from, int to) {
+    from = imax(from, d.a);
+    to = imin(to, d.b);
+    for (int k = from + lane; k <= to; k += WFA_WARP) d.vals[k - d.a] = kOffsetNull;
+  }
+  // Wavefront::trim_nulled (src/wavefront.rs:463-490) of component c at s.
+  WFA_D void trim_nulled(int c, int s, int lo, int hi) {
+    WfD d = slot(c, s);
+    Warp::sync();
+    if (!wf_present(d) || (d.flags & kNullFlag) || d.lo > d.hi || (lo <= d.lo && hi >= d.hi)) return;
+    const int nlo = imax(lo, d.lo), nhi = imin(hi, d.hi);
+    if (nlo > nhi) {
+      null_cells(d, d.lo, d.hi);
+      d.flags |= kNullFlag;
+    } else {
+      null_cells(d, d.lo, nlo - 1);
+      null_cells(d, nhi + 1, d.hi);
+    }
+    d.lo = nlo;
+    d.hi = nhi;
+    put(c, s, d);
+  }
+  // endsfree_prune (src/aligner.rs:1214-1255): null, in every component at
+  // s, the diagonals farther than (total - s) / -match from the end diagonal.
+  WFA_D void ef_prune(int s, int total) {
+    const int radius = (total - s) / -P.match, kend = m - n;
+    for (int c = 0; c < NC; ++c) trim_nulled(c, s, kend - radius, kend + radius);
+  }
+  // endsfree_dominance_prune (src/aligner.rs:1257-1320): trim from the ends
+  // the cells of component c at s that reach no further than a cell of c did
+  // at an earlier score; with `record`, keep the kept offsets.
+  WFA_D void dom_prune(int s, int c, bool record) {
+    WfD d = slot(c, s);
+    Warp::sync();
+    if (!wf_present(d) || d.lo > d.hi) return;
+    int32_t* b = ws.dom + (int64_t)c * dom_len + (d.lo - hist_lo);
+    const int cnt = d.hi - d.lo + 1;
+#if !(defined(__CUDACC__) && !defined(WFA_EMU))
+    if (d.lo < hist_lo || d.hi - hist_lo >= dom_len) std::abort();  // emulation-only check
+#endif
+    int first = cnt, last = -1;
+    for (int i = lane; i < cnt; i += WFA_WARP)
+      if (d.vals[d.lo + i - d.a] > b[i]) { first = imin(first, i); last = imax(last, i); }
+    first = Warp::min(first);
+    last = Warp::max(last) + 1;  // one past the last kept cell
+    if (first >= cnt) last = first;
+    if (record)
+      for (int i = first + lane; i < last; i += WFA_WARP) b[i] = imax(b[i], d.vals[d.lo + i - d.a]);
+    null_cells(d, d.lo, d.lo + first - 1);
+    null_cells(d, d.lo + last, d.hi);
+    if (first == last) {
+      d.lo = 1;
+      d.hi = 0;
+      d.flags |= kNullFlag;
+    } else {
+      d.hi = d.lo + last - 1;
+      d.lo = d.lo + first;
+    }
+    Warp::sync();
+    put(c, s, d);
+  }
+  // endsfree_dominance_update (src/aligner.rs:1322-1338): M after extend.
+  WFA_D void dom_update(int s) {
+    WfD d = slot(CM, s);
+    if (wf_is_null(d) || d.lo > d.hi) return;
+    int32_t* b = ws.dom + (d.lo - hist_lo);
+#if !(defined(__CUDACC__) && !defined(WFA_EMU))
+    if (d.lo < hist_lo || d.hi - hist_lo >= dom_len) std::abort();  // emulation-only check
+#endif
+    for (int k = d.lo + lane; k <= d.hi; k += WFA_WARP) b[k - d.lo] = imax(b[k - d.lo], d.vals[k - d.a]);
+    Warp::sync();
+  }
+  // extend_matches_packed_endsfree_best (src/extend.rs:179-232): extend every
+  // cell and find the free-end cell leaving the fewest bases to its free end
+  // gap (endsfree_left, src/termination.rs:65-86), the lowest diagonal on ties.
+  WFA_D bool extend_best(WfD& d, int& rk, int& roff, int& rleft) {
+    int bl = INT_MAX, bkk = INT_MAX;
+    for (int k = d.lo + lane; k <= d.hi; k += WFA_WARP) {
+      int32_t off = d.vals[k - d.a];
+      if (off < 0) continue;  // NULL (M offsets are valid or NULL)
+      int v = off - k, h = off;
+      int R = imin(n - v, m - h);
+      if (R > 0) {
+        off += lcp_fwd(pat, v, txt, h, R);
+        d.vals[k - d.a] = off;
+        v = off - k;
+        h = off;
+      }
+      const bool by_t = h >= m && n - v <= pf, by_p = v >= n && m - h <= tf;
+      if (by_t || by_p) {
+        const int left = by_t && by_p ? imin(n - v, m - h) : by_t ? n - v : m - h;
+        if (left < bl) { bl = left; bkk = k; }
+      }
+    }
+    Warp::sync();
+    rleft = Warp::min(bl);
+    if (rleft == INT_MAX) return false;
+    rk = Warp::min(bl == rleft ? bkk : INT_MAX);
+    roff = d.vals[rk - d.a];
+    return true;
+  }
+  // extend_endsfree_corrected (src/aligner.rs:1123-1211).
+  WFA_D bool extend_step_corrected(int score) {
+    const bool prune = hk() == WFA_HEURISTIC_NONE || hk() == WFA_HEURISTIC_BANDED_STATIC;
+    if (prune && c_has && c_total > score) ef_prune(score, c_total);
+    WfD d = slot(CM, score);
+    Warp::sync();
+    if (wf_present(d)) {
+      int k, off, left;
+      if (extend_best(d, k, off, left)) {
+        const int total = score + (-P.match) * left;
+        if (!c_has || total < c_total) {
+          c_has = true; c_total = total; c_score = score; c_k = k; c_off = off;
+          if (prune && total > score) ef_prune(score, total);
+        }
+      }
+      if (dom_on) dom_update(score);
+    }
+    if (c_has && c_total <= score) {  // no later cell can beat the candidate
+      end_score = c_score; end_k = c_k; end_off = c_off;
+      status = WFA_STATUS_END_REACHED;
+      return true;
+    }
+    bool done;
+    if (!wf_present(d)) done = !c_has && num_null_steps > scope;
+    else done = hk() != WFA_HEURISTIC_NONE && apply_heuristic(score);
+    if (done) {
+      if (c_has) {
+        end_score = c_score; end_k = c_k; end_off = c_off;
+        status = WFA_STATUS_END_REACHED;
+      } else {
+        status = WFA_STATUS_END_UNREACHABLE;
+      }
+      return true;
+    }
+    return false;
   }
 
   // ---- extend ----------------------------------------------------------------
@@ -1087,6 +1256,7 @@ struct PairAligner {
 
   // extend_end2end (src/aligner.rs:1004-1050) / extend_endsfree (:1053-1101).
   WFA_D bool extend_step(int score) {
+    if (GEN && corr) return extend_step_corrected(score);
     WfD d = slot(CM, score);
     if (!wf_present(d)) {
       if (num_null_steps > scope) { status = WFA_STATUS_END_UNREACHABLE; return true; }
@@ -1744,6 +1914,15 @@ struct PairAligner {
     return r;
   }
 
+  // The score a Z-drop end is backtraced from (backtrace_zdrop_end,
+  // src/aligner.rs:1393-1411): C reads med/low at the current score (where
+  // the cell may be dead), high memory at the best cell's score; Corrected
+  // reads every mode at the best cell's score.
+  WFA_D int zdrop_from(int score) const {
+    if (P.compat == WFA_COMPAT_CORRECTED) return end_score;
+    return end_score >= 0 && !pgb ? end_score : score;
+  }
+
   // ---- one pair: align_end2end_span (src/aligner.rs:638-698) and
   // align_endsfree (:707-831), C compatibility ----------------------------------
   WFA_D int32_t align() {
@@ -1757,8 +1936,16 @@ struct PairAligner {
       for (;;) {
         bool done;
         if (gphase != 0) {  // all-null score: no M to extend (extend_end2end, null branch)
-          done = num_null_steps > scope;
-          if (done) status = WFA_STATUS_END_UNREACHABLE;
+          if (GEN && corr && c_has && c_total <= score) {
+            // Corrected: the candidate is final once the score reaches its
+            // total; null steps do not end the search while one is pending.
+            done = true;
+            end_score = c_score; end_k = c_k; end_off = c_off;
+            status = WFA_STATUS_END_REACHED;
+          } else {
+            done = !(GEN && corr && c_has) && num_null_steps > scope;
+            if (done) status = WFA_STATUS_END_UNREACHABLE;
+          }
           if (!modular) {
             if ((int64_t)(score + 1) * hist_nc > P.hist_scores) { retry = true; break; }
             if (lane == 0)
@@ -1793,16 +1980,22 @@ struct PairAligner {
         if (status != WFA_STATUS_OOM) status = WFA_STATUS_COMPLETED;
       } else if (status == WFA_STATUS_END_UNREACHABLE && end_off != kOffsetNull) {
         if (cigar) {
-          backtrace_from(end_score >= 0 && !pgb ? end_score : score, end_k, end_off);
+          backtrace_from(zdrop_from(score), end_k, end_off);
           maxtrim_cigar();
         }
         if (status != WFA_STATUS_OOM) status = WFA_STATUS_PARTIAL;
       }
     } else if (status == WFA_STATUS_END_REACHED || status == WFA_STATUS_END_UNREACHABLE) {
       bool unreachable = status == WFA_STATUS_END_UNREACHABLE;
+      // Corrected mode: the candidate's cell can be from an earlier score,
+      // and its total is the alignment's score (src/aligner.rs:772-777).
+      const bool cand = GEN && corr && c_has && !unreachable;
+      if (cand) result = c_total;
       if (cigar && (status == WFA_STATUS_END_REACHED || end_off != kOffsetNull)) {
-        if (unreachable) backtrace_from(end_score >= 0 && !pgb ? end_score : score, end_k, end_off);
+        if (cand) backtrace_from(c_score, c_k, c_off);
+        else if (unreachable) backtrace_from(zdrop_from(score), end_k, end_off);
         else backtrace_from(score, end_k, end_off);
+        if (cand) cg_score = c_total;
         if (status == WFA_STATUS_OOM) return result;
         if (P.extension || unreachable) {
           bool trimmed = maxtrim_cigar();
@@ -1810,7 +2003,7 @@ struct PairAligner {
         } else {
           cg_ev = end_off - end_k;
           cg_eh = end_off;
-          result = rescore_heuristic(score);
+          if (!cand) result = rescore_heuristic(score);
           status = WFA_STATUS_COMPLETED;
         }
       } else {

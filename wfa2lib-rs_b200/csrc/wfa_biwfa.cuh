@@ -272,8 +272,14 @@ struct BiDriver {
       base.backtrace_components(score, base.end_k, base.end_off, ce);
       result = score;
     } else if (base.status == WFA_STATUS_END_UNREACHABLE && base.end_off != kOffsetNull) {
-      int from = base.end_score >= 0 ? base.end_score : score;
-      base.backtrace_components(from, base.end_k, base.end_off, ce);
+      // C: from component_end at the best cell's score; Corrected: from M
+      // (the best cell is an M cell), src/aligner.rs:3181-3192.
+      if (P.compat == WFA_COMPAT_CORRECTED) {
+        base.backtrace_components(base.end_score, base.end_k, base.end_off, CM);
+      } else {
+        int from = base.end_score >= 0 ? base.end_score : score;
+        base.backtrace_components(from, base.end_k, base.end_off, ce);
+      }
       base.maxtrim_cigar();
       st = BI_UNATTAINABLE;
     } else {

@@ -62,6 +62,7 @@ struct ScratchCfg {
   int32_t wmax;
   int32_t hist_scores;
   int64_t hist_words;
+  int64_t dom_words = 0;  // Corrected-mode dominance array per warp
 };
 
 }  // namespace
@@ -192,8 +193,6 @@ __global__ void max_lengths(const int32_t* pl, const int32_t* tl, int64_t n, int
 // Configuration checks
 // ---------------------------------------------------------------------------
 static int check_supported(wfa_aligner_t* h, bool biwfa) {
-  if (!biwfa && h->compat == WFA_COMPAT_CORRECTED && h->pen.match < 0 && h->span == WFA_SPAN_ENDSFREE)
-    return fail(h, WFA_ERR_UNSUPPORTED, "Compat::Corrected ends-free with a match reward");
   if (h->pen.scope > 1024) return fail(h, WFA_ERR_UNSUPPORTED, "max_score_scope above 1024");
   return WFA_OK;
 }
@@ -208,6 +207,7 @@ static void fill_params(const wfa_aligner_t* h, const wfa_batch_t* b, AlignParam
   // Med/low with an alignment: the piggyback backtrace (BiWFA ignores the mode).
   P.piggyback = P.compute_alignment && h->memory_mode != WFA_MEMORY_HIGH &&
                 b->span != WFA_SPAN_BIWFA;
+  P.compat = h->compat;
   P.max_steps = h->max_steps;
   P.format = b->format;
   P.seq = static_cast<const uint8_t*>(b->seq);
@@ -248,10 +248,19 @@ struct Round {
 // late in a long alignment repeats most of its work.
 static constexpr int32_t kLongPair = 2048;
 
+// The widest wavefront storage a pair can need: computed diagonals are
+// clamped to [-(n + scope + 1), m + scope + 1] (src/aligner.rs:915-924), and a
+// score with begin-free seeds (k = score / -match <= max(n, m)) covers
+// [-k, k] as well (:3426-3452).  Searches that run on past the sequence ends
+// (Corrected ends-free, whole-length free ends) reach these bounds.
+static int32_t max_width(const AlignParams& P, int32_t max_len_sum) {
+  return 2 * (max_len_sum + P.scope) + 5;
+}
+
 static Round first_round(const AlignParams& P, int nc, int32_t max_len_sum) {
   Round r;
   const bool longp = max_len_sum > kLongPair;
-  r.cfg.wmax = std::max(8, std::min(max_len_sum + 3, 8192));
+  r.cfg.wmax = std::max(8, std::min(max_width(P, max_len_sum), 8192));
   // The piggyback backtrace keeps every component's history.
   const int hnc = P.piggyback ? nc : 1;
   r.cfg.hist_scores = P.compute_alignment ? hnc * (longp ? max_len_sum + 3 : 1024) : 0;
@@ -260,15 +269,20 @@ static Round first_round(const AlignParams& P, int nc, int32_t max_len_sum) {
                          : 0;
   r.ring_smem = !longp && (size_t)P.scope * nc * kRingSmemWidth * 4 <= kRingSmemBudget;
   if (r.ring_smem) r.cfg.wmax = std::min(r.cfg.wmax, kRingSmemWidth);
+  // Corrected ends-free with begin-free seeds prunes dominated cells against
+  // a per-diagonal array over [-(n + scope + 2), m + scope + 2] per component.
+  const bool dom = P.compat == WFA_COMPAT_CORRECTED && P.match < 0 && P.span == WFA_SPAN_ENDSFREE &&
+                   !P.extension && std::max(P.p0, P.t0) > 0;
+  r.cfg.dom_words = dom ? (int64_t)nc * ((int64_t)max_len_sum + 2 * P.scope + 5) : 0;
   return r;
 }
 
 static void next_round(Round& r, const AlignParams& P, int32_t max_len_sum) {
   if (r.ring_smem) {
     r.ring_smem = false;  // retries use the scratch ring at full width
-    r.cfg.wmax = std::max(8, std::min(max_len_sum + 3, 8192));
+    r.cfg.wmax = std::max(8, std::min(max_width(P, max_len_sum), 8192));
   } else {
-    r.cfg.wmax = std::min(max_len_sum + 3, std::max(r.cfg.wmax, 1) * 4);
+    r.cfg.wmax = std::min(max_width(P, max_len_sum), std::max(r.cfg.wmax, 1) * 4);
   }
   if (P.compute_alignment) {
     r.cfg.hist_scores *= 4;
@@ -295,7 +309,7 @@ static int launch_round(wfa_aligner_t* h, AlignParams& P, const Round& r, int64_
     h->occ_smem = smem;
   }
   int64_t ring_words = r.ring_smem ? 0 : (((int64_t)P.scope * nc * r.cfg.wmax + 3) & ~(int64_t)3);
-  int64_t warp_words = ring_words + (int64_t)r.cfg.hist_scores * 4 + r.cfg.hist_words;
+  int64_t warp_words = ring_words + (int64_t)r.cfg.hist_scores * 4 + r.cfg.hist_words + r.cfg.dom_words;
   warp_words = std::max<int64_t>((warp_words + 63) & ~(int64_t)63, 64);
   int64_t max_warps = (int64_t)h->num_sms * h->occ_val * kWarpsPerBlock;
   int64_t warps = std::max<int64_t>(std::min<int64_t>(max_warps, todo), 1);
@@ -309,6 +323,7 @@ static int launch_round(wfa_aligner_t* h, AlignParams& P, const Round& r, int64_
   P.warp_words = warp_words;
   P.hist_scores = r.cfg.hist_scores;
   P.hist_words = r.cfg.hist_words;
+  P.dom_words = r.cfg.dom_words;
   P.work_counter = h->counters.as<unsigned long long>();
   P.retry_count = reinterpret_cast<int32_t*>(P.work_counter + 1);
   P.pair_list = list;
@@ -543,7 +558,7 @@ static int run_noalloc_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_
       h->occ_smem = L.total;
     }
     int64_t ring_words = r.ring_smem ? 0 : (((int64_t)P.scope * nc * r.cfg.wmax + 3) & ~(int64_t)3);
-    int64_t warp_words = ring_words + (int64_t)r.cfg.hist_scores * 4 + r.cfg.hist_words;
+    int64_t warp_words = ring_words + (int64_t)r.cfg.hist_scores * 4 + r.cfg.hist_words + r.cfg.dom_words;
     warp_words = std::max<int64_t>((warp_words + 63) & ~(int64_t)63, 64);
     const int64_t fit_blocks = kNaSliceWords / (warp_words * kWarpsPerBlock);
     if (fit_blocks < 1)
@@ -556,6 +571,7 @@ static int run_noalloc_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_
     P.warp_words = warp_words;
     P.hist_scores = r.cfg.hist_scores;
     P.hist_words = r.cfg.hist_words;
+    P.dom_words = r.cfg.dom_words;
     P.work_counter = work;
     P.retry_count = retry;
     P.pair_list = lst;

@@ -34,6 +34,8 @@ struct AlignParams {
   // 1: med/low memory with an alignment -- the piggyback backtrace (every
   // component's history, no score cap).
   int32_t piggyback;
+  // Compat: 0 C (reproduce C's known bugs), 1 Corrected (src/aligner.rs:53-94).
+  int32_t compat;
   int32_t max_steps;
   // Input.
   int32_t format;  // wfa_seq_format_t
@@ -58,6 +60,7 @@ struct AlignParams {
   int32_t max_len_sum;     // longest n + m of the launch
   int32_t hist_scores; // M history capacity (scores)
   int64_t hist_words;  // M history arena capacity (cells)
+  int64_t dom_words;   // Corrected-mode dominance array per warp (cells; 0: none)
   unsigned long long* work_counter;
   int32_t* retry_count;
 };

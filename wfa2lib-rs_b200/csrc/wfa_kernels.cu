@@ -40,6 +40,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (min_blocks<CLS, GEN>()))
                          : slice;
   ws.hist = reinterpret_cast<int4*>(slice + ring_words);
   ws.harena = slice + ring_words + (int64_t)P.hist_scores * 4;
+  ws.dom = P.dom_words ? ws.harena + P.hist_words : nullptr;
   const int sw = P.seq_smem_words;
   for (;;) {
     unsigned long long idx = 0;
