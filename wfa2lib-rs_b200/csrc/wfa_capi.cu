@@ -8,6 +8,8 @@
 // WFA_ERR_UNSUPPORTED.
 #include <cuda_runtime.h>
 
+#include <cub/block/block_scan.cuh>
+
 #include <algorithm>
 #include <condition_variable>
 #include <cstdio>
@@ -91,8 +93,12 @@ struct wfa_aligner {
   cudaStream_t stream = nullptr;    // compute (every kernel of the handle)
   cudaStream_t s_in = nullptr;      // host->device copies
   cudaStream_t s_out = nullptr;     // device->host copies
+  cudaStream_t s_cig = nullptr;     // device->host copies of packed CIGARs (host-buffer batch)
   int num_sms = 148;
   DevBuf seq, poff, plen, toff, tlen, coff, results, cigars, dense, scratch, counters, pairlist;
+  DevBuf chunkinfo;               // per-chunk counters and dense CIGAR ranges
+  int64_t* hinfo = nullptr;       // pinned host copy of the chunk info
+  size_t hinfo_cap = 0;
   int64_t launches = 0;
   uint8_t* pinned = nullptr;  // host staging for the plain per-call form
   size_t pinned_cap = 0;
@@ -123,6 +129,78 @@ struct wfa_aligner {
 };
 
 // At least `count` pooled events in h->evpool.
+// Pinned host words for the per-chunk info of the host-buffer batch.
+static cudaError_t host_info(wfa_aligner_t* h, size_t words) {
+  if (h->hinfo_cap >= words) return cudaSuccess;
+  if (h->hinfo) cudaFreeHost(h->hinfo);
+  h->hinfo = nullptr;
+  h->hinfo_cap = 0;
+  void* p = nullptr;
+  cudaError_t e = cudaHostAlloc(&p, std::max<size_t>(words, 64) * 8, cudaHostAllocDefault);
+  if (e != cudaSuccess) return e;
+  h->hinfo = static_cast<int64_t*>(p);
+  h->hinfo_cap = std::max<size_t>(words, 64);
+  return cudaSuccess;
+}
+
+// What the host-buffer batch needs to know of a chunk of pairs before it is
+// copied in: the byte range of the sequence buffer it reads (16-byte
+// aligned), its longest pair (n + m) and its CIGAR slot bytes.
+struct ChunkInfo {
+  int64_t lo = INT64_MAX, hi = 0;
+  int32_t max_len_sum = 0;
+  int64_t slots = 0;
+};
+static void scan_chunks(const wfa_batch_t* b, int64_t n, int64_t chunk, bool packed, bool aln,
+                        std::vector<ChunkInfo>& out) {
+  const int64_t nchunks = (int64_t)out.size();
+  const int64_t unit = packed ? 4 : 1;  // bytes per offset unit
+  // One pass over [i0, i1), accumulated per chunk into `acc`.
+  auto pass = [&](int64_t i0, int64_t i1, std::vector<ChunkInfo>& acc) {
+    for (int64_t i = i0; i < i1;) {
+      const int64_t ci = i / chunk, e = std::min(i1, (ci + 1) * chunk);
+      ChunkInfo& c = acc[(size_t)ci];
+      int64_t lo = c.lo, hi = c.hi, slots = c.slots;
+      int32_t mx = c.max_len_sum;
+      for (; i < e; ++i) {
+        const int64_t pl = b->p_len[i], tl = b->t_len[i], po = b->p_off[i], to = b->t_off[i];
+        const int64_t pe = packed ? (po + (pl + 15) / 16) * 4 : po + pl;
+        const int64_t te = packed ? (to + (tl + 15) / 16) * 4 : to + tl;
+        lo = std::min(lo, std::min(po, to) * unit);
+        hi = std::max(hi, std::max(pe, te));
+        mx = std::max<int32_t>(mx, (int32_t)(pl + tl));
+        slots += 2 * (pl + tl) + 1;
+      }
+      c.lo = lo; c.hi = hi; c.slots = slots; c.max_len_sum = mx;
+    }
+  };
+  const int64_t kPerThread = 131072;
+  const int nt = (int)std::max<int64_t>(1, std::min<int64_t>(8, n / kPerThread));
+  std::vector<std::vector<ChunkInfo>> part((size_t)nt, std::vector<ChunkInfo>((size_t)nchunks));
+  if (nt == 1) {
+    pass(0, n, part[0]);
+  } else {
+    std::vector<std::thread> th;
+    for (int t = 0; t < nt; ++t)
+      th.emplace_back(pass, n * t / nt, n * (t + 1) / nt, std::ref(part[(size_t)t]));
+    for (auto& x : th) x.join();
+  }
+  for (int64_t ci = 0; ci < nchunks; ++ci) {
+    ChunkInfo c;
+    for (int t = 0; t < nt; ++t) {
+      const ChunkInfo& p = part[(size_t)t][(size_t)ci];
+      c.lo = std::min(c.lo, p.lo);
+      c.hi = std::max(c.hi, p.hi);
+      c.max_len_sum = std::max(c.max_len_sum, p.max_len_sum);
+      c.slots += p.slots;
+    }
+    c.lo = c.lo == INT64_MAX ? 0 : (c.lo & ~(int64_t)15);
+    c.hi = std::min<int64_t>(b->seq_bytes, (c.hi + 15) & ~(int64_t)15);
+    if (!aln) c.slots = 0;
+    out[(size_t)ci] = c;
+  }
+}
+
 static cudaError_t event_pool(wfa_aligner_t* h, size_t count) {
   while (h->evpool.size() < count) {
     cudaEvent_t e = nullptr;
@@ -168,8 +246,8 @@ __global__ void collect_retries(const wfa_result_t* res, const int64_t* list, in
 }
 
 // Copies every pair's CIGAR from its slot to dense[dst_off[i]..] (one warp
-// per pair, coalesced byte copies).
-__global__ void compact_cigars(const wfa_result_t* res, const int64_t* slot_off,
+// per pair, coalesced byte copies) and makes that its cigar_begin.
+__global__ void compact_cigars(wfa_result_t* res, const int64_t* slot_off,
                                const uint8_t* slots, const int64_t* dst_off, uint8_t* dense,
                                int64_t n) {
   int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -179,6 +257,79 @@ __global__ void compact_cigars(const wfa_result_t* res, const int64_t* slot_off,
   const uint8_t* src = slots + slot_off[w] + res[w].cigar_begin;
   uint8_t* dst = dense + dst_off[w];
   for (int32_t i = lane; i < len; i += 32) dst[i] = src[i];
+  __syncwarp();
+  if (lane == 0) res[w].cigar_begin = (int32_t)dst_off[w];  // now an offset into the dense bytes
+}
+
+// Exclusive prefix sums of a chunk's per-pair values, in three short
+// launches (tile sums, a one-block scan of the tile sums, the tiles' own
+// scans): MODE 0 the CIGAR slot sizes 2 (n + m) + 1 from the lengths, MODE 1
+// the CIGAR lengths of the results (0 for pairs to be re-run).
+constexpr int kScanBlock = 256, kScanItems = 8, kScanTile = kScanBlock * kScanItems;
+template <int MODE>
+__device__ __forceinline__ long long scan_value(const int32_t* pl, const int32_t* tl,
+                                                const wfa_result_t* res, int64_t i) {
+  if (MODE == 0) return 2ll * ((long long)pl[i] + tl[i]) + 1;
+  return res[i].status == kStatusRetry ? 0 : res[i].cigar_length;
+}
+template <int MODE, bool APPLY>
+__global__ void __launch_bounds__(kScanBlock)
+    scan_tiles(const int32_t* pl, const int32_t* tl, const wfa_result_t* res, int64_t n,
+               long long* tile, int64_t* out) {
+  using Scan = cub::BlockScan<long long, kScanBlock>;
+  __shared__ typename Scan::TempStorage tmp;
+  const int64_t i0 = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+  long long v[kScanItems], sum = 0;
+  for (int j = 0; j < kScanItems; ++j) {
+    v[j] = i0 + j < n ? scan_value<MODE>(pl, tl, res, i0 + j) : 0;
+    sum += v[j];
+  }
+  long long excl, total;
+  Scan(tmp).ExclusiveSum(sum, excl, total);
+  if (!APPLY) {
+    if (threadIdx.x == 0) tile[blockIdx.x] = total;
+    return;
+  }
+  long long run = tile[blockIdx.x] + excl;
+  for (int j = 0; j < kScanItems; ++j) {
+    if (i0 + j < n) out[i0 + j] = run;
+    run += v[j];
+  }
+}
+// The tile sums in place become tile offsets from the chunk's base: `base0`,
+// or *base (then advanced past the chunk).  range = [begin, end).
+__global__ void __launch_bounds__(1024)
+    scan_tile_offsets(long long* tile, int64_t ntiles, int64_t base0, int64_t* base, int64_t* range) {
+  using Scan = cub::BlockScan<long long, 1024>;
+  __shared__ typename Scan::TempStorage tmp;
+  __shared__ long long carry;
+  if (threadIdx.x == 0) carry = base ? *base : base0;
+  __syncthreads();
+  const long long begin = carry;
+  for (int64_t t0 = 0; t0 < ntiles; t0 += 1024) {
+    const int64_t t = t0 + threadIdx.x;
+    const long long v = t < ntiles ? tile[t] : 0;
+    long long excl, total;
+    Scan(tmp).ExclusiveSum(v, excl, total);
+    if (t < ntiles) tile[t] = carry + excl;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += total;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    if (base) *base = carry;
+    if (range) { range[0] = begin; range[1] = carry; }
+  }
+}
+template <int MODE>
+static cudaError_t chunk_scan(const int32_t* pl, const int32_t* tl, const wfa_result_t* res, int64_t n,
+                              int64_t base0, int64_t* base, int64_t* out, int64_t* range, long long* tile,
+                              cudaStream_t st) {
+  const int64_t ntiles = (n + kScanTile - 1) / kScanTile;
+  if (ntiles > 0) scan_tiles<MODE, false><<<(unsigned)ntiles, kScanBlock, 0, st>>>(pl, tl, res, n, tile, out);
+  scan_tile_offsets<<<1, 1024, 0, st>>>(tile, ntiles, base0, base, range);
+  if (ntiles > 0) scan_tiles<MODE, true><<<(unsigned)ntiles, kScanBlock, 0, st>>>(pl, tl, res, n, tile, out);
+  return cudaGetLastError();
 }
 
 __global__ void max_lengths(const int32_t* pl, const int32_t* tl, int64_t n, int32_t* out) {
@@ -293,7 +444,7 @@ static void next_round(Round& r, const AlignParams& P, int32_t max_len_sum) {
 // Sizes the scratch for round r and launches the alignment kernel over
 // `todo` pairs (`list`: their indices, or NULL for 0..todo-1).  No sync.
 static int launch_round(wfa_aligner_t* h, AlignParams& P, const Round& r, int64_t todo,
-                        const int64_t* list, cudaStream_t st) {
+                        const int64_t* list, cudaStream_t st, unsigned long long* ctr = nullptr) {
   const int cls = metric_class(P.metric);
   const int nc = metric_components(P.metric);
   P.seq_smem_words = kSeqSmemWords;
@@ -324,7 +475,7 @@ static int launch_round(wfa_aligner_t* h, AlignParams& P, const Round& r, int64_
   P.hist_scores = r.cfg.hist_scores;
   P.hist_words = r.cfg.hist_words;
   P.dom_words = r.cfg.dom_words;
-  P.work_counter = h->counters.as<unsigned long long>();
+  P.work_counter = ctr ? ctr : h->counters.as<unsigned long long>();
   P.retry_count = reinterpret_cast<int32_t*>(P.work_counter + 1);
   P.pair_list = list;
   P.num_pairs = todo;
@@ -645,13 +796,14 @@ wfa_aligner_t* wfa_aligner_create(wfa_metric_t metric, const wfa_penalties_t* pe
   if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&h->s_in, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&h->s_out, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&h->s_cig, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess) {
     delete h;
     if (err) *err = WFA_ERR_CUDA;
     return nullptr;
   }
   for (DevBuf* b : {&h->seq, &h->poff, &h->plen, &h->toff, &h->tlen, &h->coff, &h->results,
-                    &h->cigars, &h->dense, &h->scratch, &h->counters, &h->pairlist})
+                    &h->cigars, &h->dense, &h->scratch, &h->counters, &h->pairlist, &h->chunkinfo})
     b->st = h->stream;
   if (event_pool(h, 32) != cudaSuccess) {
     wfa_aligner_destroy(h);
@@ -673,18 +825,21 @@ void wfa_aligner_destroy(wfa_aligner_t* h) {
     h->async_worker.join();
   }
   cudaSetDevice(h->device);
-  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (cudaStream_t x : {h->stream, h->s_in, h->s_out, h->s_cig})
+    if (x) cudaStreamSynchronize(x);
   for (DevBuf* b : {&h->seq, &h->poff, &h->plen, &h->toff, &h->tlen, &h->coff, &h->results,
-                    &h->cigars, &h->dense, &h->scratch, &h->counters, &h->pairlist})
+                    &h->cigars, &h->dense, &h->scratch, &h->counters, &h->pairlist, &h->chunkinfo})
     b->release();
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->pinned) cudaFreeHost(h->pinned);
+  if (h->hinfo) cudaFreeHost(h->hinfo);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   for (cudaEvent_t e : h->evpool) cudaEventDestroy(e);
   if (h->stream) cudaStreamDestroy(h->stream);
   if (h->s_in) cudaStreamDestroy(h->s_in);
   if (h->s_out) cudaStreamDestroy(h->s_out);
+  if (h->s_cig) cudaStreamDestroy(h->s_cig);
   delete h;
 }
 
@@ -1032,11 +1187,14 @@ static int batch_align_simple(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result
 }
 
 // Host-buffer batch, pipelined in chunks of pairs: while chunk c aligns on
-// the compute stream, chunk c+1's inputs are copied in and chunk c-1's results
-// and CIGARs are copied out.  CIGARs are packed densely per chunk, in input
-// order; results[i].cigar_begin is the offset of pair i's ops in `cigars`.
-// Pairs that need more scratch than the first configuration are re-run at
-// the end by the batch driver.
+// the compute stream, chunk c+1's inputs are copied in and chunk c-1's packed
+// CIGARs (packed on the device right after its alignment: a prefix sum of
+// the CIGAR lengths, then the compaction) are copied out with its results.
+// The host only waits for each chunk's results to issue the copy of its
+// packed CIGAR bytes.  CIGARs are
+// packed densely in input order; results[i].cigar_begin is the offset of
+// pair i's ops in `cigars`.  Pairs that need more scratch than the first
+// configuration are re-run at the end by the batch driver.
 int wfa_batch_align(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* results, uint8_t* cigars) {
   int r = batch_common(h, b);
   if (r != WFA_OK) return r;
@@ -1048,38 +1206,18 @@ int wfa_batch_align(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* result
   cudaSetDevice(h->device);
   if (b->span == WFA_SPAN_BIWFA) return batch_align_simple(h, b, results, cigars);
   cudaStream_t sc = h->stream, si = h->s_in, so = h->s_out;
-  const int64_t chunk = std::max<int64_t>(65536, std::min<int64_t>(262144, (n + 3) / 4));
+  const int64_t chunk = std::max<int64_t>(65536, std::min<int64_t>(262144, (n + 7) / 8));
   const int64_t nchunks = (n + chunk - 1) / chunk;
   const bool packed = b->format == WFA_SEQ_PACKED2;
-  const int64_t unit = packed ? 4 : 1;  // bytes per offset unit
 
-  // Per chunk: sequence byte range, longest pair, CIGAR slot range.
-  std::vector<int64_t> slot_off(aln ? (size_t)n : 0);
-  std::vector<int64_t> c_lo((size_t)nchunks), c_hi((size_t)nchunks), c_slot0((size_t)nchunks + 1);
-  std::vector<int32_t> c_max((size_t)nchunks);
-  int64_t slot_total = 0;
-  for (int64_t ci = 0; ci < nchunks; ++ci) {
-    int64_t a = ci * chunk, e = std::min(n, a + chunk);
-    int64_t lo = INT64_MAX, hi = 0;
-    int32_t mx = 0;
-    c_slot0[(size_t)ci] = slot_total;
-    for (int64_t i = a; i < e; ++i) {
-      int64_t pl = b->p_len[i], tl = b->t_len[i];
-      int64_t pe = packed ? b->p_off[i] * 4 + (pl + 15) / 16 * 4 : b->p_off[i] + pl;
-      int64_t te = packed ? b->t_off[i] * 4 + (tl + 15) / 16 * 4 : b->t_off[i] + tl;
-      lo = std::min(lo, std::min(b->p_off[i], b->t_off[i]) * unit);
-      hi = std::max(hi, std::max(pe, te));
-      mx = std::max<int32_t>(mx, (int32_t)(pl + tl));
-      if (aln) {
-        slot_off[(size_t)i] = slot_total;
-        slot_total += 2 * (pl + tl) + 1;
-      }
-    }
-    c_lo[(size_t)ci] = lo == INT64_MAX ? 0 : (lo & ~(int64_t)15);
-    c_hi[(size_t)ci] = std::min<int64_t>(b->seq_bytes, (hi + 15) & ~(int64_t)15);
-    c_max[(size_t)ci] = mx;
-  }
-  c_slot0[(size_t)nchunks] = slot_total;
+  // Per chunk: sequence byte range, longest pair, CIGAR slot bytes -- one
+  // pass over the host arrays, split across host threads.
+  std::vector<ChunkInfo> ci_info((size_t)nchunks);
+  scan_chunks(b, n, chunk, packed, aln, ci_info);
+  std::vector<int64_t> c_slot0((size_t)nchunks + 1, 0);
+  for (int64_t ci = 0; ci < nchunks; ++ci)
+    c_slot0[(size_t)ci + 1] = c_slot0[(size_t)ci] + ci_info[(size_t)ci].slots;
+  const int64_t slot_total = c_slot0[(size_t)nchunks];
 
   size_t seq_bytes = ((size_t)b->seq_bytes + 15) & ~(size_t)15;
   CUDA_TRY(h, h->seq.ensure(seq_bytes + 16), "seq");
@@ -1094,41 +1232,58 @@ int wfa_batch_align(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* result
     CUDA_TRY(h, h->dense.ensure((size_t)slot_total + 16), "dense cigars");
     CUDA_TRY(h, h->pairlist.ensure((size_t)n * 8), "dense offsets");
   }
+  // Per chunk on the device: work/retry counters (2 words) and the dense
+  // CIGAR range [begin, end) (2 words), plus the running dense total.
+  const int64_t ntiles = (chunk + kScanTile - 1) / kScanTile;
+  CUDA_TRY(h, h->chunkinfo.ensure((size_t)(4 * nchunks + 1 + ntiles) * 8), "chunk counters");
+  CUDA_TRY(h, host_info(h, (size_t)nchunks * 4), "pinned chunk info");
   CUDA_TRY(h, event_pool(h, 4 * (size_t)nchunks), "events");
   cudaEvent_t* ev_in = h->evpool.data();
   cudaEvent_t* ev_k = ev_in + nchunks;
-  cudaEvent_t* ev_res = ev_k + nchunks;
-  cudaEvent_t* ev_off = ev_res + nchunks;
-  auto destroy = []() {};  // the events stay in the handle's pool
+  cudaEvent_t* ev_x = ev_k + nchunks;
+  cudaEvent_t* ev_res = ev_x + nchunks;
   uint8_t* dseq = h->seq.as<uint8_t>();
   int64_t *dpo = h->poff.as<int64_t>(), *dto = h->toff.as<int64_t>();
   int32_t *dpl = h->plen.as<int32_t>(), *dtl = h->tlen.as<int32_t>();
   wfa_result_t* dres = h->results.as<wfa_result_t>();
   int64_t* dco = aln ? h->coff.as<int64_t>() : nullptr;
   int64_t* ddst = aln ? h->pairlist.as<int64_t>() : nullptr;
+  unsigned long long* dctr = h->chunkinfo.as<unsigned long long>();  // [chunk][work, retry]
+  int64_t* drange = reinterpret_cast<int64_t*>(dctr + 2 * nchunks);    // [chunk][begin, end]
+  int64_t* dtotal = drange + 2 * nchunks;                               // running dense total
+  long long* dtile = reinterpret_cast<long long*>(dtotal + 1);           // scan tile sums
+  int64_t* hinfo = h->hinfo;                                            // [chunk][begin, end, retry, -]
   h->last_kernel_ms = 0.0;
 
-#define PIPE_TRY(expr, what)                                                         \
-  do {                                                                               \
-    cudaError_t _e = (expr);                                                         \
-    if (_e != cudaSuccess) {                                                         \
-      destroy();                                                                     \
-      return fail(h, _e == cudaErrorMemoryAllocation ? WFA_ERR_OOM : WFA_ERR_CUDA, what, _e); \
-    }                                                                                \
+#define PIPE_TRY(expr, what)                                                                      \
+  do {                                                                                            \
+    cudaError_t _e = (expr);                                                                      \
+    if (_e != cudaSuccess)                                                                        \
+      return fail(h, _e == cudaErrorMemoryAllocation ? WFA_ERR_OOM : WFA_ERR_CUDA, what, _e);     \
   } while (0)
 
-  // Phase 1, every chunk: inputs in (s_in), align (compute), results out (s_out).
+  if (aln) PIPE_TRY(cudaMemsetAsync(dtotal, 0, 8, sc), "memset");
+  // Every chunk: inputs in (s_in); slot offsets, the alignment, the dense
+  // CIGAR offsets and the compaction (compute stream, a few short launches
+  // around the alignment kernel); results, chunk info and CIGAR bytes out
+  // (s_out) while the next chunk aligns.
   for (int64_t ci = 0; ci < nchunks; ++ci) {
     const int64_t a = ci * chunk, e = std::min(n, a + chunk), cn = e - a;
-    const size_t lo = (size_t)c_lo[(size_t)ci], hi = (size_t)c_hi[(size_t)ci];
-    if (hi > lo) PIPE_TRY(cudaMemcpyAsync(dseq + lo, (const uint8_t*)b->seq + lo, hi - lo, cudaMemcpyHostToDevice, si), "H2D");
+    const ChunkInfo& I = ci_info[(size_t)ci];
+    if (I.hi > I.lo)
+      PIPE_TRY(cudaMemcpyAsync(dseq + I.lo, (const uint8_t*)b->seq + I.lo, (size_t)(I.hi - I.lo),
+                               cudaMemcpyHostToDevice, si), "H2D");
     PIPE_TRY(cudaMemcpyAsync(dpo + a, b->p_off + a, (size_t)cn * 8, cudaMemcpyHostToDevice, si), "H2D");
     PIPE_TRY(cudaMemcpyAsync(dto + a, b->t_off + a, (size_t)cn * 8, cudaMemcpyHostToDevice, si), "H2D");
     PIPE_TRY(cudaMemcpyAsync(dpl + a, b->p_len + a, (size_t)cn * 4, cudaMemcpyHostToDevice, si), "H2D");
     PIPE_TRY(cudaMemcpyAsync(dtl + a, b->t_len + a, (size_t)cn * 4, cudaMemcpyHostToDevice, si), "H2D");
-    if (aln) PIPE_TRY(cudaMemcpyAsync(dco + a, slot_off.data() + a, (size_t)cn * 8, cudaMemcpyHostToDevice, si), "H2D");
     PIPE_TRY(cudaEventRecord(ev_in[(size_t)ci], si), "event");
     PIPE_TRY(cudaStreamWaitEvent(sc, ev_in[(size_t)ci], 0), "wait");
+    if (aln) {
+      PIPE_TRY(chunk_scan<0>(dpl + a, dtl + a, nullptr, cn, c_slot0[(size_t)ci], nullptr, dco + a, nullptr,
+                             dtile, sc), "slot offsets");
+      h->launches += 3;
+    }
     wfa_batch_t cb = *b;
     cb.num_pairs = cn;
     cb.seq = dseq;
@@ -1140,50 +1295,52 @@ int wfa_batch_align(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* result
     fill_params(h, &cb, P);
     P.results = dres + a;
     P.cigars = aln ? h->cigars.as<uint8_t>() : nullptr;
-    Round rd = first_round(P, metric_components(P.metric), c_max[(size_t)ci]);
-    int e2 = launch_round(h, P, rd, cn, nullptr, sc);
-    if (e2 != WFA_OK) { destroy(); return e2; }
+    Round rd = first_round(P, metric_components(P.metric), I.max_len_sum);
+    int e2 = launch_round(h, P, rd, cn, nullptr, sc, dctr + 2 * ci);
+    if (e2 != WFA_OK) return e2;
     PIPE_TRY(cudaEventRecord(ev_k[(size_t)ci], sc), "event");
-    PIPE_TRY(cudaStreamWaitEvent(so, ev_k[(size_t)ci], 0), "wait");
+    cudaEvent_t ready = ev_k[(size_t)ci];
+    if (aln) {
+      PIPE_TRY(chunk_scan<1>(nullptr, nullptr, dres + a, cn, 0, dtotal, ddst + a, drange + 2 * ci, dtile,
+                             sc), "dense offsets");
+      compact_cigars<<<(unsigned)((cn * 32 + 255) / 256), 256, 0, sc>>>(
+          dres + a, dco + a, h->cigars.as<uint8_t>(), ddst + a, h->dense.as<uint8_t>(), cn);
+      h->launches += 4;
+      PIPE_TRY(cudaGetLastError(), "compact cigars");
+      PIPE_TRY(cudaEventRecord(ev_x[(size_t)ci], sc), "event");
+      ready = ev_x[(size_t)ci];
+    }
+    PIPE_TRY(cudaStreamWaitEvent(so, ready, 0), "wait");
     PIPE_TRY(cudaMemcpyAsync(results + a, dres + a, (size_t)cn * sizeof(wfa_result_t), cudaMemcpyDeviceToHost, so), "D2H");
+    if (aln)
+      PIPE_TRY(cudaMemcpyAsync(hinfo + 4 * ci, drange + 2 * ci, 16, cudaMemcpyDeviceToHost, so), "D2H");
+    PIPE_TRY(cudaMemcpyAsync(hinfo + 4 * ci + 2, dctr + 2 * ci + 1, 8, cudaMemcpyDeviceToHost, so), "D2H");
     PIPE_TRY(cudaEventRecord(ev_res[(size_t)ci], so), "event");
   }
 
-  // Phase 2, as each chunk's results arrive: dense CIGAR offsets (host), then
-  // compaction (compute stream) and the dense copy out (s_out).
-  std::vector<int64_t> dst(aln ? (size_t)n : 0);
+  // As each chunk's info arrives: its dense CIGAR bytes out, on their own
+  // stream (s_out already holds every later chunk's result copies).
   std::vector<int64_t> retry;
   int64_t dense_total = 0;
   for (int64_t ci = 0; ci < nchunks; ++ci) {
-    const int64_t a = ci * chunk, e = std::min(n, a + chunk), cn = e - a;
+    const int64_t a = ci * chunk, e = std::min(n, a + chunk);
     PIPE_TRY(cudaEventSynchronize(ev_res[(size_t)ci]), "results");
-    const int64_t d0 = dense_total;
-    for (int64_t i = a; i < e; ++i) {
-      if (results[i].status == kStatusRetry) { retry.push_back(i); results[i].cigar_length = 0; }
-      if (aln) {
-        dst[(size_t)i] = dense_total;
-        dense_total += results[i].cigar_length;
-      }
-    }
-    if (!aln || dense_total == d0) continue;
-    PIPE_TRY(cudaMemcpyAsync(ddst + a, dst.data() + a, (size_t)cn * 8, cudaMemcpyHostToDevice, si), "H2D");
-    PIPE_TRY(cudaEventRecord(ev_off[(size_t)ci], si), "event");
-    PIPE_TRY(cudaStreamWaitEvent(sc, ev_off[(size_t)ci], 0), "wait");
-    compact_cigars<<<(unsigned)((cn * 32 + 255) / 256), 256, 0, sc>>>(
-        dres + a, dco + a, h->cigars.as<uint8_t>(), ddst + a, h->dense.as<uint8_t>(), cn);
-    h->launches++;
-    PIPE_TRY(cudaGetLastError(), "compact cigars");
-    PIPE_TRY(cudaEventRecord(ev_k[(size_t)ci], sc), "event");
-    PIPE_TRY(cudaStreamWaitEvent(so, ev_k[(size_t)ci], 0), "wait");
-    PIPE_TRY(cudaMemcpyAsync(cigars + d0, h->dense.as<uint8_t>() + d0, (size_t)(dense_total - d0),
-                             cudaMemcpyDeviceToHost, so), "D2H");
+    const int32_t nretry = (int32_t)(hinfo[4 * ci + 2] & 0xffffffff);
+    if (nretry > 0)
+      for (int64_t i = a; i < e; ++i)
+        if (results[i].status == kStatusRetry) { retry.push_back(i); results[i].cigar_length = 0; }
+    if (!aln) continue;
+    const int64_t d0 = hinfo[4 * ci], d1 = hinfo[4 * ci + 1];
+    if (d1 > d0)
+      PIPE_TRY(cudaMemcpyAsync(cigars + d0, h->dense.as<uint8_t>() + d0, (size_t)(d1 - d0),
+                               cudaMemcpyDeviceToHost, h->s_cig), "D2H");
+    dense_total = d1;
   }
   PIPE_TRY(cudaStreamSynchronize(so), "D2H");
+  PIPE_TRY(cudaStreamSynchronize(h->s_cig), "D2H");
   PIPE_TRY(cudaStreamSynchronize(sc), "compute");
-  destroy();
 #undef PIPE_TRY
-  for (int64_t i = 0; i < n; ++i)
-    if (aln) results[i].cigar_begin = (int32_t)dst[(size_t)i];
+
 
   // Pairs that outgrew the first configuration: re-run with the batch driver.
   if (!retry.empty()) {
