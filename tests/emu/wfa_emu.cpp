@@ -40,7 +40,8 @@ static bool run_lane_g(const AlignParams& P, const Workspace& ws, int64_t i) {
 // end-to-end alignments without a heuristic, the general one otherwise.
 template <int CLS>
 static bool run_lane(const AlignParams& P, const Workspace& ws, int64_t i) {
-  if (P.span == WFA_SPAN_END2END && P.hkind == WFA_HEURISTIC_NONE) return run_lane_g<CLS, false>(P, ws, i);
+  if (P.span == WFA_SPAN_END2END && P.hkind == WFA_HEURISTIC_NONE && !P.piggyback)
+    return run_lane_g<CLS, false>(P, ws, i);
   return run_lane_g<CLS, true>(P, ws, i);
 }
 

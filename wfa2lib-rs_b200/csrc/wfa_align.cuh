@@ -358,7 +358,7 @@ struct PairAligner {
         if (hused + w > P.hist_words) { retry = true; return; }
         for (int64_t i = lane; i < w; i += WFA_WARP) ws.harena[hused + i] = d.vals[i];
         r.z = (int32_t)hused;
-        r.w = c == CM ? 1 | (seed_flags << 1) : 1;
+        r.w = GEN && c == CM ? 1 | (seed_flags << 1) : 1;
         hused += w;
       }
       if (lane == 0) ws.hist[(int64_t)s * hist_nc + c] = r;
@@ -525,10 +525,10 @@ struct PairAligner {
     // Corrected mode (src/aligner.rs:912-947): no candidate yet; dominance
     // pruning only with begin-free seeds (at most 4 bases unless gap-linear)
     // and no heuristic that reads the wavefronts.
-    corr = ef() && P.compat == WFA_COMPAT_CORRECTED && P.match < 0;
+    corr = GEN && ef() && P.compat == WFA_COMPAT_CORRECTED && P.match < 0;
     c_has = false;
     const int bfree = imax(p0, t0);
-    dom_on = corr && bfree > 0 && (CLS == kLinearClass || bfree <= 4) &&
+    dom_on = GEN && corr && bfree > 0 && (CLS == kLinearClass || bfree <= 4) &&
              (hk() == WFA_HEURISTIC_NONE || hk() == WFA_HEURISTIC_BANDED_STATIC);
     if (dom_on) {
       dom_len = hist_hi - hist_lo + 1;
@@ -914,7 +914,7 @@ struct PairAligner {
     // Dominance pruning of the outputs, after their trims (src/aligner.rs:
     // 1999-2001, 2187-2191, 2541-2550): M without recording, the gap
     // components recording the offsets they keep.
-    if (dom_on && !retry)
+    if (GEN && dom_on && !retry)
       for (int c = 0; c < NC; ++c) dom_prune(s, c, c != CM);
   }
 
@@ -1755,7 +1755,7 @@ struct PairAligner {
 
   WFA_D void backtrace_from(int score, int k, int offset) {  // src/aligner.rs:1414-1436
     Warp::sync();
-    if (pgb) {
+    if (GEN && pgb) {
       backtrace_piggyback(score, k, offset);
       cg_score = score;
       Warp::sync();
@@ -1919,8 +1919,8 @@ struct PairAligner {
   // the cell may be dead), high memory at the best cell's score; Corrected
   // reads every mode at the best cell's score.
   WFA_D int zdrop_from(int score) const {
-    if (P.compat == WFA_COMPAT_CORRECTED) return end_score;
-    return end_score >= 0 && !pgb ? end_score : score;
+    if (GEN && P.compat == WFA_COMPAT_CORRECTED) return end_score;
+    return end_score >= 0 && !(GEN && pgb) ? end_score : score;
   }
 
   // ---- one pair: align_end2end_span (src/aligner.rs:638-698) and
@@ -2028,7 +2028,7 @@ WFA_D bool align_one(const AlignParams& P, const Workspace& ws, int64_t pair, S 
   A.scope = P.scope;
   A.wmax = P.wmax;
   A.modular = P.compute_alignment == 0;
-  A.pgb = !A.modular && P.piggyback != 0;
+  A.pgb = GEN && !A.modular && P.piggyback != 0;
   // Med/low components are modular: no score cap.
   A.cap = A.modular || A.pgb ? INT_MAX : imax(A.dims_num(1000, 1000), A.dims_num(A.n, A.m));
   A.endsfree = P.span == WFA_SPAN_ENDSFREE;

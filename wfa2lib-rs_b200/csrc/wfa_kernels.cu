@@ -130,8 +130,11 @@ static cudaError_t launch_g(const AlignParams& P, int cls, int blocks, size_t sm
   }
 }
 
+// The lean instantiation runs end-to-end high-memory alignments without a
+// heuristic; everything else (ends-free, heuristics, the med/low piggyback
+// backtrace) runs the general one.
 bool needs_general(const AlignParams& P) {
-  return P.span != WFA_SPAN_END2END || P.hkind != WFA_HEURISTIC_NONE;
+  return P.span != WFA_SPAN_END2END || P.hkind != WFA_HEURISTIC_NONE || P.piggyback;
 }
 
 cudaError_t launch_unialign(const AlignParams& P, int metric_class, int blocks, size_t smem,
