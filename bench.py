@@ -160,6 +160,20 @@ def dram_traffic(kind, pairs):
     return None
 
 
+def profile_figure(name, kind):
+    """A per-pair figure of the workload's ncu capture (profiles/<name>_<kind>.txt,
+    a line `<name> <value>`), or None without one."""
+    path = os.path.join(ROOT, "profiles", f"{name}_{kind}.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith(name):
+                    return float(line.split()[1])
+    except OSError:
+        pass
+    return None
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -362,6 +376,17 @@ def run_gpu(args):
                          "kernel_ms": kms, "algorithmic_bytes_per_launch": alg_bytes},
             "gpu_launches": int(launches),
             "clocks": clk.summary()}
+    # The alignment kernel is bound by instruction issue: warp instructions
+    # per pair (ncu) x pairs/s against 4 schedulers x SMs x the sampled clock.
+    ipp = profile_figure("warp_inst_per_pair", args.workload)
+    if ipp is not None:
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        mhz = line["clocks"].get("sm_mhz") or 1965.0
+        issue_peak = 4 * sms * mhz * 1e6
+        issue = value / world * ipp
+        line["roofline_issue"] = {"bound": "issue", "achieved": issue, "peak": issue_peak,
+                                  "unit": "warp-inst/s", "frac": issue / issue_peak,
+                                  "warp_inst_per_pair": ipp}
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
         rate, m, secs = cpu_baseline(ps, threads, max_pairs=args.cpu_sample, metric=metric, pen=pen,
