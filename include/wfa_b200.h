@@ -114,7 +114,11 @@ WFA_API wfa_aligner_t* wfa_aligner_create(wfa_metric_t metric, const wfa_penalti
                                   int device, int* err);
 WFA_API void wfa_aligner_destroy(wfa_aligner_t* h);
 
-/* Builder setters, src/aligner.rs:462-613.  Return WFA_OK or an error. */
+/* Builder setters, src/aligner.rs:462-613.  Return WFA_OK or an error.
+ * Med/low memory with an alignment gives the reference's med/low CIGARs (its
+ * piggyback backtrace); the device keeps every component's history for it,
+ * so wfa_set_max_memory_compact (the reference's backtrace-buffer compaction
+ * limit) is accepted and has no effect on results or on device memory. */
 WFA_API int wfa_set_memory_mode(wfa_aligner_t* h, wfa_memory_t mode);               /* :462 */
 WFA_API int wfa_set_max_memory_compact(wfa_aligner_t* h, uint64_t bytes);           /* :469 */
 WFA_API int wfa_set_max_alignment_steps(wfa_aligner_t* h, int32_t max_steps);       /* :533 */
