@@ -151,14 +151,15 @@ struct ChunkInfo {
   int32_t max_len_sum = 0;
   int64_t slots = 0;
 };
-static void scan_chunks(const wfa_batch_t* b, int64_t n, int64_t chunk, bool packed, bool aln,
-                        std::vector<ChunkInfo>& out) {
+static void scan_chunks(const wfa_batch_t* b, int64_t n, const std::vector<int64_t>& bnd, bool packed,
+                        bool aln, std::vector<ChunkInfo>& out) {
   const int64_t nchunks = (int64_t)out.size();
   const int64_t unit = packed ? 4 : 1;  // bytes per offset unit
   // One pass over [i0, i1), accumulated per chunk into `acc`.
   auto pass = [&](int64_t i0, int64_t i1, std::vector<ChunkInfo>& acc) {
-    for (int64_t i = i0; i < i1;) {
-      const int64_t ci = i / chunk, e = std::min(i1, (ci + 1) * chunk);
+    int64_t ci = std::upper_bound(bnd.begin(), bnd.end(), i0) - bnd.begin() - 1;
+    for (int64_t i = i0; i < i1; ++ci) {
+      const int64_t e = std::min(i1, bnd[(size_t)ci + 1]);
       ChunkInfo& c = acc[(size_t)ci];
       int64_t lo = c.lo, hi = c.hi, slots = c.slots;
       int32_t mx = c.max_len_sum;
@@ -1206,14 +1207,28 @@ int wfa_batch_align(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* result
   cudaSetDevice(h->device);
   if (b->span == WFA_SPAN_BIWFA) return batch_align_simple(h, b, results, cigars);
   cudaStream_t sc = h->stream, si = h->s_in, so = h->s_out;
+  // Chunks of `chunk` pairs, the first and last a quarter of that: a short
+  // first chunk starts the device sooner, a short last one leaves less to
+  // copy out after the last alignment.
   const int64_t chunk = std::max<int64_t>(65536, std::min<int64_t>(262144, (n + 7) / 8));
-  const int64_t nchunks = (n + chunk - 1) / chunk;
+  std::vector<int64_t> bnd{0};
+  {
+    const int64_t edge = std::max<int64_t>(chunk / 4, 1);
+    int64_t at = std::min(n, edge);
+    bnd.push_back(at);
+    while (n - at > edge) {
+      at += std::min(chunk, n - at - edge);
+      bnd.push_back(at);
+    }
+    if (at < n) bnd.push_back(n);
+  }
+  const int64_t nchunks = (int64_t)bnd.size() - 1;
   const bool packed = b->format == WFA_SEQ_PACKED2;
 
   // Per chunk: sequence byte range, longest pair, CIGAR slot bytes -- one
   // pass over the host arrays, split across host threads.
   std::vector<ChunkInfo> ci_info((size_t)nchunks);
-  scan_chunks(b, n, chunk, packed, aln, ci_info);
+  scan_chunks(b, n, bnd, packed, aln, ci_info);
   std::vector<int64_t> c_slot0((size_t)nchunks + 1, 0);
   for (int64_t ci = 0; ci < nchunks; ++ci)
     c_slot0[(size_t)ci + 1] = c_slot0[(size_t)ci] + ci_info[(size_t)ci].slots;
@@ -1268,7 +1283,7 @@ int wfa_batch_align(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* result
   // around the alignment kernel); results, chunk info and CIGAR bytes out
   // (s_out) while the next chunk aligns.
   for (int64_t ci = 0; ci < nchunks; ++ci) {
-    const int64_t a = ci * chunk, e = std::min(n, a + chunk), cn = e - a;
+    const int64_t a = bnd[(size_t)ci], e = bnd[(size_t)ci + 1], cn = e - a;
     const ChunkInfo& I = ci_info[(size_t)ci];
     if (I.hi > I.lo)
       PIPE_TRY(cudaMemcpyAsync(dseq + I.lo, (const uint8_t*)b->seq + I.lo, (size_t)(I.hi - I.lo),
@@ -1323,7 +1338,7 @@ int wfa_batch_align(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* result
   std::vector<int64_t> retry;
   int64_t dense_total = 0;
   for (int64_t ci = 0; ci < nchunks; ++ci) {
-    const int64_t a = ci * chunk, e = std::min(n, a + chunk);
+    const int64_t a = bnd[(size_t)ci], e = bnd[(size_t)ci + 1];
     PIPE_TRY(cudaEventSynchronize(ev_res[(size_t)ci]), "results");
     const int32_t nretry = (int32_t)(hinfo[4 * ci + 2] & 0xffffffff);
     if (nretry > 0)
