@@ -368,6 +368,57 @@ def test_device_api_matches_host_api(pkg):
         assert a_ops.tobytes() == b_ops.tobytes(), i
 
 
+def test_host_batch_across_chunks(pkg):
+    """A host-buffer batch large enough to run in several chunks (short first
+    and last ones), with empty patterns and one long pair, matches the
+    device-buffer call pair by pair, and its packed CIGARs tile the output."""
+    import torch
+    from wfa_b200 import synth
+    base = synth.uniform_pairs(200000, 100, 150, 0.0, 0.04, 91)
+    r = random.Random(3)
+    lp = bytes(r.choice(b"ACGT") for _ in range(3000))
+    lt = bytearray(lp)
+    for _ in range(250):
+        lt[r.randrange(len(lt))] = r.choice(b"ACGT")
+    buf = np.concatenate([base.buf, np.frombuffer(lp + bytes(lt), np.uint8)])
+    p_off, p_len = base.p_off.copy(), base.p_len.copy()
+    t_off, t_len = base.t_off.copy(), base.t_len.copy()
+    p_len[::997] = 0
+    p_off[100000], p_len[100000] = len(base.buf), len(lp)
+    t_off[100000], t_len[100000] = len(base.buf) + len(lp), len(lt)
+    ps = synth.PairSet(buf, p_off, p_len, t_off, t_len)
+    words, pwo, two = synth.pack2bits(ps)
+    words = np.concatenate([words, np.zeros(4, np.uint32)])
+    a = pkg.WavefrontAligner(3, [0, 4, 6, 2])
+    a.set_alignment_scope(True)
+    res_h, cig_h = a.align_batch(words, pwo, ps.p_len, two, ps.t_len, packed=True)
+    dev = torch.device("cuda:0")
+    w = torch.from_numpy(words.view(np.int32)).to(dev)
+    caps = 2 * (ps.p_len.astype(np.int64) + ps.t_len) + 1
+    coff = np.concatenate([[0], np.cumsum(caps)[:-1]]).astype(np.int64)
+    args = [torch.from_numpy(x).to(dev) for x in (pwo, ps.p_len, two, ps.t_len, coff)]
+    cig = torch.zeros(int(caps.sum()) + 16, dtype=torch.uint8, device=dev)
+    res = torch.zeros(len(ps) * 10, dtype=torch.int32, device=dev)
+    a.align_batch_device(w.data_ptr(), w.numel() * 4, args[0].data_ptr(), args[1].data_ptr(),
+                         args[2].data_ptr(), args[3].data_ptr(), len(ps), res.data_ptr(), cig.data_ptr(),
+                         args[4].data_ptr(), int(caps.sum()), packed=True)
+    torch.cuda.synchronize()
+    rd = res.cpu().numpy().view(res_h.dtype)
+    cd = cig.cpu().numpy()
+    for f in ("score", "status", "cigar_length", "cigar_score", "end_v", "end_h"):
+        assert np.array_equal(rd[f], res_h[f]), f
+    assert res_h["cigar_length"][100000] >= 3000
+    # The packed CIGARs tile the output without gaps or overlaps.
+    beg = res_h["cigar_begin"].astype(np.int64)
+    order = np.argsort(beg, kind="stable")
+    ends = beg[order] + res_h["cigar_length"][order]
+    assert beg[order][0] == 0 and np.array_equal(beg[order][1:], ends[:-1])
+    for i in list(range(0, len(ps), 1013)) + [100000, len(ps) - 1]:
+        a_ops = cd[coff[i] + rd["cigar_begin"][i]: coff[i] + rd["cigar_begin"][i] + rd["cigar_length"][i]]
+        b_ops = cig_h[res_h["cigar_begin"][i]: res_h["cigar_begin"][i] + res_h["cigar_length"][i]]
+        assert a_ops.tobytes() == b_ops.tobytes(), i
+
+
 def test_async_batches_match_the_blocking_call(pkg):
     """wfa_batch_submit / poll / wait: three batches queued at once give the
     results of wfa_batch_align, in order."""
