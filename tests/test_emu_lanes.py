@@ -33,3 +33,29 @@ def test_32_lanes(metric, pen, span, free, hk, hp):
     for i, (p, t) in enumerate(pairs):
         s, st, ops, ep, _ = oracle_run(metric, pen, p, t, True, span, free, hk, list(hp))
         assert (int(res["score"][i]), int(res["status"][i]), cig[i]) == (s, st, ops), i
+
+
+# Med/low (the piggyback backtrace) and Compat::Corrected ends-free with a
+# match reward (candidate, diagonal pruning, begin-free dominance pruning).
+CASES_MODES = [
+    (3, [0, 4, 6, 2], 0, None, "med", 0),
+    (4, [0, 4, 6, 2, 24, 1], 1, [5, 5, 5, 5], "low", 0),
+    (2, [-1, 3, 2], 1, [3, 12, 3, 12], "high", 1),
+    (3, [-3, 5, 3, 2], 1, [2, 40, 2, 40], "med", 1),
+    (4, [-1, 4, 6, 2, 24, 1], 1, [260, 260, 260, 260], "high", 1),
+]
+
+
+@pytest.mark.parametrize("metric,pen,span,free,memory,compat", CASES_MODES)
+def test_32_lanes_memory_modes_and_corrected(metric, pen, span, free, memory, compat):
+    pairs = lcg_pairs(131 + metric, 3, 200)
+    fr = None
+    if free:
+        fr = [min(free[0], min(len(p) for p, _ in pairs)), min(free[1], min(len(p) for p, _ in pairs)),
+              min(free[2], min(len(t) for _, t in pairs)), min(free[3], min(len(t) for _, t in pairs))]
+    res, cig = emu_lib.run(metric, pen, pairs, span=span, free=fr, lanes=32,
+                           piggyback=memory != "high", compat=compat)
+    for i, (p, t) in enumerate(pairs):
+        s, st, ops, ep, _ = oracle_run(metric, pen, p, t, True, span, fr, 0, [0, 0, 0],
+                                       memory=memory, compat=compat)
+        assert (int(res["score"][i]), int(res["status"][i]), cig[i]) == (s, st, ops), i
