@@ -196,6 +196,35 @@ def cpu_baseline(ps, threads, max_pairs=None, metric=3, pen=PEN, mode=0, heur=(0
     return n / secs, n, secs
 
 
+# Shared-memory bytes per computed cell of each metric's compute step
+# (reads + writes of 4-byte offsets): edit 4, indel 3, linear 4, affine 8,
+# affine 2-piece 14; indexed by the oracle's metric number.
+CELL_RW = {0: 3, 1: 4, 2: 4, 3: 8, 4: 14}
+
+
+def oracle_check(ps, n_check, metric, pen, omode, heur, threads, checks):
+    """Scores, statuses and CIGARs (FNV-1a hashes) of the first n_check pairs
+    against the oracle, outside every timed region.  checks: name ->
+    (result records, CIGAR byte buffer, begin offset of each pair's CIGAR in
+    it).  Returns ({name: mismatching pairs}, the oracle's work sums over
+    those pairs: cells computed, bases compared, CIGAR ops)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    sub = ps.subset(np.arange(n_check))
+    hp = tuple(heur[1]) + (0, 0, 0)
+    work = np.zeros(3, np.int64)
+    _, sc, st, hs = O.batch(metric, pen, ps.buf.tobytes(), sub.p_off, sub.p_len, sub.t_off,
+                            sub.t_len, compute_alignment=True, mode=omode, heuristic=heur[0],
+                            hparams=hp[:3], threads=threads, want_results=True, work=work)
+    out = {}
+    for name, (rec, ops, begin) in checks.items():
+        r = rec[:n_check]
+        gh = O.hash_ops(ops, begin[:n_check], r["cigar_length"], threads)
+        bad = (r["score"] != sc) | (r["status"] != st) | (gh != hs)
+        out[name] = int(bad.sum())
+    return out, work
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -287,6 +316,7 @@ def run_gpu(args):
             kern_ms.append(a.last_kernel_ms())
     torch.cuda.synchronize()
     launches = a.kernel_launches() - launches0
+    reruns = a.last_rerun_pairs()
     total_ms = sum(step_ms)
     if world > 1:
         t = torch.tensor([total_ms], device=dev)
@@ -375,6 +405,7 @@ def run_gpu(args):
                          "peak_kind": peak_kind,
                          "kernel_ms": kms, "algorithmic_bytes_per_launch": alg_bytes},
             "gpu_launches": int(launches),
+            "rerun_pairs_per_step": int(reruns),
             "clocks": clk.summary()}
     # The alignment kernel is bound by instruction issue: warp instructions
     # per pair (ncu) x pairs/s against 4 schedulers x SMs x the sampled clock.
@@ -387,6 +418,40 @@ def run_gpu(args):
         line["roofline_issue"] = {"bound": "issue", "achieved": issue, "peak": issue_peak,
                                   "unit": "warp-inst/s", "frac": issue / issue_peak,
                                   "warp_inst_per_pair": ipp}
+    if rank == 0 and not args.no_parity:
+        # Every checked pair against the oracle: the last timed device step's
+        # slots and the last host-buffer call's packed CIGARs.
+        threads = os.cpu_count() or 1
+        n_check = min(n, args.parity_pairs)
+        dev_cig = cig.cpu().numpy()
+        checks = {"device": (rd, dev_cig, coff + rd["cigar_begin"]),
+                  "e2e": (hr, hc, hr["cigar_begin"].astype(np.int64))}
+        bad, work = oracle_check(ps, n_check, metric, pen, omode, heur, threads, checks)
+        line["parity"] = {"pairs_checked": n_check, "mismatches": bad["device"],
+                          "e2e_mismatches": bad["e2e"], "oracle": "port (C++ restatement)",
+                          "fields": "score, status, CIGAR bytes (FNV-1a 64 per pair)"}
+        # Shared-memory roofline (on-chip wavefront traffic): per pair
+        # C x 4 B x (R + W) + 2 ceil(X / 4) + 4 L from the oracle's work
+        # counters, scaled to the whole launch; peak = SMs x 128 B/clk x
+        # the sampled SM clock.
+        scale = n / n_check
+        cells, bases, ops = (float(x) * scale for x in work)
+        smem_bytes = cells * 4 * CELL_RW[metric] + 2 * np.ceil(bases / 4) + 4 * ops
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        mhz = line["clocks"].get("sm_mhz") or 1965.0
+        smem_peak = sms * 128 * mhz * 1e6 / 1e9
+        smem_ach = smem_bytes / (kms / 1000.0) / 1e9
+        line["roofline_smem"] = {"bound": "smem", "achieved": smem_ach, "peak": smem_peak,
+                                 "unit": "GB/s", "frac": smem_ach / smem_peak,
+                                 "bytes_per_pair": smem_bytes / n,
+                                 "peak_kind": f"{sms} SMs x 128 B/clk x sampled {mhz:.0f} MHz",
+                                 "work_per_pair": {"cells": cells / n, "bases": bases / n,
+                                                   "cigar_ops": ops / n}}
+        bound_hbm = hbm_peak * 1e9 / (alg_bytes / n)
+        bound_smem = smem_peak * 1e9 / (smem_bytes / n)
+        lim = "hbm" if bound_hbm < bound_smem else "smem"
+        line["roofline_memory"] = {"limit": lim, "pairs_per_s_bound": min(bound_hbm, bound_smem),
+                                   "frac": value / world / min(bound_hbm, bound_smem)}
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
         rate, m, secs = cpu_baseline(ps, threads, max_pairs=args.cpu_sample, metric=metric, pen=pen,
@@ -499,6 +564,9 @@ def main():
     ap.add_argument("--plain-pairs", type=int, default=None)
     ap.add_argument("--cpu-sample", type=int, default=None)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--parity-pairs", type=int, default=None,
+                    help="pairs checked against the oracle after the timed region")
+    ap.add_argument("--no-parity", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer and plain forms")
     args = ap.parse_args()
     if args.workload == "serve":
@@ -521,6 +589,7 @@ def main():
     args.pairs = pairs if args.pairs is None else args.pairs
     args.plain_pairs = plain if args.plain_pairs is None else args.plain_pairs
     args.cpu_sample = cpu if args.cpu_sample is None else args.cpu_sample
+    args.parity_pairs = cpu if args.parity_pairs is None else args.parity_pairs
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -248,8 +248,9 @@ WFA_API int wfa_batch_wait(wfa_aligner_t* h, int64_t ticket);
  * on each device where it has been used, until the process exits; it calls
  * no allocation routine.
  *
- * - The first call on a device looks up the array's device address; make
- *   that first call before any stream capture.
+ * - The first call on a device looks up the array's device address (again
+ *   after the device's context was re-created, e.g. by cudaDeviceReset);
+ *   make that first call before any stream capture.
  * - Limits: the longest pair of the batch must have p_len + t_len <=
  *   WFA_NOALLOC_MAX_LEN_SUM, else WFA_ERR_ARGUMENT; an alignment that needs
  *   more scratch than a quarter of the array fails with WFA_ERR_OOM (use
@@ -340,6 +341,11 @@ WFA_API int wfa_server_stop(wfa_server_t* s);
 
 /* Number of the library's own kernel launches issued so far by this handle. */
 WFA_API int64_t wfa_kernel_launches(const wfa_aligner_t* h);
+
+/* Pairs the handle's last batch call re-ran with larger scratch (a pair
+ * re-run twice counts twice); 0 when every pair finished in the first
+ * launch.  No counterpart in the reference (it has no device scratch). */
+WFA_API int64_t wfa_last_rerun_pairs(const wfa_aligner_t* h);
 
 /* Device time (ms, CUDA events on the launching stream) of the alignment
  * kernel launches of the handle's last call, retries included. */

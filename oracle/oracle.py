@@ -54,8 +54,10 @@ def lib(fast=False):
                                i32, ctypes.c_char_p, i32, ctypes.c_char_p, i32]
     L.wfo_cli_line.restype = i32
     L.wfo_batch.argtypes = [ctypes.c_int, P32, ctypes.c_int, ctypes.c_int, ctypes.c_int, P32, P32,
-                            ctypes.c_char_p, P64, P32, P64, P32, i64, ctypes.c_int, P32, P32, P64]
+                            ctypes.c_char_p, P64, P32, P64, P32, i64, ctypes.c_int, P32, P32, P64,
+                            P64]
     L.wfo_batch.restype = ctypes.c_double
+    L.wfo_hash_ops.argtypes = [vp, P64, P32, i64, ctypes.c_int, P64]
     _lib[name] = L
     return L
 
@@ -206,8 +208,10 @@ def run_cli_case(case, fast=False):
 
 
 def batch(metric, penalties, seqbuf, p_off, p_len, t_off, t_len, compute_alignment=True, mode=0,
-          heuristic=0, hparams=(0, 0, 0), free=None, threads=1, want_results=True):
-    """Multi-threaded batch over the fast build; returns (seconds, scores, status, cigar_hash)."""
+          heuristic=0, hparams=(0, 0, 0), free=None, threads=1, want_results=True, work=None):
+    """Multi-threaded batch over the fast build; returns (seconds, scores, status, cigar_hash).
+    work: an int64 array of 3 that receives the batch's summed work counters
+    (cells computed, bases compared, CIGAR ops)."""
     import numpy as np
     L = lib(fast=True)
     n = len(p_len)
@@ -227,5 +231,21 @@ def batch(metric, penalties, seqbuf, p_off, p_len, t_off, t_len, compute_alignme
                        t_off.ctypes.data_as(P64), t_len.ctypes.data_as(P32), n, threads,
                        scores.ctypes.data_as(P32) if want_results else None,
                        status.ctypes.data_as(P32) if want_results else None,
-                       hashes.ctypes.data_as(P64) if want_results else None)
+                       hashes.ctypes.data_as(P64) if want_results else None,
+                       work.ctypes.data_as(P64) if work is not None else None)
     return secs, scores, status, hashes
+
+
+def hash_ops(ops, begin, length, threads=1):
+    """FNV-1a hashes of ops[begin[i]:begin[i]+length[i]] (uint8 array), the
+    hash `batch` reports per CIGAR."""
+    import numpy as np
+    ops = np.ascontiguousarray(ops, dtype=np.uint8)
+    begin = np.ascontiguousarray(begin, dtype=np.int64)
+    length = np.ascontiguousarray(length, dtype=np.int32)
+    out = np.zeros(len(begin), np.int64)
+    L = lib(fast=True)
+    L.wfo_hash_ops(ctypes.c_void_p(ops.ctypes.data), begin.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                   length.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), len(begin), threads,
+                   out.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
+    return out

@@ -2390,12 +2390,14 @@ int32_t wfo_cli_line(void* h, int span, const int32_t* free4, int biwfa, int sco
 double wfo_batch(int metric, const int32_t* pen, int compute_alignment, int mode, int hkind,
                  const int32_t* hp, const int32_t* free4, const char* seqs, const int64_t* p_off,
                  const int32_t* p_len, const int64_t* t_off, const int32_t* t_len, int64_t count,
-                 int threads, int32_t* scores, int32_t* status, int64_t* cigar_hash) {
+                 int threads, int32_t* scores, int32_t* status, int64_t* cigar_hash,
+                 int64_t* work3) {
   if (threads < 1) threads = 1;
   std::vector<std::thread> pool;
   std::atomic<int> ready{0};
   std::atomic<bool> go{false};
   std::vector<double> secs((size_t)threads, 0.0);
+  std::vector<int64_t> work((size_t)threads * 3, 0);
   for (int tid = 0; tid < threads; ++tid) {
     pool.emplace_back([&, tid]() {
       Aligner* a = static_cast<Aligner*>(wfo_create(metric, pen));
@@ -2418,6 +2420,11 @@ double wfo_batch(int metric, const int32_t* pen, int compute_alignment, int mode
         else s = a->align_biwfa(P, p_len[i], T, t_len[i]);
         if (scores) scores[i] = s;
         if (status) status[i] = a->status;
+        if (work3) {
+          work[(size_t)tid * 3] += a->ctr.cells;
+          work[(size_t)tid * 3 + 1] += a->ctr.bases;
+          work[(size_t)tid * 3 + 2] += a->ctr.ops;
+        }
         if (cigar_hash) {
           uint64_t hsh = 1469598103934665603ull;
           const Cigar& c = a->cigar;
@@ -2436,7 +2443,29 @@ double wfo_batch(int metric, const int32_t* pen, int compute_alignment, int mode
   for (auto& th : pool) th.join();
   double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - w0).count();
   (void)secs;
+  if (work3) {
+    work3[0] = work3[1] = work3[2] = 0;
+    for (int tid = 0; tid < threads; ++tid)
+      for (int j = 0; j < 3; ++j) work3[j] += work[(size_t)tid * 3 + j];
+  }
   return wall;
+}
+
+void wfo_hash_ops(const uint8_t* ops, const int64_t* begin, const int32_t* len, int64_t count,
+                  int threads, int64_t* out) {
+  if (threads < 1) threads = 1;
+  std::vector<std::thread> pool;
+  for (int tid = 0; tid < threads; ++tid) {
+    pool.emplace_back([=]() {
+      for (int64_t i = tid; i < count; i += threads) {
+        uint64_t hsh = 1469598103934665603ull;
+        const uint8_t* c = ops + begin[i];
+        for (int32_t j = 0; j < len[i]; ++j) hsh = (hsh ^ c[j]) * 1099511628211ull;
+        out[i] = (int64_t)hsh;
+      }
+    });
+  }
+  for (auto& th : pool) th.join();
 }
 
 }  // extern "C"

@@ -72,12 +72,20 @@ int32_t wfo_cli_line(void* h, int span, const int32_t* free4, int biwfa, int sco
 /* Multi-threaded batch (CPU baseline): pairs i in [0,count) at
  * seq + p_off[i] (length p_len[i]) and seq + t_off[i] (t_len[i]); mode 0
  * end2end, 1 endsfree, 2 biwfa.  Returns wall seconds of the align calls
- * (max over threads).  scores/status may be NULL. */
+ * (max over threads).  scores/status/cigar_hash may be NULL; work3, if
+ * not NULL, receives the sums over the batch of the wfo_counters figures
+ * (cells computed, bases compared, CIGAR ops). */
 double wfo_batch(int metric, const int32_t* pen, int compute_alignment, int mode,
                  int heuristic_kind, const int32_t* hparams, const int32_t* free4,
                  const char* seq, const int64_t* p_off, const int32_t* p_len,
                  const int64_t* t_off, const int32_t* t_len, int64_t count, int threads,
-                 int32_t* scores, int32_t* status, int64_t* cigar_hash);
+                 int32_t* scores, int32_t* status, int64_t* cigar_hash, int64_t* work3);
+
+/* FNV-1a 64-bit hash of ops[begin[i] .. begin[i] + len[i]) for every i (the
+ * same hash wfo_batch reports per CIGAR), so a CIGAR buffer produced
+ * elsewhere compares against the oracle's without copying CIGARs around. */
+void wfo_hash_ops(const uint8_t* ops, const int64_t* begin, const int32_t* len, int64_t count,
+                  int threads, int64_t* out);
 
 #ifdef __cplusplus
 }

@@ -6,16 +6,19 @@ literals of tests/cli_output.rs, the C-driver outputs under tests/data/, and
 the Z-drop expectation of tests/corrected_zdrop.rs.  Every sequence and every
 expected line below is read from those files; nothing is typed in by hand.
 
-Run from the repository root:  python tests/golden/make_golden.py [REF_ROOT]
-(REF_ROOT defaults to the read-only reference checkout).  The committed JSON is
-what the tests read; the reference tree is not needed at test time.
+Run from the repository root:  python tests/golden/make_golden.py REF_ROOT
+where REF_ROOT is a checkout of the reference crate (or set WFA_REFERENCE_ROOT).
+The committed JSON is what the tests read; the reference tree is not needed
+at test time.
 """
 import json
 import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("WFA_REFERENCE_ROOT")
+if not REF:
+    sys.exit("usage: make_golden.py REF_ROOT (or set WFA_REFERENCE_ROOT)")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_cases.json")
 
 

@@ -86,3 +86,41 @@ def test_biwfa_plain_and_golden_cli(pkg, golden):
             lines.append(cli_format.line(metric, orig, case["score_only"], True, rec,
                                          "" if case["score_only"] else c.operations.decode(), len(pb), len(tb)))
         assert lines == case["expected"], case["name"]
+
+
+def _batch_vs_oracle(pkg, metric, pen, ps):
+    """A packed host-buffer BiWFA batch against the oracle's align_biwfa on
+    every pair: score, status and CIGAR (hashes of the op bytes)."""
+    import os
+    from wfa_b200 import synth
+    a = pkg.WavefrontAligner(metric, pen)
+    a.set_alignment_scope(True)
+    words, pwo, two = synth.pack2bits(ps)
+    res, cig = a.align_batch(np.concatenate([words, np.zeros(4, np.uint32)]), pwo, ps.p_len, two,
+                             ps.t_len, packed=True, span=2)
+    a.close()
+    threads = os.cpu_count() or 1
+    _, sc, st, hs = O.batch(metric, pen, ps.buf.tobytes(), ps.p_off, ps.p_len, ps.t_off, ps.t_len,
+                            mode=2, threads=threads)
+    gh = O.hash_ops(cig, res["cigar_begin"].astype(np.int64), res["cigar_length"], threads)
+    assert np.array_equal(res["score"], sc)
+    assert np.array_equal(res["status"], st)
+    assert np.array_equal(gh, hs)
+
+
+def test_biwfa_longread_sizes(pkg):
+    """Pairs of the uneven long-read batch at its long end: 16 pairs of
+    8.5-20 kbp at 5-15 % edits (60 % indels), gap-affine 2-piece -- deep
+    breakpoint recursions and the recovery threshold."""
+    from wfa_b200 import synth
+    pool = synth.config3(400, synth.SEED_BASE + 3)
+    ps = pool.subset(np.where(pool.p_len >= 8000)[0][:16])
+    assert len(ps) == 16 and ps.p_len.max() > 15000
+    _batch_vs_oracle(pkg, 4, [0, 4, 6, 2, 24, 1], ps)
+
+
+def test_biwfa_serving_long_lane(pkg):
+    """Two 50 kbp pairs at 10 % edits, gap-affine: the serving mix's BiWFA lane."""
+    from wfa_b200 import synth
+    ps = synth.pairs_with_lengths([50000, 50000], [0.1, 0.1], 77)
+    _batch_vs_oracle(pkg, 3, [0, 4, 6, 2], ps)

@@ -11,10 +11,15 @@ integers: the comparison is exact.
 
 This file is named to be collected last, after every other test.
 """
+import os
+import sys
+
 import numpy as np
 import pytest
 
 from _pkg import load
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 pytestmark = pytest.mark.gpu
 
@@ -45,12 +50,19 @@ def _device_batch(ps, packed):
             "co": t(coff), "coff": coff, "cap": int(caps.sum()), "n": len(ps), "packed": packed}
 
 
-def _run(a, d, noalloc, span=0):
-    """One call of either entry point into fresh (poisoned) output buffers."""
+def _outputs(d):
     import torch
     dev = torch.device("cuda:0")
     res = torch.full((d["n"] * 10,), -7, dtype=torch.int32, device=dev)
     cig = torch.full((d["cap"] + 16,), 0xAB, dtype=torch.uint8, device=dev)
+    return res, cig
+
+
+def _run(a, d, noalloc, span=0, out=None):
+    """One call of either entry point into fresh (poisoned) output buffers,
+    or into `out` (results, CIGAR slots) when given."""
+    import torch
+    res, cig = out if out is not None else _outputs(d)
     fn = a.align_batch_device_noalloc if noalloc else a.align_batch_device
     fn(d["seq"].data_ptr(), d["seq"].numel(), d["po"].data_ptr(), d["pl"].data_ptr(),
        d["to"].data_ptr(), d["tl"].data_ptr(), d["n"], res.data_ptr(), cig.data_ptr(),
@@ -87,6 +99,50 @@ def test_two_calls_in_a_row_match_the_device_batch(pkg):
     a.close()
 
 
+def test_matches_the_oracle(pkg):
+    """Scores, statuses and CIGARs of a no-allocation call equal the oracle's
+    (the CPU restatement of the reference) pair for pair."""
+    from wfa_b200 import synth
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    ps = synth.uniform_pairs(5_000, 100, 400, 0.0, 0.08, 906)
+    d = _device_batch(ps, packed=True)
+    a = pkg.WavefrontAligner(pkg.GAP_AFFINE, [0, 4, 6, 2])
+    a.set_alignment_scope(True)
+    res, cig = _run(a, d, noalloc=True)
+    a.close()
+    r = res.view(pkg.RESULT_DTYPE)
+    _, sc, st, hs = O.batch(3, [0, 4, 6, 2], ps.buf.tobytes(), ps.p_off, ps.p_len, ps.t_off,
+                            ps.t_len, threads=os.cpu_count() or 1)
+    gh = O.hash_ops(cig, d["coff"] + r["cigar_begin"], r["cigar_length"])
+    assert np.array_equal(r["score"], sc)
+    assert np.array_equal(r["status"], st)
+    assert np.array_equal(gh, hs)
+
+
+def test_allocates_no_device_memory(pkg):
+    """Free device memory is the same before and after a call that re-runs
+    pairs with larger slices (the path that would grow an ordinary scratch).
+    The handle, the inputs and the outputs are made first; one call before
+    the measured one loads the module that holds the array."""
+    import torch
+    from wfa_b200 import synth
+    ps = synth.uniform_pairs(4_000, 300, 1500, 0.08, 0.12, 907)
+    d = _device_batch(ps, packed=True)
+    a = pkg.WavefrontAligner(pkg.GAP_AFFINE, [0, 4, 6, 2])
+    a.set_alignment_scope(True)
+    out = _outputs(d)
+    _run(a, d, noalloc=True, out=out)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    _run(a, d, noalloc=True, out=out)
+    torch.cuda.synchronize()
+    free1 = torch.cuda.mem_get_info()[0]
+    assert a.last_rerun_pairs() > 0  # the measured call did re-run pairs
+    assert free1 == free0
+    a.close()
+
+
 def test_more_reruns_than_one_round_holds(pkg):
     """More pairs to re-run than one round gathers (65,536): the rest are
     gathered in later rounds.  Score-only and ends-free calls as well."""
@@ -96,6 +152,9 @@ def test_more_reruns_than_one_round_holds(pkg):
     a = pkg.WavefrontAligner(pkg.GAP_AFFINE, [0, 4, 6, 2])
     a.set_alignment_scope(True)
     _same(a, d)
+    # The call just made (the no-allocation one) re-ran more pairs than one
+    # gathering round holds, so the later rounds were exercised.
+    assert a.last_rerun_pairs() > 65_536
     a.set_alignment_scope(False)
     _same(a, d, compute=False)
     e = pkg.WavefrontAligner(pkg.EDIT, None)

@@ -112,6 +112,7 @@ def lib():
         "wfa_server_pending": (i64, [vp]),
         "wfa_server_stop": (ctypes.c_int, [vp]),
         "wfa_kernel_launches": (i64, [vp]),
+        "wfa_last_rerun_pairs": (i64, [vp]),
         "wfa_last_kernel_ms": (ctypes.c_double, [vp]),
         "wfa_cigar_rle": (i32, [vp, i32, ctypes.c_char_p, i32]),
         "wfa_version": (ctypes.c_char_p, []),
@@ -263,6 +264,10 @@ class WavefrontAligner:
 
     def last_kernel_ms(self):
         return self._L.wfa_last_kernel_ms(self._h)
+
+    def last_rerun_pairs(self):
+        """Pairs the last batch call re-ran with larger scratch."""
+        return self._L.wfa_last_rerun_pairs(self._h)
 
     # --- batches ---
     def align_batch(self, seq, p_off, p_len, t_off, t_len, packed=False, span=SPAN_END2END,

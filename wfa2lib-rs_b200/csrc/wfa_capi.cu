@@ -107,6 +107,7 @@ struct wfa_aligner {
   int occ_val = 1;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_kernel_ms = 0.0;
+  int64_t last_reruns = 0;  // pair re-runs (larger scratch) of the last call
   // Events of the pipelined host-buffer batch, created once and reused:
   // creating and destroying events waits for work running on the device
   // (other handles' kernels included).
@@ -531,6 +532,7 @@ static int run_device_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t
     CUDA_TRY(h, cudaStreamSynchronize(st), "collect retries");
     list = out;
     todo = got;
+    h->last_reruns += got;
     next_round(r, P, max_len_sum);
   }
   return WFA_OK;
@@ -634,6 +636,7 @@ static int run_biwfa_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t*
     CUDA_TRY(h, cudaStreamSynchronize(st), "collect retries");
     list = out;
     todo = got;
+    h->last_reruns += got;
     cfg.wmax = std::min(wfull, cfg.wmax * 2);
     wbase = std::min(cfg.wmax, wbase * 2);
     cfg.hist_scores *= 4;
@@ -730,6 +733,7 @@ static int run_noalloc_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_
     P.num_pairs = todo;
     CUDA_TRY(h, cudaMemsetAsync(base, 0, 16, st), "memset");
     CUDA_TRY(h, cudaEventRecord(h->ev0, st), "event");
+    CUDA_TRY(h, cudaGetLastError(), "an earlier CUDA call of this thread");
     CUDA_TRY(h, launch_unialign(P, cls, (int)blocks, L.total, st), "kernel launch");
     CUDA_TRY(h, cudaEventRecord(h->ev1, st), "event");
     h->launches++;
@@ -757,6 +761,7 @@ static int run_noalloc_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_
     CUDA_TRY(h, cudaStreamSynchronize(st), "collect retries");
     if (got == 0) break;
     todo = std::min(got, kNaListCap);
+    if (retries > 0) h->last_reruns += retries;
     pending = got - todo;
     lst = list;
   }
@@ -1063,6 +1068,7 @@ int wfa_alignment_end_pos(const wfa_aligner_t* h, int32_t* s, int32_t* k, int32_
 int wfa_last_error(const wfa_aligner_t* h) { return h ? h->last_err : WFA_ERR_ARGUMENT; }
 const char* wfa_last_error_string(const wfa_aligner_t* h) { return h ? h->err_str.c_str() : "null handle"; }
 int64_t wfa_kernel_launches(const wfa_aligner_t* h) { return h ? h->launches : 0; }
+int64_t wfa_last_rerun_pairs(const wfa_aligner_t* h) { return h ? h->last_reruns : 0; }
 double wfa_last_kernel_ms(const wfa_aligner_t* h) { return h ? h->last_kernel_ms : 0.0; }
 
 static int batch_common(wfa_aligner_t* h, const wfa_batch_t* b) {
@@ -1072,6 +1078,7 @@ static int batch_common(wfa_aligner_t* h, const wfa_batch_t* b) {
   if (b->span != WFA_SPAN_END2END && b->span != WFA_SPAN_ENDSFREE && b->span != WFA_SPAN_BIWFA)
     return WFA_ERR_ARGUMENT;
   h->last_err = WFA_OK;
+  h->last_reruns = 0;
   int saved = h->span;
   h->span = b->span;
   int r = check_supported(h, b->span == WFA_SPAN_BIWFA);
@@ -1360,6 +1367,7 @@ int wfa_batch_align(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* result
   // Pairs that outgrew the first configuration: re-run with the batch driver.
   if (!retry.empty()) {
     const int64_t rn = (int64_t)retry.size();
+    h->last_reruns += rn;
     std::vector<int64_t> po(rn), to(rn), co(rn);
     std::vector<int32_t> pl(rn), tl(rn);
     int32_t mx = 0;
