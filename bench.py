@@ -272,6 +272,8 @@ def run_gpu(args):
     n = len(ps)
     a = pkg.WavefrontAligner(metric, pen, device=local)
     a.set_alignment_scope(True)
+    if args.lanes:
+        a.set_lanes_per_pair(args.lanes)
     if span == 1:
         a.set_alignment_extension()
     if heur[0]:
@@ -317,6 +319,9 @@ def run_gpu(args):
     torch.cuda.synchronize()
     launches = a.kernel_launches() - launches0
     reruns = a.last_rerun_pairs()
+    lanes = a.last_lanes_per_pair()
+    from wfa_b200.aligner import autotune_report
+    tuned = [ln for ln in autotune_report().splitlines() if ln]
     total_ms = sum(step_ms)
     if world > 1:
         t = torch.tensor([total_ms], device=dev)
@@ -341,7 +346,8 @@ def run_gpu(args):
     if args.no_e2e:
         line = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
                 "ms_per_step": total_ms / args.steps, "kernel_ms": kms, "gpu_launches": int(launches),
-                "roofline_achieved_gbs": achieved}
+                "roofline_achieved_gbs": achieved, "lanes_per_pair": lanes,
+                "rerun_pairs_per_step": int(reruns), "autotune": tuned}
         if rank == 0:
             print(json.dumps(line), flush=True)
         a.close()
@@ -406,6 +412,7 @@ def run_gpu(args):
                          "kernel_ms": kms, "algorithmic_bytes_per_launch": alg_bytes},
             "gpu_launches": int(launches),
             "rerun_pairs_per_step": int(reruns),
+            "lanes_per_pair": lanes, "autotune": tuned,
             "clocks": clk.summary()}
     # The alignment kernel is bound by instruction issue: warp instructions
     # per pair (ncu) x pairs/s against 4 schedulers x SMs x the sampled clock.
@@ -567,6 +574,8 @@ def main():
     ap.add_argument("--parity-pairs", type=int, default=None,
                     help="pairs checked against the oracle after the timed region")
     ap.add_argument("--no-parity", action="store_true")
+    ap.add_argument("--lanes", type=int, default=0,
+                    help="lanes per pair (8, 16, 32); 0: autotuned")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer and plain forms")
     args = ap.parse_args()
     if args.workload == "serve":

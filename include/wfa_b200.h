@@ -347,6 +347,23 @@ WFA_API int64_t wfa_kernel_launches(const wfa_aligner_t* h);
  * launch.  No counterpart in the reference (it has no device scratch). */
 WFA_API int64_t wfa_last_rerun_pairs(const wfa_aligner_t* h);
 
+/* Lanes per pair of the unidirectional kernel for end-to-end alignments
+ * without a heuristic: 8, 16 or 32 (a lane group of that width aligns one
+ * pair; 32 / lanes pairs share a warp), or 0 (the default) for the
+ * autotuned choice.  The first device batch of each kind (device, metric,
+ * encoding, score-only or CIGAR, length bucket n + m <= 384 / 1024 / 2048)
+ * in a process times the candidates on a sample of its pairs and keeps the
+ * fastest; ends-free, heuristic and med/low alignments and pairs above
+ * n + m = 2048 always take whole warps.  Results never depend on it.  No
+ * counterpart in the reference (it aligns one pair per call on the CPU). */
+WFA_API int wfa_set_lanes_per_pair(wfa_aligner_t* h, int32_t lanes);
+/* Lanes per pair the handle's last batch ran with (first round). */
+WFA_API int32_t wfa_last_lanes_per_pair(const wfa_aligner_t* h);
+/* The autotuner's choices so far, one line per kind with the candidates'
+ * sample times, into out (NUL-terminated, at most cap bytes); returns the
+ * full length. */
+WFA_API int32_t wfa_autotune_report(char* out, int32_t cap);
+
 /* Device time (ms, CUDA events on the launching stream) of the alignment
  * kernel launches of the handle's last call, retries included. */
 WFA_API double wfa_last_kernel_ms(const wfa_aligner_t* h);

@@ -1,6 +1,7 @@
 // wfa_emu.cpp -- TEST-ONLY host builds of the device aligner (wfa_align.cuh).
 // Default build: a one-lane warp.  With -DWFA_EMU_THREADS: 32 host threads
-// per warp, __syncwarp and the reductions as barriers.  The CPU tests compare
+// per warp (WFA_EMU_LANES=8: an 8-lane group), __syncwarp and the reductions
+// as barriers.  The CPU tests compare
 // them with the oracle so the kernel's logic is checked before it runs on a
 // GPU.  Not part of the product.
 #define WFA_EMU 1
@@ -45,28 +46,32 @@ static bool run_lane(const AlignParams& P, const Workspace& ws, int64_t i) {
   return run_lane_g<CLS, true>(P, ws, i);
 }
 
+// The kernel's compact ring: P.ring_slots slots of P.wmax cells (narrow, as
+// the shared-memory slots are), rows wider than that in the spill ring of
+// P.wspill cells per slot -- both paths run in every emulated alignment.
 template <int CLS>
 static bool run_pair(const AlignParams& P, int64_t i) {
   constexpr int NC = CLS == kAffine2pClass ? 5 : CLS == kAffineClass ? 3 : 1;
   std::vector<WfD> ring((size_t)P.scope * NC);
-  std::vector<int32_t> ringv((size_t)P.scope * NC * P.wmax, 0x5A5A5A5A);
+  std::vector<int32_t> ringv((size_t)P.ring_slots * P.wmax, 0x5A5A5A5A);
+  std::vector<int32_t> ringg((size_t)P.ring_slots * P.wspill, 0x5A5A5A5A);
   std::vector<int4> hist((size_t)P.hist_scores, int4{0, -1, 0, 0});
   std::vector<int32_t> harena((size_t)P.hist_words, 0x5A5A5A5A);
   std::vector<int32_t> dom((size_t)P.dom_words, 0x5A5A5A5A);
   Workspace ws{ring.data(), ringv.data(), hist.data(), harena.data(),
-               P.dom_words ? dom.data() : nullptr};
+               P.dom_words ? dom.data() : nullptr, ringg.data()};
 #ifdef WFA_EMU_THREADS
   EmuWarp warp;
   g_emu_warp = &warp;
-  bool retry[32];
+  bool retry[WFA_WARP];
   std::vector<std::thread> lanes;
-  for (int l = 0; l < 32; ++l)
+  for (int l = 0; l < WFA_WARP; ++l)
     lanes.emplace_back([&, l]() {
       g_emu_lane = l;
       retry[l] = run_lane<CLS>(P, ws, i);
     });
   for (auto& t : lanes) t.join();
-  for (int l = 1; l < 32; ++l)
+  for (int l = 1; l < WFA_WARP; ++l)
     if (retry[l] != retry[0]) std::abort();  // lanes disagreed: not warp-uniform
   return retry[0];
 #else
@@ -103,9 +108,11 @@ extern "C" int64_t wfa_emu_batch(int metric, const int32_t* pen6, int compute_al
   P.cigars = cigars;
   P.results = results;
   P.num_pairs = num_pairs;
-  P.wmax = wmax;
+  P.wmax = wmax < 12 ? wmax : 12;
+  P.wspill = wmax;
   P.hist_scores = hist_scores;
   P.hist_words = hist_words;
+  P.ring_slots = compact_ring_slots(P, metric_class(metric));
   int32_t max_len_sum = 0;
   for (int64_t i = 0; i < num_pairs; ++i) max_len_sum = std::max(max_len_sum, p_len[i] + t_len[i]);
   const int nc = metric == WFA_METRIC_GAP_AFFINE_2P ? 5 : metric == WFA_METRIC_GAP_AFFINE ? 3 : 1;
@@ -179,15 +186,15 @@ static bool bi_pair(const AlignParams& P, int64_t i) {
 #ifdef WFA_EMU_THREADS
   EmuWarp warp;
   g_emu_warp = &warp;
-  bool retry[32];
+  bool retry[WFA_WARP];
   std::vector<std::thread> lanes;
-  for (int l = 0; l < 32; ++l)
+  for (int l = 0; l < WFA_WARP; ++l)
     lanes.emplace_back([&, l]() {
       g_emu_lane = l;
       retry[l] = go();
     });
   for (auto& t : lanes) t.join();
-  for (int l = 1; l < 32; ++l)
+  for (int l = 1; l < WFA_WARP; ++l)
     if (retry[l] != retry[0]) std::abort();
   return retry[0];
 #else

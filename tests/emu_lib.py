@@ -15,7 +15,7 @@ LANES = int(os.environ.get("WFA_EMU_LANES", "1"))
 def lib(lanes=None):
     lanes = LANES if lanes is None else lanes
     if lanes not in _L:
-        name = "libwfa_emu32.so" if lanes == 32 else "libwfa_emu.so"
+        name = {32: "libwfa_emu32.so", 8: "libwfa_emu8.so"}.get(lanes, "libwfa_emu.so")
         path = os.path.join(HERE, "emu", "_build", name)
         if os.system(f"make -s -C {os.path.join(HERE, 'emu')}") != 0 or not os.path.exists(path):
             raise RuntimeError("cannot build the emulation library")

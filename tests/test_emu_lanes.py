@@ -1,4 +1,5 @@
-"""The device aligner with a full 32-lane warp emulated by host threads.
+"""The device aligner with a full 32-lane warp, or an 8-lane group (the
+short-pair kernel's), emulated by host threads.
 
 Lane partitioning of the diagonals, the warp reductions behind trims,
 termination and heuristics, and warp-uniform control flow (a lane that
@@ -25,11 +26,12 @@ CASES = [
 ]
 
 
+@pytest.mark.parametrize("lanes", [32, 8])
 @pytest.mark.parametrize("metric,pen,span,free,hk,hp", CASES)
-def test_32_lanes(metric, pen, span, free, hk, hp):
+def test_lane_groups(metric, pen, span, free, hk, hp, lanes):
     pairs = lcg_pairs(101 + metric + hk, 3, 260)
     res, cig = emu_lib.run(metric, pen, pairs, span=span, free=free, heuristic=hk, hparams=hp,
-                           lanes=32, packed=metric == 3)
+                           lanes=lanes, packed=metric == 3)
     for i, (p, t) in enumerate(pairs):
         s, st, ops, ep, _ = oracle_run(metric, pen, p, t, True, span, free, hk, list(hp))
         assert (int(res["score"][i]), int(res["status"][i]), cig[i]) == (s, st, ops), i

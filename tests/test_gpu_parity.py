@@ -324,14 +324,40 @@ def test_config2_sample_packed(pkg):
                                            ps.t_off, ps.t_len, threads=8)
     assert np.array_equal(res["score"], scores)
     assert np.array_equal(res["status"], status)
-    idx = np.random.default_rng(0).choice(len(ps), 5000, replace=False)
-    for i in idx:
-        r = res[i]
-        ops = cig[r["cigar_begin"]:r["cigar_begin"] + r["cigar_length"]].tobytes()
-        h = 1469598103934665603
-        for c in ops:
-            h = ((h ^ c) * 1099511628211) & (2**64 - 1)
-        assert (h - 2**64 if h >= 2**63 else h) == hashes[i], i
+    got = O.hash_ops(cig, res["cigar_begin"].astype(np.int64), res["cigar_length"], 8)
+    assert np.array_equal(got, hashes)
+
+
+@pytest.mark.parametrize("lanes", [8, 16, 32])
+@pytest.mark.parametrize("metric,pen", PENS)
+def test_lane_group_widths(pkg, metric, pen, lanes):
+    """Every lane-group width of the end-to-end kernel, every metric, both
+    encodings, score-only and CIGAR: 100-400 bp pairs at 0-15 % edits (some
+    wavefronts wider than the shared-memory ring slots, which spill), every
+    pair against the oracle."""
+    from wfa_b200 import synth
+    ps = synth.uniform_pairs(3000, 100, 400, 0.0, 0.15, 0x5EED0000 + 300 + metric)
+    words, pwo, two = synth.pack2bits(ps)
+    words = np.concatenate([words, np.zeros(4, np.uint32)])
+    for compute in (True, False):
+        _, scores, status, hashes = O.batch(metric, pen, ps.buf.tobytes(), ps.p_off, ps.p_len,
+                                            ps.t_off, ps.t_len, compute_alignment=compute, threads=8)
+        for packed in (True, False):
+            a = pkg.WavefrontAligner(metric, pen)
+            a.set_alignment_scope(compute)
+            a.set_lanes_per_pair(lanes)
+            if packed:
+                res, cig = a.align_batch(words, pwo, ps.p_len, two, ps.t_len, packed=True)
+            else:
+                res, cig = a.align_batch(ps.buf, ps.p_off, ps.p_len, ps.t_off, ps.t_len)
+            # (a scope too large for narrow groups' rings runs wider groups)
+            assert a.last_lanes_per_pair() == lanes or (lanes < 32 and metric == 4 and pen[0] < 0)
+            a.close()
+            assert np.array_equal(res["score"], scores), (compute, packed)
+            assert np.array_equal(res["status"], status), (compute, packed)
+            if compute:
+                got = O.hash_ops(cig, res["cigar_begin"].astype(np.int64), res["cigar_length"], 8)
+                assert np.array_equal(got, hashes), packed
 
 
 def test_device_api_matches_host_api(pkg):

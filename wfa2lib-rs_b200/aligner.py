@@ -113,6 +113,9 @@ def lib():
         "wfa_server_stop": (ctypes.c_int, [vp]),
         "wfa_kernel_launches": (i64, [vp]),
         "wfa_last_rerun_pairs": (i64, [vp]),
+        "wfa_set_lanes_per_pair": (ctypes.c_int, [vp, i32]),
+        "wfa_last_lanes_per_pair": (i32, [vp]),
+        "wfa_autotune_report": (i32, [ctypes.c_char_p, i32]),
         "wfa_last_kernel_ms": (ctypes.c_double, [vp]),
         "wfa_cigar_rle": (i32, [vp, i32, ctypes.c_char_p, i32]),
         "wfa_version": (ctypes.c_char_p, []),
@@ -269,6 +272,14 @@ class WavefrontAligner:
         """Pairs the last batch call re-ran with larger scratch."""
         return self._L.wfa_last_rerun_pairs(self._h)
 
+    def set_lanes_per_pair(self, lanes):
+        """8, 16 or 32 lanes per pair for end-to-end alignments without a
+        heuristic, or 0 for the autotuned choice (the default)."""
+        return self._check(self._L.wfa_set_lanes_per_pair(self._h, lanes))
+
+    def last_lanes_per_pair(self):
+        return self._L.wfa_last_lanes_per_pair(self._h)
+
     # --- batches ---
     def align_batch(self, seq, p_off, p_len, t_off, t_len, packed=False, span=SPAN_END2END,
                     out_results=None, out_cigars=None):
@@ -424,4 +435,13 @@ def cigar_rle(ops):
     n = L.wfa_cigar_rle(ops, len(ops), None, 0)
     buf = ctypes.create_string_buffer(n + 1)
     L.wfa_cigar_rle(ops, len(ops), buf, n + 1)
+    return buf.value.decode()
+
+
+def autotune_report():
+    """The lane-width autotuner's choices in this process, one line per kind."""
+    L = lib()
+    n = L.wfa_autotune_report(None, 0)
+    buf = ctypes.create_string_buffer(n + 1)
+    L.wfa_autotune_report(buf, n + 1)
     return buf.value.decode()

@@ -43,7 +43,11 @@ struct int4 { int x, y, z, w; };
 #define WFA_DN inline
 #ifdef WFA_EMU_THREADS
 #include <barrier>
-#define WFA_WARP 32
+// Lanes of the emulated warp (32; 8 emulates an 8-lane group of the kernel).
+#ifndef WFA_EMU_LANES
+#define WFA_EMU_LANES 32
+#endif
+#define WFA_WARP WFA_EMU_LANES
 #else
 #define WFA_WARP 1
 #endif
@@ -55,12 +59,13 @@ namespace wfab {
 // Warp primitives (one-lane stand-ins in the emulation build)
 // ---------------------------------------------------------------------------
 #if defined(WFA_EMU_THREADS)
-// Test-only: 32 host threads play the lanes of one warp; __syncwarp and the
-// warp reductions become barriers, so lane partitioning, reductions and
-// warp-uniform control flow are exercised exactly as on the GPU.
+// Test-only: WFA_WARP host threads play the lanes of one warp (or lane
+// group); __syncwarp and the warp reductions become barriers, so lane
+// partitioning, reductions and warp-uniform control flow are exercised
+// exactly as on the GPU.
 struct EmuWarp {
-  std::barrier<> bar{32};
-  int red[32];
+  std::barrier<> bar{WFA_WARP};
+  int red[WFA_WARP];
 };
 extern thread_local int g_emu_lane;
 extern EmuWarp* g_emu_warp;
@@ -75,7 +80,7 @@ struct Warp {
     w->red[g_emu_lane] = v;
     w->bar.arrive_and_wait();
     int r = w->red[0];
-    for (int i = 1; i < 32; ++i) r = mx ? (w->red[i] > r ? w->red[i] : r) : (w->red[i] < r ? w->red[i] : r);
+    for (int i = 1; i < WFA_WARP; ++i) r = mx ? (w->red[i] > r ? w->red[i] : r) : (w->red[i] < r ? w->red[i] : r);
     w->bar.arrive_and_wait();
     return r;
   }
@@ -113,6 +118,31 @@ struct Warp {
   }
 #endif
 };
+
+// A group of LW lanes that aligns one pair: LW = 32 is the whole warp; 8 or
+// 16 put 4 or 2 pairs in a warp (short pairs, whose wavefronts are a few
+// diagonals wide).  The groups of a warp run the same code on different
+// pairs; every collective names only the group's own lanes.  In the
+// emulation builds the emulated warp is the group.
+#if defined(WFA_CUDA_WARP)
+template <int LW>
+struct Lanes {
+  static_assert(LW == 8 || LW == 16 || LW == 32, "lane group width");
+  static WFA_D unsigned mask() {
+    return LW == 32 ? 0xffffffffu : ((1u << LW) - 1u) << ((threadIdx.x & 31) & ~(LW - 1));
+  }
+  static WFA_D int lane() { return threadIdx.x & (LW - 1); }
+  static WFA_D int min(int v) { return __reduce_min_sync(mask(), v); }
+  static WFA_D int max(int v) { return __reduce_max_sync(mask(), v); }
+  static WFA_D unsigned any(bool p) { return __ballot_sync(mask(), p) & mask(); }
+  static WFA_D void sync() { __syncwarp(mask()); }
+};
+#else
+template <int LW>
+struct Lanes : Warp {
+  static_assert(LW == WFA_WARP, "the emulated warp is the lane group");
+};
+#endif
 
 WFA_D int imin(int a, int b) { return a < b ? a : b; }
 WFA_D int imax(int a, int b) { return a > b ? a : b; }
@@ -242,6 +272,7 @@ struct Workspace {
   int4* hist;       // [hist_scores] M history records {a, b, cell offset of a, present}
   int32_t* harena;  // M history cells
   int32_t* dom;     // Corrected-mode dominance array (NC x diagonals), or null
+  int32_t* ringg;   // compact ring: rows wider than the ring's slots (device memory), or null
 };
 
 // GEN = false compiles the common configuration only (end-to-end, no
@@ -250,8 +281,9 @@ struct Workspace {
 // compute and of the BiWFA extend: their loads are all issued before any
 // result is stored, so a lane keeps UNR cells' loads in flight (wide
 // wavefronts of long pairs, whose cells live in device memory).
-template <int CLS, class S, bool GEN = true, int UNR = 1>
+template <int CLS, class S, bool GEN = true, int UNR = 1, int LW = WFA_WARP>
 struct PairAligner {
+  using G = Lanes<LW>;
   static constexpr int NC = CLS == kAffine2pClass ? 5 : CLS == kAffineClass ? 3 : 1;
   static constexpr bool AFF = CLS >= kAffineClass;
   static constexpr bool TWO = CLS == kAffine2pClass;
@@ -262,6 +294,20 @@ struct PairAligner {
   int32_t n, m;
   int32_t lane;
   int32_t scope, wmax;
+  // Compact cell ring (the unidirectional aligner; BiWFA's overlap scans read
+  // every slot of the scope, so its rings keep one slot per score): a
+  // component's cells are only read within a fixed number of scores after
+  // they are written (M at s + x, s + o + e; a gap component at s + e), and
+  // only scores that are multiples of gstep hold wavefronts, so each
+  // component gets a round-robin ring of depth (its longest read offset /
+  // gstep) + 1, a new slot per wavefront it stores.  Rows wider than wmax go
+  // to the same slot of a second ring of width P.wspill in device memory.
+  // The launch provides P.ring_slots slots per lane group (0: this layout is
+  // off).  I and D of a piece are always stored together, so they share one
+  // slot counter (advanced by D's allocation).
+  bool compact = false;
+  int16_t dm = 0, d1 = 0, d2 = 0;  // depths: M, I1/D1, I2/D2
+  int16_t nm = 0, n1 = 0, n2 = 0;  // next slots: M, piece 1, piece 2
   bool modular;  // score-only: no M history
   int32_t cap;   // num_wavefronts score cap (high memory)
   int32_t p0, pf, t0, tf;
@@ -336,13 +382,40 @@ struct PairAligner {
   }
   WFA_D void put(int c, int s, const WfD& d) {
     put_ns(c, s, d);
-    Warp::sync();
+    G::sync();
   }
-  // Storage for an output of component c at score s covering [L, H].
+  // Storage for an output of component c at score s covering [L, H]
+  // (s is always the current score).
   WFA_D int32_t* alloc(int c, int s, int L, int H) {
     int64_t w = (int64_t)H - L + 1;
-    if (w > wmax) { retry = true; return nullptr; }
-    return ws.ringv + ((int64_t)(sidx(s) * NC + c)) * wmax;
+    int64_t idx;
+    if (compact) {
+      if (c == CM) {
+        idx = nm;
+        nm = nm + 1 == dm ? 0 : nm + 1;
+      } else if (c == CI1 || c == CD1) {
+        idx = dm + (c == CD1 ? d1 : 0) + n1;
+        if (c == CD1) n1 = n1 + 1 == d1 ? 0 : n1 + 1;
+      } else {
+        idx = dm + 2 * d1 + (c == CD2 ? d2 : 0) + n2;
+        if (c == CD2) n2 = n2 + 1 == d2 ? 0 : n2 + 1;
+      }
+    } else {
+      idx = (int64_t)sidx(s) * NC + c;
+    }
+    if (w <= wmax) return ws.ringv + idx * wmax;
+    if (compact && ws.ringg && w <= P.wspill) return ws.ringg + idx * P.wspill;
+    retry = true;
+    return nullptr;
+  }
+  // Depths of the compact ring for score step gstep (the longest read offset
+  // of M is scope - 1; of a gap component its extension penalty).
+  WFA_D void compact_depths() {
+    dm = (int16_t)((scope - 1) / gstep + 1);
+    d1 = (int16_t)(AFF ? P.e1 / gstep + 1 : 0);
+    d2 = (int16_t)(TWO ? P.e2 / gstep + 1 : 0);
+    nm = n1 = n2 = 0;
+    if (dm + 2 * d1 + 2 * d2 > P.ring_slots) retry = true;
   }
   // High memory: once M at score s is final (after its extend step), copy its
   // initialised range to the history arena for the backtrace.
@@ -356,7 +429,7 @@ struct PairAligner {
       if (wf_present(d)) {
         int64_t w = d.b >= d.a ? (int64_t)d.b - d.a + 1 : 0;
         if (hused + w > P.hist_words) { retry = true; return; }
-        for (int64_t i = lane; i < w; i += WFA_WARP) ws.harena[hused + i] = d.vals[i];
+        for (int64_t i = lane; i < w; i += LW) ws.harena[hused + i] = d.vals[i];
         r.z = (int32_t)hused;
         r.w = GEN && c == CM ? 1 | (seed_flags << 1) : 1;
         hused += w;
@@ -421,41 +494,41 @@ struct PairAligner {
   // Trim pass over stored cells [lo, hi] (used after endsfree_init).
   WFA_D WfD trim_pass(int32_t* base, int L, int lo, int hi) {
     int vmin = INT_MAX, vmax = INT_MIN;
-    Warp::sync();
-    for (int k = lo + lane; k <= hi; k += WFA_WARP) {
+    G::sync();
+    for (int k = lo + lane; k <= hi; k += LW) {
       if (cell_in_bounds(base[k - L], k, n, m)) { vmin = imin(vmin, k); vmax = imax(vmax, k); }
     }
-    vmin = Warp::min(vmin);
-    vmax = Warp::max(vmax);
+    vmin = G::min(vmin);
+    vmax = G::max(vmax);
     return finish(base, L, lo, hi, vmin, vmax);
   }
 
   // endsfree_init, src/aligner.rs:3426-3452, on M stored at base (cell L)
   // and computed over [lo, hi]; returns the new limits through lo/hi.
   WFA_D void endsfree_init(int32_t* base, int L, int& lo, int& hi, int k) {
-    Warp::sync();
+    G::sync();
     if (t0 >= k) {
       if (hi >= k) {
-        if (base[k - L] <= k) { Warp::sync(); if (lane == 0) base[k - L] = k; seed_flags |= 1; }
+        if (base[k - L] <= k) { G::sync(); if (lane == 0) base[k - L] = k; seed_flags |= 1; }
       } else {
-        for (int kk = hi + 1 + lane; kk < k; kk += WFA_WARP) base[kk - L] = kOffsetNull;
+        for (int kk = hi + 1 + lane; kk < k; kk += LW) base[kk - L] = kOffsetNull;
         if (lane == 0) base[k - L] = k;
         seed_flags |= 1;
         hi = k;
       }
     }
-    Warp::sync();
+    G::sync();
     if (p0 >= k) {
       if (lo <= -k) {
-        if (base[-k - L] <= 0) { Warp::sync(); if (lane == 0) base[-k - L] = 0; seed_flags |= 2; }
+        if (base[-k - L] <= 0) { G::sync(); if (lane == 0) base[-k - L] = 0; seed_flags |= 2; }
       } else {
         if (lane == 0) base[-k - L] = 0;
         seed_flags |= 2;
-        for (int kk = -k + 1 + lane; kk < lo; kk += WFA_WARP) base[kk - L] = kOffsetNull;
+        for (int kk = -k + 1 + lane; kk < lo; kk += LW) base[kk - L] = kOffsetNull;
         lo = -k;
       }
     }
-    Warp::sync();
+    G::sync();
   }
 
   // endsfree_null_m, src/aligner.rs:3470-3494
@@ -468,14 +541,14 @@ struct PairAligner {
     else { lo = 0; hi = 0; }
     int32_t* v = alloc(CM, s, lo, hi);
     if (retry) return wf_none();
-    for (int kk = lo + lane; kk <= hi; kk += WFA_WARP) v[kk - lo] = kOffsetNull;
-    Warp::sync();
+    for (int kk = lo + lane; kk <= hi; kk += LW) v[kk - lo] = kOffsetNull;
+    G::sync();
     if (lane == 0) {
       if (text) v[k - lo] = k;
       if (pattern) v[-k - lo] = 0;
     }
     seed_flags |= (text ? 1 : 0) | (pattern ? 2 : 0);
-    Warp::sync();
+    G::sync();
     WfD d;
     d.vals = v; d.lo = lo; d.hi = hi; d.a = lo; d.b = hi; d.flags = kPresent; d.adub = kAdUnknown;
     return d;
@@ -483,11 +556,11 @@ struct PairAligner {
 
   WFA_D void set_none(int s, int from_c, int to_c) {
     for (int c = from_c; c < to_c; ++c) put_ns(c, s, wf_none());
-    Warp::sync();
+    G::sync();
   }
   WFA_D void set_m(int s, const WfD& d) {
     put_ns(CM, s, d);
-    Warp::sync();
+    G::sync();
   }
 
   // ---- init_alignment, src/aligner.rs:846-1000 ------------------------------
@@ -511,8 +584,12 @@ struct PairAligner {
     cidx = 0;
     gstep = score_step_gcd();
     gphase = 0;
-    for (int i = lane; i < scope * NC; i += WFA_WARP) ws.ring[i] = wf_none();
-    Warp::sync();
+    if (compact) {
+      compact_depths();
+      if (retry) return;
+    }
+    for (int i = lane; i < scope * NC; i += LW) ws.ring[i] = wf_none();
+    G::sync();
     hist_lo = -(n + scope + 2);
     hist_hi = m + scope + 2;
     num_null_steps = 0;
@@ -533,19 +610,19 @@ struct PairAligner {
     if (dom_on) {
       dom_len = hist_hi - hist_lo + 1;
       if (!ws.dom || (int64_t)NC * dom_len > P.dom_words) { retry = true; return; }
-      for (int64_t i = lane; i < (int64_t)NC * dom_len; i += WFA_WARP) ws.dom[i] = -1;
-      Warp::sync();
+      for (int64_t i = lane; i < (int64_t)NC * dom_len; i += LW) ws.dom[i] = -1;
+      G::sync();
     }
     int lo0 = 0, hi0 = 0;
     bool seeds = ef() && P.match == 0;
     if (seeds) { lo0 = -p0; hi0 = t0; }
     int32_t* v = alloc(CM, 0, lo0, hi0);
     if (retry) return;
-    for (int k = lo0 + lane; k <= hi0; k += WFA_WARP) {
+    for (int k = lo0 + lane; k <= hi0; k += LW) {
       int32_t val = k == 0 ? 0 : (k > 0 ? k : 0);  // seeds: (h,0) on k=h, (0,v) on k=-v
       v[k - lo0] = val;
     }
-    Warp::sync();
+    G::sync();
     WfD d;
     d.vals = v; d.lo = lo0; d.hi = hi0; d.a = lo0; d.b = hi0; d.flags = kPresent; d.adub = kAdUnknown;
     set_m(0, d);
@@ -569,12 +646,12 @@ struct PairAligner {
         if (hr.w && ks[i] >= hr.x && ks[i] <= hr.y) ws.harena[hr.z + ks[i] - hr.x] = kOffsetNull;
       }
     }
-    Warp::sync();
+    G::sync();
     int32_t* out = alloc(CM, s, lo, hi);
     if (retry) return;
     bool indel = P.metric == WFA_METRIC_INDEL;
     int vmin = INT_MAX, vmax = INT_MIN;
-    for (int k = lo + lane; k <= hi; k += WFA_WARP) {
+    for (int k = lo + lane; k <= hi; k += LW) {
       int32_t ins = rd(prev, k - 1), del = rd(prev, k + 1), mx;
       if (indel) mx = imax(del, ins + 1);
       else mx = imax(del, imax(ins, rd(prev, k)) + 1);
@@ -582,8 +659,8 @@ struct PairAligner {
       out[k - lo] = mx;
       if (mx != kOffsetNull) { vmin = imin(vmin, k); vmax = imax(vmax, k); }
     }
-    vmin = Warp::min(vmin);
-    vmax = Warp::max(vmax);
+    vmin = G::min(vmin);
+    vmax = G::max(vmax);
     set_m(s, finish(out, lo, lo, hi, vmin, vmax));
   }
 
@@ -611,7 +688,7 @@ struct PairAligner {
     int32_t* out = alloc(CM, s, L, H);
     if (retry) return;
     int vmin = INT_MAX, vmax = INT_MIN;
-    for (int k = lo + lane; k <= hi; k += WFA_WARP) {
+    for (int k = lo + lane; k <= hi; k += LW) {
       int32_t a = rd(mi, k) + 1, ins = rd(gp, k - 1) + 1, del = rd(gp, k + 1);
       int32_t mx = imax(del, imax(ins, a));
       if (!cell_in_bounds(mx, k, n, m)) mx = kOffsetNull;
@@ -622,8 +699,8 @@ struct PairAligner {
       endsfree_init(out, L, lo, hi, bk);
       set_m(s, trim_pass(out, L, lo, hi));
     } else {
-      vmin = Warp::min(vmin);
-      vmax = Warp::max(vmax);
+      vmin = G::min(vmin);
+      vmax = G::max(vmax);
       set_m(s, finish(out, L, lo, hi, vmin, vmax));
     }
   }
@@ -697,13 +774,13 @@ struct PairAligner {
     int mn_m = INT_MAX, mx_m = INT_MIN, mn_i1 = INT_MAX, mx_i1 = INT_MIN, mn_d1 = INT_MAX, mx_d1 = INT_MIN;
     int mn_i2 = INT_MAX, mx_i2 = INT_MIN, mn_d2 = INT_MAX, mx_d2 = INT_MIN;
     const bool two = TWO && !affine_kernel;
-    for (int k0 = lo + lane; k0 <= hi; k0 += WFA_WARP * UNR) {
+    for (int k0 = lo + lane; k0 <= hi; k0 += LW * UNR) {
       // Inputs of UNR diagonals first (reads stay inside each input's
       // initialised range, also for k > hi), then the results.
       int32_t vi1[UNR], vd1[UNR], vm[UNR], vi2[UNR], vd2[UNR];
 #pragma unroll
       for (int u = 0; u < UNR; ++u) {
-        const int k = k0 + u * WFA_WARP;
+        const int k = k0 + u * LW;
         vi1[u] = imax(rd(mo1, k - 1), rd(i1e, k - 1)) + 1;
         vd1[u] = imax(rd(mo1, k + 1), rd(d1e, k + 1));
         vm[u] = rd(mm, k) + 1;
@@ -714,7 +791,7 @@ struct PairAligner {
       }
 #pragma unroll
       for (int u = 0; u < UNR; ++u) {
-        const int k = k0 + u * WFA_WARP;
+        const int k = k0 + u * LW;
         if (k > hi) break;
         const int32_t i1 = vi1[u], d1 = vd1[u];
         int32_t mx;
@@ -737,8 +814,8 @@ struct PairAligner {
         if (cell_in_bounds(d1, k, n, m)) { mn_d1 = imin(mn_d1, k); mx_d1 = imax(mx_d1, k); }
       }
     }
-    mn_i1 = Warp::min(mn_i1); mx_i1 = Warp::max(mx_i1);
-    mn_d1 = Warp::min(mn_d1); mx_d1 = Warp::max(mx_d1);
+    mn_i1 = G::min(mn_i1); mx_i1 = G::max(mx_i1);
+    mn_d1 = G::min(mn_d1); mx_d1 = G::max(mx_d1);
     put_ns(CI1, s, finish(oi1, lo, lo, hi, mn_i1, mx_i1));
     put_ns(CD1, s, finish(od1, lo, lo, hi, mn_d1, mx_d1));
     if (TWO) {
@@ -746,8 +823,8 @@ struct PairAligner {
         put_ns(CI2, s, wf_none());
         put_ns(CD2, s, wf_none());
       } else {
-        mn_i2 = Warp::min(mn_i2); mx_i2 = Warp::max(mx_i2);
-        mn_d2 = Warp::min(mn_d2); mx_d2 = Warp::max(mx_d2);
+        mn_i2 = G::min(mn_i2); mx_i2 = G::max(mx_i2);
+        mn_d2 = G::min(mn_d2); mx_d2 = G::max(mx_d2);
         put_ns(CI2, s, finish(oi2, lo, lo, hi, mn_i2, mx_i2));
         put_ns(CD2, s, finish(od2, lo, lo, hi, mn_d2, mx_d2));
       }
@@ -757,7 +834,7 @@ struct PairAligner {
       endsfree_init(om, L, mlo, mhi, bk);
       set_m(s, trim_pass(om, L, mlo, mhi));
     } else {
-      mn_m = Warp::min(mn_m); mx_m = Warp::max(mx_m);
+      mn_m = G::min(mn_m); mx_m = G::max(mx_m);
       set_m(s, finish(om, L, lo, hi, mn_m, mx_m));
     }
   }
@@ -772,11 +849,11 @@ struct PairAligner {
   WFA_D void wide_pass(int kb, int ke, int lo, const WfD& mm, const WfD& mo1, const WfD& i1e,
                        const WfD& d1e, const WfD& mo2, const WfD& i2e, const WfD& d2e, bool two,
                        int32_t* om, int32_t* oi1, int32_t* od1, int32_t* oi2, int32_t* od2) {
-    for (int k0 = kb + lane; k0 <= ke; k0 += WFA_WARP * U) {
+    for (int k0 = kb + lane; k0 <= ke; k0 += LW * U) {
       int32_t vi1[U], vd1[U], vm[U], vi2[U], vd2[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        const int k = imin(k0 + u * WFA_WARP, ke);  // lanes past ke repeat ke's reads
+        const int k = imin(k0 + u * LW, ke);  // lanes past ke repeat ke's reads
         if (CHK) {
           vi1[u] = imax(rd(mo1, k - 1), rd(i1e, k - 1)) + 1;
           vd1[u] = imax(rd(mo1, k + 1), rd(d1e, k + 1));
@@ -797,7 +874,7 @@ struct PairAligner {
       }
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        const int k = k0 + u * WFA_WARP;
+        const int k = k0 + u * LW;
         if (k > ke) break;
         int32_t mx = imax(vm[u], imax(vi1[u], vd1[u]));
         if (two) mx = imax(mx, imax(vi2[u], vd2[u]));
@@ -815,19 +892,19 @@ struct PairAligner {
   // Highest / lowest k of row[lo..hi] (row[0] is cell lo) holding an
   // in-bounds offset; INT_MIN / INT_MAX if none.
   WFA_D int row_last(const int32_t* row, int lo, int hi) const {
-    for (int top = hi; top >= lo; top -= WFA_WARP) {
+    for (int top = hi; top >= lo; top -= LW) {
       const int k = top - lane;
       const bool ok = k >= lo && cell_in_bounds(row[k - lo], k, n, m);
-      const int best = Warp::max(ok ? k : INT_MIN);
+      const int best = G::max(ok ? k : INT_MIN);
       if (best != INT_MIN) return best;
     }
     return INT_MIN;
   }
   WFA_D int row_first(const int32_t* row, int lo, int hi) const {
-    for (int bot = lo; bot <= hi; bot += WFA_WARP) {
+    for (int bot = lo; bot <= hi; bot += LW) {
       const int k = bot + lane;
       const bool ok = k <= hi && cell_in_bounds(row[k - lo], k, n, m);
-      const int best = Warp::min(ok ? k : INT_MAX);
+      const int best = G::min(ok ? k : INT_MAX);
       if (best != INT_MAX) return best;
     }
     return INT_MAX;
@@ -854,9 +931,9 @@ struct PairAligner {
     }
     if (ilo <= ihi)
       wide_pass<false, UNR>(ilo, ihi, lo, mm, mo1, i1e, d1e, mo2, i2e, d2e, two, om, oi1, od1, oi2, od2);
-    Warp::sync();  // the scans read cells other lanes stored
+    G::sync();  // the scans read cells other lanes stored
     // Trims of the rows I1, D1 (, I2, D2) and M: the top and then the bottom
-    // WFA_WARP cells of every row are checked together; a row whose end
+    // LW cells of every row are checked together; a row whose end
     // chunk holds no in-bounds cell continues with a scan.
     constexpr int RN = TWO ? 5 : 3;
     int32_t* rows[RN];
@@ -871,24 +948,24 @@ struct PairAligner {
 #pragma unroll
       for (int r = 0; r < RN; ++r) v[r] = (k >= lo && (two || r < 2 || r == RN - 1)) ? rows[r][k - lo] : kOffsetNull;
 #pragma unroll
-      for (int r = 0; r < RN; ++r) last[r] = Warp::max(cell_in_bounds(v[r], k, n, m) ? k : INT_MIN);
+      for (int r = 0; r < RN; ++r) last[r] = G::max(cell_in_bounds(v[r], k, n, m) ? k : INT_MIN);
     }
 #pragma unroll
     for (int r = 0; r < RN; ++r)
-      if (last[r] == INT_MIN && (two || r < 2 || r == RN - 1) && hi - WFA_WARP >= lo)
-        last[r] = row_last(rows[r], lo, hi - WFA_WARP);
+      if (last[r] == INT_MIN && (two || r < 2 || r == RN - 1) && hi - LW >= lo)
+        last[r] = row_last(rows[r], lo, hi - LW);
     {
       const int k = lo + lane;
       int32_t v[RN];
 #pragma unroll
       for (int r = 0; r < RN; ++r) v[r] = (k <= last[r]) ? rows[r][k - lo] : kOffsetNull;
 #pragma unroll
-      for (int r = 0; r < RN; ++r) first[r] = Warp::min(cell_in_bounds(v[r], k, n, m) ? k : INT_MAX);
+      for (int r = 0; r < RN; ++r) first[r] = G::min(cell_in_bounds(v[r], k, n, m) ? k : INT_MAX);
     }
 #pragma unroll
     for (int r = 0; r < RN; ++r)
       if (first[r] == INT_MAX && last[r] != INT_MIN)
-        first[r] = row_first(rows[r] + WFA_WARP, lo + WFA_WARP, last[r]);
+        first[r] = row_first(rows[r] + LW, lo + LW, last[r]);
     // Antidiagonal bounds: I[k] = max(M'[k-1], I'[k-1]) + 1 and
     // D[k] = max(M'[k+1], D'[k+1]) both lie one antidiagonal above a source
     // cell.  M's bound is set by the extend step.
@@ -923,12 +1000,12 @@ struct PairAligner {
   WFA_D void null_cells(const WfD& d, int from, int to) {
     from = imax(from, d.a);
     to = imin(to, d.b);
-    for (int k = from + lane; k <= to; k += WFA_WARP) d.vals[k - d.a] = kOffsetNull;
+    for (int k = from + lane; k <= to; k += LW) d.vals[k - d.a] = kOffsetNull;
   }
   // Wavefront::trim_nulled (src/wavefront.rs:463-490) of component c at s.
   WFA_D void trim_nulled(int c, int s, int lo, int hi) {
     WfD d = slot(c, s);
-    Warp::sync();
+    G::sync();
     if (!wf_present(d) || (d.flags & kNullFlag) || d.lo > d.hi || (lo <= d.lo && hi >= d.hi)) return;
     const int nlo = imax(lo, d.lo), nhi = imin(hi, d.hi);
     if (nlo > nhi) {
@@ -953,7 +1030,7 @@ struct PairAligner {
   // at an earlier score; with `record`, keep the kept offsets.
   WFA_D void dom_prune(int s, int c, bool record) {
     WfD d = slot(c, s);
-    Warp::sync();
+    G::sync();
     if (!wf_present(d) || d.lo > d.hi) return;
     int32_t* b = ws.dom + (int64_t)c * dom_len + (d.lo - hist_lo);
     const int cnt = d.hi - d.lo + 1;
@@ -961,13 +1038,13 @@ struct PairAligner {
     if (d.lo < hist_lo || d.hi - hist_lo >= dom_len) std::abort();  // emulation-only check
 #endif
     int first = cnt, last = -1;
-    for (int i = lane; i < cnt; i += WFA_WARP)
+    for (int i = lane; i < cnt; i += LW)
       if (d.vals[d.lo + i - d.a] > b[i]) { first = imin(first, i); last = imax(last, i); }
-    first = Warp::min(first);
-    last = Warp::max(last) + 1;  // one past the last kept cell
+    first = G::min(first);
+    last = G::max(last) + 1;  // one past the last kept cell
     if (first >= cnt) last = first;
     if (record)
-      for (int i = first + lane; i < last; i += WFA_WARP) b[i] = imax(b[i], d.vals[d.lo + i - d.a]);
+      for (int i = first + lane; i < last; i += LW) b[i] = imax(b[i], d.vals[d.lo + i - d.a]);
     null_cells(d, d.lo, d.lo + first - 1);
     null_cells(d, d.lo + last, d.hi);
     if (first == last) {
@@ -978,7 +1055,7 @@ struct PairAligner {
       d.hi = d.lo + last - 1;
       d.lo = d.lo + first;
     }
-    Warp::sync();
+    G::sync();
     put(c, s, d);
   }
   // endsfree_dominance_update (src/aligner.rs:1322-1338): M after extend.
@@ -989,15 +1066,15 @@ struct PairAligner {
 #if !(defined(__CUDACC__) && !defined(WFA_EMU))
     if (d.lo < hist_lo || d.hi - hist_lo >= dom_len) std::abort();  // emulation-only check
 #endif
-    for (int k = d.lo + lane; k <= d.hi; k += WFA_WARP) b[k - d.lo] = imax(b[k - d.lo], d.vals[k - d.a]);
-    Warp::sync();
+    for (int k = d.lo + lane; k <= d.hi; k += LW) b[k - d.lo] = imax(b[k - d.lo], d.vals[k - d.a]);
+    G::sync();
   }
   // extend_matches_packed_endsfree_best (src/extend.rs:179-232): extend every
   // cell and find the free-end cell leaving the fewest bases to its free end
   // gap (endsfree_left, src/termination.rs:65-86), the lowest diagonal on ties.
   WFA_D bool extend_best(WfD& d, int& rk, int& roff, int& rleft) {
     int bl = INT_MAX, bkk = INT_MAX;
-    for (int k = d.lo + lane; k <= d.hi; k += WFA_WARP) {
+    for (int k = d.lo + lane; k <= d.hi; k += LW) {
       int32_t off = d.vals[k - d.a];
       if (off < 0) continue;  // NULL (M offsets are valid or NULL)
       int v = off - k, h = off;
@@ -1014,10 +1091,10 @@ struct PairAligner {
         if (left < bl) { bl = left; bkk = k; }
       }
     }
-    Warp::sync();
-    rleft = Warp::min(bl);
+    G::sync();
+    rleft = G::min(bl);
     if (rleft == INT_MAX) return false;
-    rk = Warp::min(bl == rleft ? bkk : INT_MAX);
+    rk = G::min(bl == rleft ? bkk : INT_MAX);
     roff = d.vals[rk - d.a];
     return true;
   }
@@ -1026,7 +1103,7 @@ struct PairAligner {
     const bool prune = hk() == WFA_HEURISTIC_NONE || hk() == WFA_HEURISTIC_BANDED_STATIC;
     if (prune && c_has && c_total > score) ef_prune(score, c_total);
     WfD d = slot(CM, score);
-    Warp::sync();
+    G::sync();
     if (wf_present(d)) {
       int k, off, left;
       if (extend_best(d, k, off, left)) {
@@ -1065,7 +1142,7 @@ struct PairAligner {
   // src/termination.rs:31-58) when `endsfree_term`, else INT_MAX.
   WFA_D int extend_wf(WfD& d, bool endsfree_term, int& term_off) {
     int best = INT_MAX, best_off = 0;
-    for (int k = d.lo + lane; k <= d.hi; k += WFA_WARP) {
+    for (int k = d.lo + lane; k <= d.hi; k += LW) {
       int32_t off = d.vals[k - d.a];
       if (off >= 0) {
         int v = off - k, h = off;
@@ -1080,9 +1157,9 @@ struct PairAligner {
         }
       }
     }
-    Warp::sync();
+    G::sync();
     if (endsfree_term) {
-      int kb = Warp::min(best);
+      int kb = G::min(best);
       if (kb != INT_MAX) term_off = d.vals[kb - d.a];
       (void)best_off;
       return kb;
@@ -1111,14 +1188,14 @@ struct PairAligner {
   // Warp max of the SW scores with the lowest diagonal among the maxima.
   WFA_D void sw_max(const WfD& d, int score, int& cmax, int& ck, int& coff) {
     int best = INT_MIN, bk = INT_MAX;
-    for (int k = d.lo + lane; k <= d.hi; k += WFA_WARP) {
+    for (int k = d.lo + lane; k <= d.hi; k += LW) {
       bool ok;
       int sw = sw_score(d, k, score, ok);
       if (ok && (sw > best || (sw == best && k < bk))) { best = sw; bk = k; }
     }
-    cmax = Warp::max(best);
+    cmax = G::max(best);
     int cand = (best == cmax) ? bk : INT_MAX;
-    ck = Warp::min(cand);
+    ck = G::min(cand);
     if (cmax == INT_MIN) { ck = 0; coff = 0; }
     else coff = d.vals[ck - d.a];
   }
@@ -1133,22 +1210,22 @@ struct PairAligner {
         int blo = d.lo, bhi = d.hi;
         if (bhi - blo + 1 < hp0) return false;
         int mn = INT_MAX;
-        for (int k = blo + lane; k <= bhi; k += WFA_WARP) mn = imin(mn, dist(d, k));
-        int min_d = imin(Warp::min(mn), imax(n, m));
+        for (int k = blo + lane; k <= bhi; k += LW) mn = imin(mn, dist(d, k));
+        int min_d = imin(G::min(mn), imax(n, m));
         int ak = m - n, thr = hp1;
         auto ok = [&](int k) { return (int32_t)((uint32_t)dist(d, k) - (uint32_t)min_d) <= thr; };
         int top = imin(ak, d.hi), nlo = d.lo;
         if (top > d.lo) {
           int f = INT_MAX;
-          for (int k = d.lo + lane; k < top; k += WFA_WARP) if (ok(k)) { f = k; break; }
-          f = Warp::min(f);
+          for (int k = d.lo + lane; k < top; k += LW) if (ok(k)) { f = k; break; }
+          f = G::min(f);
           nlo = imin(f, top);
         }
         int bottom = imax(ak, nlo), nhi = d.hi;
         if (d.hi > bottom) {
           int l = INT_MIN;
-          for (int k = d.hi - lane; k > bottom; k -= WFA_WARP) if (ok(k)) { l = k; break; }
-          l = Warp::max(l);
+          for (int k = d.hi - lane; k > bottom; k -= LW) if (ok(k)) { l = k; break; }
+          l = G::max(l);
           nhi = imax(l, bottom);
         }
         d.lo = nlo;
@@ -1189,11 +1266,11 @@ struct PairAligner {
             return ok && !(mx - sw >= xd);
           };
           int f = INT_MAX;
-          for (int k = d.lo + lane; k <= d.hi; k += WFA_WARP) if (keep(k)) { f = k; break; }
-          int nlo = imin(Warp::min(f), d.hi + 1);
+          for (int k = d.lo + lane; k <= d.hi; k += LW) if (keep(k)) { f = k; break; }
+          int nlo = imin(G::min(f), d.hi + 1);
           int l = INT_MIN;
-          for (int k = d.hi - lane; k >= nlo; k -= WFA_WARP) if (keep(k)) { l = k; break; }
-          int nhi = imax(Warp::max(l), nlo - 1);
+          for (int k = d.hi - lane; k >= nlo; k -= LW) if (keep(k)) { l = k; break; }
+          int nhi = imax(G::max(l), nlo - 1);
           d.lo = nlo;
           d.hi = nhi;
           if (cmax > hs.max_sw_score) { hs.max_sw_score = cmax; hs.max_sw_k = ck; }
@@ -1238,7 +1315,7 @@ struct PairAligner {
     if (d.lo > d.hi) { d.flags |= kNullFlag; d.a = d.lo; d.b = d.hi; }
     WfD eq[NC];
     for (int c = 1; c < NC; ++c) eq[c] = slot(c, score);
-    Warp::sync();
+    G::sync();
     put_ns(CM, score, d);
     if (AFF) {
       for (int c = 1; c < NC; ++c) {
@@ -1250,7 +1327,7 @@ struct PairAligner {
         put_ns(c, score, w);
       }
     }
-    Warp::sync();
+    G::sync();
     return false;
   }
 
@@ -1293,8 +1370,8 @@ struct PairAligner {
     cidx = 0;
     gstep = score_step_gcd();
     gphase = 0;
-    for (int i = lane; i < scope * NC; i += WFA_WARP) ws.ring[i] = wf_none();
-    Warp::sync();
+    for (int i = lane; i < scope * NC; i += LW) ws.ring[i] = wf_none();
+    G::sync();
     hist_lo = -(n + scope + 2);
     hist_hi = m + scope + 2;
     num_null_steps = 0;
@@ -1321,7 +1398,7 @@ struct PairAligner {
     if (gphase != 0) {
       ++num_null_steps;
       for (int c = 0; c < NC; ++c) put_ns(c, s, wf_none());
-      Warp::sync();
+      G::sync();
     } else {
       compute_step(s);
     }
@@ -1338,18 +1415,18 @@ struct PairAligner {
       return false;
     }
     int ak = 0;
-    for (int k0 = d.lo + lane; k0 <= d.hi; k0 += WFA_WARP * UNR) {
+    for (int k0 = d.lo + lane; k0 <= d.hi; k0 += LW * UNR) {
       // Offsets and first sequence words of UNR diagonals, then the rest.
       int32_t off[UNR], R[UNR];
       uint32_t x[UNR];
 #pragma unroll
       for (int u = 0; u < UNR; ++u) {
-        const int k = k0 + u * WFA_WARP;
+        const int k = k0 + u * LW;
         off[u] = k <= d.hi ? d.vals[k - d.a] : -1;
       }
 #pragma unroll
       for (int u = 0; u < UNR; ++u) {
-        const int k = k0 + u * WFA_WARP;
+        const int k = k0 + u * LW;
         R[u] = 0;
         x[u] = 0;
         if (off[u] >= 0) {
@@ -1359,7 +1436,7 @@ struct PairAligner {
       }
 #pragma unroll
       for (int u = 0; u < UNR; ++u) {
-        const int k = k0 + u * WFA_WARP;
+        const int k = k0 + u * LW;
         if (off[u] < 0) continue;
         if (R[u] > 0) {
           // lcp_fwd with its first compare done above
@@ -1377,9 +1454,9 @@ struct PairAligner {
         ak = imax(ak, 2 * off[u] - k);
       }
     }
-    ak = Warp::max(ak);
+    ak = G::max(ak);
     if (lane == 0) slot(CM, score).adub = ak;
-    Warp::sync();
+    G::sync();
     // check_component_termination, src/aligner.rs:3268-3302
     WfD e = slot(comp_end, score);
     int kend = m - n;
@@ -1465,12 +1542,12 @@ struct PairAligner {
     }
     cg_begin += 1;
     cg_score = ascore;
-    Warp::sync();
+    G::sync();
   }
 
   // backtrace_components (src/aligner.rs:1489-1535): the BiWFA base case's.
   WFA_D void backtrace_components(int score, int k, int offset, int cend) {
-    Warp::sync();
+    G::sync();
     if (AFF) {
       backtrace_affine_classic(score, k, offset, cend);
     } else {
@@ -1479,7 +1556,7 @@ struct PairAligner {
       backtrace_linear(score, k, offset);
       cg_begin += 1;
       cg_score = score;
-      Warp::sync();
+      G::sync();
     }
   }
 
@@ -1487,7 +1564,7 @@ struct PairAligner {
   WFA_D void run(uint8_t op, int cnt) {  // write_ops, src/backtrace.rs:689-698
     if (cnt <= 0) return;
     if (cg_begin - cnt + 1 < 0) { status = WFA_STATUS_OOM; cg_begin = -1; return; }
-    for (int i = lane; i < cnt; i += WFA_WARP) cg[cg_begin - i] = op;
+    for (int i = lane; i < cnt; i += LW) cg[cg_begin - i] = op;
     cg_begin -= cnt;
   }
   WFA_D void matches(int cnt) {  // write_matches, src/backtrace.rs:111-128
@@ -1688,7 +1765,7 @@ struct PairAligner {
   WFA_D bool fwd(int64_t& p, int64_t limit, uint8_t op, int cnt) {
     if (cnt <= 0) return true;
     if (p + cnt > limit) { status = WFA_STATUS_OOM; return false; }
-    for (int i = lane; i < cnt; i += WFA_WARP) cg[p + i] = op;
+    for (int i = lane; i < cnt; i += LW) cg[p + i] = op;
     p += cnt;
     return true;
   }
@@ -1724,7 +1801,7 @@ struct PairAligner {
       if (lane == 0) cg[rd] = st.op;
       c = st.c; s = st.s; kk = st.k;
     }
-    Warp::sync();
+    G::sync();
     const bool affine = AFF;
     int64_t p = 0;
     int v = bv, h = bh;
@@ -1732,7 +1809,7 @@ struct PairAligner {
     bool in_m = true;
     for (int64_t i = rd; i < cg_cap; ++i) {
       const uint8_t op = cg[i];
-      Warp::sync();  // every lane has read cg[i] before it may be overwritten
+      G::sync();  // every lane has read cg[i] before it may be overwritten
       if (in_m || !affine) {
         const int nm = lcp_fwd(pat, v, txt, h, imax(0, imin(n - v, m - h)));
         if (!fwd(p, i + 1, 'M', nm)) return;
@@ -1754,11 +1831,11 @@ struct PairAligner {
   }
 
   WFA_D void backtrace_from(int score, int k, int offset) {  // src/aligner.rs:1414-1436
-    Warp::sync();
+    G::sync();
     if (GEN && pgb) {
       backtrace_piggyback(score, k, offset);
       cg_score = score;
-      Warp::sync();
+      G::sync();
       return;
     }
     cg_end = cg_cap;
@@ -1767,7 +1844,7 @@ struct PairAligner {
     else backtrace_linear(score, k, offset);
     cg_begin += 1;
     cg_score = score;
-    Warp::sync();
+    G::sync();
   }
 
   // ---- CIGAR post-processing: src/cigar.rs, src/aligner.rs:1545-1640 ----------
@@ -1925,47 +2002,70 @@ struct PairAligner {
 
   // ---- one pair: align_end2end_span (src/aligner.rs:638-698) and
   // align_endsfree (:707-831), C compatibility ----------------------------------
-  WFA_D int32_t align() {
+  // The score loop as begin() / step() / finish(): step() runs the loop from
+  // the extend of one score that can hold a wavefront (a multiple of gstep)
+  // through the next such score's compute, with the all-null scores between.
+  // align() is begin(), steps until one returns true, finish().
+  int32_t cur;  // the score loop's current score
+  WFA_D void begin() {
     retry = false;
     hused = 0;
     cg_begin = 0; cg_end = 0; cg_score = INT_MIN; cg_ev = -1; cg_eh = -1;
     init_alignment();
-    int score = 0;
+    cur = 0;
+  }
+  // One step of the score loop; true when the loop is over (status set, or
+  // retry).
+  WFA_D bool step() {
     const int hard_limit = 1 << 26;  // no reference alignment runs this long
-    if (!retry) {
-      for (;;) {
-        bool done;
-        if (gphase != 0) {  // all-null score: no M to extend (extend_end2end, null branch)
-          if (GEN && corr && c_has && c_total <= score) {
-            // Corrected: the candidate is final once the score reaches its
-            // total; null steps do not end the search while one is pending.
-            done = true;
-            end_score = c_score; end_k = c_k; end_off = c_off;
-            status = WFA_STATUS_END_REACHED;
-          } else {
-            done = !(GEN && corr && c_has) && num_null_steps > scope;
-            if (done) status = WFA_STATUS_END_UNREACHABLE;
-          }
-          if (!modular) {
-            if ((int64_t)(score + 1) * hist_nc > P.hist_scores) { retry = true; break; }
-            if (lane == 0)
-              for (int c = 0; c < hist_nc; ++c) ws.hist[(int64_t)score * hist_nc + c] = int4{1, 0, 0, 0};
-          }
+    int score = cur;
+    for (;;) {
+      bool done;
+      if (gphase != 0) {  // all-null score: no M to extend (extend_end2end, null branch)
+        if (GEN && corr && c_has && c_total <= score) {
+          // Corrected: the candidate is final once the score reaches its
+          // total; null steps do not end the search while one is pending.
+          done = true;
+          end_score = c_score; end_k = c_k; end_off = c_off;
+          status = WFA_STATUS_END_REACHED;
         } else {
-          done = extend_step(score);
-          hist_commit(score);
+          done = !(GEN && corr && c_has) && num_null_steps > scope;
+          if (done) status = WFA_STATUS_END_UNREACHABLE;
         }
-        if (done || retry) break;
-        ++score;
-        advance();
-        gphase = gphase + 1 == gstep ? 0 : gphase + 1;
-        if (!has_slot(score)) { status = WFA_STATUS_MAX_STEPS_REACHED; break; }
-        if (gphase != 0) ++num_null_steps;
-        else compute_step(score);
-        if (retry) break;
-        if (score >= P.max_steps || score >= hard_limit) { status = WFA_STATUS_MAX_STEPS_REACHED; break; }
+        if (!modular) {
+          if ((int64_t)(score + 1) * hist_nc > P.hist_scores) { retry = true; break; }
+          if (lane == 0)
+            for (int c = 0; c < hist_nc; ++c) ws.hist[(int64_t)score * hist_nc + c] = int4{1, 0, 0, 0};
+        }
+      } else {
+        done = extend_step(score);
+        hist_commit(score);
       }
+      if (done || retry) break;
+      ++score;
+      advance();
+      gphase = gphase + 1 == gstep ? 0 : gphase + 1;
+      if (!has_slot(score)) { status = WFA_STATUS_MAX_STEPS_REACHED; break; }
+      const bool computed = gphase == 0;
+      if (computed) compute_step(score);
+      else ++num_null_steps;
+      if (retry) break;
+      if (score >= P.max_steps || score >= hard_limit) { status = WFA_STATUS_MAX_STEPS_REACHED; break; }
+      if (computed) { cur = score; return false; }
     }
+    cur = score;
+    return true;
+  }
+  WFA_D int32_t align() {
+    begin();
+    if (!retry)
+      while (!step()) {
+      }
+    return finish();
+  }
+  // After the score loop: backtrace, CIGAR post-processing and the status.
+  WFA_D int32_t finish() {
+    const int32_t score = cur;
     if (retry) { status = kStatusRetry; return 0; }
     int32_t result = score;
     const bool cigar = P.compute_alignment != 0;
@@ -2014,26 +2114,25 @@ struct PairAligner {
   }
 };
 
-// Set up and align pair `pair` of the launch with workspace `ws`, writing
-// its result.  Returns true if the pair must be retried with more scratch.
-template <int CLS, class S, bool GEN = true>
-WFA_D bool align_one(const AlignParams& P, const Workspace& ws, int64_t pair, S pat, S txt) {
-  PairAligner<CLS, S, GEN> A(P);
-  A.ws = ws;
-  A.lane = Warp::lane();
+// Per-pair set-up of an aligner A (its workspace and lane already set) for
+// pair `pair` of the launch.
+template <int CLS, class S, bool GEN, int LW>
+WFA_D void setup_pair(PairAligner<CLS, S, GEN, 1, LW>& A, const AlignParams& P, int64_t pair, S pat,
+                      S txt) {
   A.pat = pat;
   A.txt = txt;
   A.n = P.p_len[pair];
   A.m = P.t_len[pair];
   A.scope = P.scope;
   A.wmax = P.wmax;
+  A.compact = P.ring_slots > 0;
   A.modular = P.compute_alignment == 0;
   A.pgb = GEN && !A.modular && P.piggyback != 0;
   // Med/low components are modular: no score cap.
   A.cap = A.modular || A.pgb ? INT_MAX : imax(A.dims_num(1000, 1000), A.dims_num(A.n, A.m));
   A.endsfree = P.span == WFA_SPAN_ENDSFREE;
   A.hkind = P.hkind; A.hp0 = P.hp0; A.hp1 = P.hp1; A.hp2 = P.hp2;
-  A.hist_nc = A.pgb ? PairAligner<CLS, S, GEN>::NC : 1;
+  A.hist_nc = A.pgb ? PairAligner<CLS, S, GEN, 1, LW>::NC : 1;
   A.keep_null_slots = false;
   A.comp_end = CM;
   if (P.extension) { A.p0 = 0; A.pf = A.n; A.t0 = 0; A.tf = A.m; }
@@ -2045,8 +2144,12 @@ WFA_D bool align_one(const AlignParams& P, const Workspace& ws, int64_t pair, S 
     A.cg = P.cigars + P.cigar_off[pair];
     A.cg_cap = 2 * ((int64_t)A.n + A.m) + 1;
   }
-  int32_t score = A.align();
-  if (A.status == kStatusRetry) return true;
+}
+
+// The result record of an aligned pair (lane 0 of the group writes it).
+template <int CLS, class S, bool GEN, int LW>
+WFA_D void write_result(const PairAligner<CLS, S, GEN, 1, LW>& A, const AlignParams& P, int64_t pair,
+                        int32_t score) {
   if (A.lane == 0) {
     wfa_result_t r;
     r.score = score;
@@ -2062,6 +2165,19 @@ WFA_D bool align_one(const AlignParams& P, const Workspace& ws, int64_t pair, S 
     r.end_offset = A.end_off;
     P.results[pair] = r;
   }
+}
+
+// Set up and align pair `pair` of the launch with workspace `ws`, writing
+// its result.  Returns true if the pair must be retried with more scratch.
+template <int CLS, class S, bool GEN = true, int LW = WFA_WARP>
+WFA_D bool align_one(const AlignParams& P, const Workspace& ws, int64_t pair, S pat, S txt) {
+  PairAligner<CLS, S, GEN, 1, LW> A(P);
+  A.ws = ws;
+  A.lane = Lanes<LW>::lane();
+  setup_pair(A, P, pair, pat, txt);
+  int32_t score = A.align();
+  if (A.status == kStatusRetry) return true;
+  write_result(A, P, pair, score);
   return false;
 }
 

@@ -62,6 +62,7 @@ struct DevBuf {
 
 struct ScratchCfg {
   int32_t wmax;
+  int32_t ring_slots = 0;  // compact ring slots (0: one per score and component)
   int32_t hist_scores;
   int64_t hist_words;
   int64_t dom_words = 0;  // Corrected-mode dominance array per warp
@@ -105,6 +106,9 @@ struct wfa_aligner {
   int occ_key = -1;
   size_t occ_smem = 0;
   int occ_val = 1;
+  int lanes_forced = 0;  // lanes per pair of the lean kernel (0: autotuned)
+  int last_lanes = 0;    // lanes per pair of the last batch's first round
+  int launch_lanes = 0;  // lanes per pair of the last launch
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_kernel_ms = 0.0;
   int64_t last_reruns = 0;  // pair re-runs (larger scratch) of the last call
@@ -371,13 +375,16 @@ static void fill_params(const wfa_aligner_t* h, const wfa_batch_t* b, AlignParam
   P.pair_list = nullptr;
 }
 
-// Initial scratch configuration for a batch whose longest pair has
-// n + m = max_len_sum.  First pass: ring cells in shared memory when a slot
-// of kRingSmemWidth cells per (score, component) fits the budget, and
-// sequences of up to kSeqSmemWords words staged in shared memory.  Pairs that
-// outgrow a configuration are re-run with a larger one (next_cfg).
-static constexpr int kRingSmemWidth = 64, kSeqSmemWords = 64;
-static constexpr size_t kRingSmemBudget = 8 * 1024;  // bytes per warp
+// Scratch configuration of one launch over pairs whose longest has
+// n + m = max_len_sum.  The unidirectional kernel keeps the compact ring
+// (compact_ring_slots): for pairs up to kLongPair its cells sit in shared
+// memory, rows wider than the shared-memory slot going to a spill ring in
+// the lane group's scratch slice as wide as any wavefront of the launch can
+// be, so only an M history that outgrows its slice makes a pair re-run;
+// sequences short enough are staged in shared memory too.  Longer pairs keep
+// the whole ring in the scratch slice.  Pairs that outgrow a configuration
+// are re-run with a larger one (next_round).
+static constexpr int kSeqSmemWords = 64;
 static constexpr size_t kScratchBudget = (size_t)6 << 30;
 
 // Scratch may grow to half of the device memory that is free (counting the
@@ -394,10 +401,13 @@ static size_t scratch_budget(wfa_aligner_t* h) {
 struct Round {
   ScratchCfg cfg;
   bool ring_smem;
+  int lanes;         // lanes per pair (8, 16 or 32)
+  int32_t wspill;    // spill ring width (0: none)
+  int32_t seq_words; // words per sequence staged in shared memory
 };
 
 // Long pairs (n + m above kLongPair) start with the ring in the scratch
-// slice and an M history sized from the lengths: a re-run after an overflow
+// slice and an M history sized from their lengths: a re-run after an overflow
 // late in a long alignment repeats most of its work.
 static constexpr int32_t kLongPair = 2048;
 
@@ -410,18 +420,36 @@ static int32_t max_width(const AlignParams& P, int32_t max_len_sum) {
   return 2 * (max_len_sum + P.scope) + 5;
 }
 
-static Round first_round(const AlignParams& P, int nc, int32_t max_len_sum) {
+// Shared-memory slot width of the compact ring per lane-group width: narrow
+// groups keep many pairs in flight per SM, each with a narrower slot (rows
+// above it spill).
+static int32_t smem_slot_width(int lanes) { return lanes == 8 ? 32 : 64; }
+
+static Round first_round(const AlignParams& P, int nc, int32_t max_len_sum, int lanes = 32,
+                         bool spill = true) {
   Round r;
+  const int cls = metric_class(P.metric);
   const bool longp = max_len_sum > kLongPair;
+  r.lanes = lanes;
   r.cfg.wmax = std::max(8, std::min(max_width(P, max_len_sum), 8192));
+  r.cfg.ring_slots = compact_ring_slots(P, cls);
   // The piggyback backtrace keeps every component's history.
   const int hnc = P.piggyback ? nc : 1;
   r.cfg.hist_scores = P.compute_alignment ? hnc * (longp ? max_len_sum + 3 : 1024) : 0;
   r.cfg.hist_words = P.compute_alignment
                          ? hnc * (int64_t)std::max(32768, (longp ? 64 : 16) * (max_len_sum + 3))
                          : 0;
-  r.ring_smem = !longp && (size_t)P.scope * nc * kRingSmemWidth * 4 <= kRingSmemBudget;
-  if (r.ring_smem) r.cfg.wmax = std::min(r.cfg.wmax, kRingSmemWidth);
+  r.ring_smem = !longp;
+  r.wspill = 0;
+  if (r.ring_smem) {
+    const int32_t wsm = smem_slot_width(lanes);
+    if (spill && r.cfg.wmax > wsm) r.wspill = r.cfg.wmax;
+    r.cfg.wmax = std::min(r.cfg.wmax, wsm);
+  }
+  // Each sequence of the launch is at most max_len_sum long.
+  const bool packed = P.format == WFA_SEQ_PACKED2;
+  r.seq_words = std::min(kSeqSmemWords, packed ? (max_len_sum + 15) / 16 : (max_len_sum + 3) / 4 + 1);
+  r.seq_words = (r.seq_words + 1) & ~1;
   // Corrected ends-free with begin-free seeds prunes dominated cells against
   // a per-diagonal array over [-(n + scope + 2), m + scope + 2] per component.
   const bool dom = P.compat == WFA_COMPAT_CORRECTED && P.match < 0 && P.span == WFA_SPAN_ENDSFREE &&
@@ -431,52 +459,81 @@ static Round first_round(const AlignParams& P, int nc, int32_t max_len_sum) {
 }
 
 static void next_round(Round& r, const AlignParams& P, int32_t max_len_sum) {
-  if (r.ring_smem) {
+  const int32_t full = std::max(8, std::min(max_width(P, max_len_sum), 8192));
+  if (r.ring_smem && r.wspill == 0) {
     r.ring_smem = false;  // retries use the scratch ring at full width
-    r.cfg.wmax = std::max(8, std::min(max_width(P, max_len_sum), 8192));
-  } else {
+    r.cfg.wmax = full;
+  } else if (!r.ring_smem) {
     r.cfg.wmax = std::min(max_width(P, max_len_sum), std::max(r.cfg.wmax, 1) * 4);
   }
+  // (with a spill ring, every row already fits: only the history grows)
   if (P.compute_alignment) {
     r.cfg.hist_scores *= 4;
     r.cfg.hist_words *= 4;
   }
 }
 
-// Sizes the scratch for round r and launches the alignment kernel over
-// `todo` pairs (`list`: their indices, or NULL for 0..todo-1).  No sync.
-static int launch_round(wfa_aligner_t* h, AlignParams& P, const Round& r, int64_t todo,
-                        const int64_t* list, cudaStream_t st, unsigned long long* ctr = nullptr) {
-  const int cls = metric_class(P.metric);
-  const int nc = metric_components(P.metric);
-  P.seq_smem_words = kSeqSmemWords;
+// Fills the launch fields of P for round r and returns the per-block shared
+// memory and the words of one lane group's scratch slice.
+static SmemLayout round_layout(AlignParams& P, const Round& r, int nc, int64_t* group_words) {
+  P.seq_smem_words = r.seq_words;
   P.ring_smem = r.ring_smem ? 1 : 0;
   P.wmax = r.cfg.wmax;
-  const SmemLayout L = smem_layout(P.scope, nc, r.ring_smem ? r.cfg.wmax : 0, P.seq_smem_words);
-  const size_t smem = L.total;
-  if (smem > 200 * 1024) return fail(h, WFA_ERR_UNSUPPORTED, "wavefront ring too large");
-  const int key = cls * 4 + (P.format == WFA_SEQ_PACKED2) * 2 + (needs_general(P) ? 1 : 0);
-  if (key != h->occ_key || smem != h->occ_smem) {
-    h->occ_val = occupancy_blocks_per_sm(P, cls, smem);
-    h->occ_key = key;
-    h->occ_smem = smem;
-  }
-  int64_t ring_words = r.ring_smem ? 0 : (((int64_t)P.scope * nc * r.cfg.wmax + 3) & ~(int64_t)3);
-  int64_t warp_words = ring_words + (int64_t)r.cfg.hist_scores * 4 + r.cfg.hist_words + r.cfg.dom_words;
-  warp_words = std::max<int64_t>((warp_words + 63) & ~(int64_t)63, 64);
-  int64_t max_warps = (int64_t)h->num_sms * h->occ_val * kWarpsPerBlock;
-  int64_t warps = std::max<int64_t>(std::min<int64_t>(max_warps, todo), 1);
-  const size_t budget = (size_t)warps * warp_words * 4 > kScratchBudget ? scratch_budget(h) : kScratchBudget;
-  while (warps > kWarpsPerBlock && (size_t)warps * warp_words * 4 > budget) warps /= 2;
-  int blocks = (int)((warps + kWarpsPerBlock - 1) / kWarpsPerBlock);
-  size_t scratch_bytes = (size_t)blocks * kWarpsPerBlock * warp_words * 4;
-  CUDA_TRY(h, h->scratch.ensure(scratch_bytes), "scratch");
-  CUDA_TRY(h, h->counters.ensure(64), "counters");
-  P.scratch = h->scratch.as<int32_t>();
-  P.warp_words = warp_words;
+  P.ring_slots = r.cfg.ring_slots;
+  P.wspill = r.wspill;
   P.hist_scores = r.cfg.hist_scores;
   P.hist_words = r.cfg.hist_words;
   P.dom_words = r.cfg.dom_words;
+  const int groups = kWarpsPerBlock * 32 / r.lanes;
+  const SmemLayout L = smem_layout(P.scope, nc, cell_slots(P, nc), r.ring_smem ? r.cfg.wmax : 0,
+                                   r.seq_words, groups);
+  int64_t w = slice_ring_words(P, nc) + (int64_t)r.cfg.hist_scores * 4 + r.cfg.hist_words + r.cfg.dom_words;
+  *group_words = std::max<int64_t>((w + 63) & ~(int64_t)63, 64);
+  return L;
+}
+
+// Resident blocks per SM of the round's kernel (cached per handle).
+static int round_occupancy(wfa_aligner_t* h, const AlignParams& P, int cls, int lanes, size_t smem) {
+  const int key = ((cls * 4 + (P.format == WFA_SEQ_PACKED2) * 2 + (needs_general(P) ? 1 : 0)) << 6) | lanes;
+  if (key != h->occ_key || smem != h->occ_smem) {
+    h->occ_val = occupancy_blocks_per_sm(P, cls, lanes, smem);
+    h->occ_key = key;
+    h->occ_smem = smem;
+  }
+  return h->occ_val;
+}
+
+// Sizes the scratch for round r and launches the alignment kernel over
+// `todo` pairs (`list`: their indices, or NULL for 0..todo-1).  No sync.
+static int launch_round(wfa_aligner_t* h, AlignParams& P, const Round& r0, int64_t todo,
+                        const int64_t* list, cudaStream_t st, unsigned long long* ctr = nullptr) {
+  const int cls = metric_class(P.metric);
+  const int nc = metric_components(P.metric);
+  int64_t group_words = 0;
+  // Narrow lane groups keep more rings in a block; a large score scope
+  // (penalties with a match reward) may not fit them, then wider groups run.
+  Round r = r0;
+  SmemLayout L = round_layout(P, r, nc, &group_words);
+  while (L.total > 200 * 1024 && r.lanes < 32) {
+    r.lanes *= 2;
+    L = round_layout(P, r, nc, &group_words);
+  }
+  h->launch_lanes = r.lanes;
+  const size_t smem = L.total;
+  if (smem > 200 * 1024) return fail(h, WFA_ERR_UNSUPPORTED, "wavefront ring too large");
+  const int occ = round_occupancy(h, P, cls, r.lanes, smem);
+  const int gpb = kWarpsPerBlock * 32 / r.lanes;  // lane groups per block
+  int64_t max_groups = (int64_t)h->num_sms * occ * gpb;
+  int64_t groups = std::max<int64_t>(std::min<int64_t>(max_groups, todo), 1);
+  const size_t budget =
+      (size_t)groups * group_words * 4 > kScratchBudget ? scratch_budget(h) : kScratchBudget;
+  while (groups > gpb && (size_t)groups * group_words * 4 > budget) groups /= 2;
+  int blocks = (int)((groups + gpb - 1) / gpb);
+  size_t scratch_bytes = (size_t)blocks * gpb * group_words * 4;
+  CUDA_TRY(h, h->scratch.ensure(scratch_bytes), "scratch");
+  CUDA_TRY(h, h->counters.ensure(64), "counters");
+  P.scratch = h->scratch.as<int32_t>();
+  P.warp_words = group_words;
   P.work_counter = ctr ? ctr : h->counters.as<unsigned long long>();
   P.retry_count = reinterpret_cast<int32_t*>(P.work_counter + 1);
   P.pair_list = list;
@@ -484,10 +541,79 @@ static int launch_round(wfa_aligner_t* h, AlignParams& P, const Round& r, int64_
   CUDA_TRY(h, cudaMemsetAsync(P.work_counter, 0, 16, st), "memset");
   CUDA_TRY(h, cudaEventRecord(h->ev0, st), "event");
   CUDA_TRY(h, cudaGetLastError(), "an earlier CUDA call of this thread");
-  CUDA_TRY(h, launch_unialign(P, cls, blocks, smem, st), "alignment kernel launch");
+  CUDA_TRY(h, launch_unialign(P, cls, r.lanes, blocks, smem, st), "alignment kernel launch");
   CUDA_TRY(h, cudaEventRecord(h->ev1, st), "event");
   h->launches++;
   return WFA_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Lanes per pair of the lean kernel, autotuned per length bucket
+// ---------------------------------------------------------------------------
+// The first device batch of a (device, metric class, encoding, CIGAR or
+// score, length bucket) times each candidate lane-group width on a sample of
+// its pairs (the first kTuneSample, twice each, the faster run counting) and
+// keeps the fastest for the process; the general kernel always takes whole
+// warps.  Results do not depend on the width: every width runs the same
+// per-pair algorithm.
+static constexpr int64_t kTuneSample = 262144, kTuneMinPairs = 65536;
+
+static int length_bucket(int32_t max_len_sum) {
+  return max_len_sum <= 384 ? 0 : max_len_sum <= 1024 ? 1 : max_len_sum <= kLongPair ? 2 : 3;
+}
+static int default_lanes(const AlignParams& P, int bucket) {
+  if (needs_general(P) || bucket == 3) return 32;
+  return bucket == 0 ? 8 : 16;
+}
+
+struct TuneEntry {
+  int lanes;
+  float ms[3];  // candidates 8, 16, 32 (0: not tried)
+  int64_t sample;
+};
+static std::mutex g_tune_mu;
+static std::map<std::vector<int>, TuneEntry> g_tune;
+
+static std::vector<int> tune_key(const wfa_aligner_t* h, const AlignParams& P, int32_t max_len_sum) {
+  return {h->device, metric_class(P.metric), P.format, P.compute_alignment, length_bucket(max_len_sum)};
+}
+
+// Lanes per pair for a batch of `todo` pairs (0..todo-1 on the device).
+static int choose_lanes(wfa_aligner_t* h, const AlignParams& P0, int32_t max_len_sum, int64_t todo,
+                        cudaStream_t st, bool may_tune) {
+  const int bucket = length_bucket(max_len_sum);
+  if (needs_general(P0) || bucket == 3) return 32;
+  if (h->lanes_forced) return h->lanes_forced;
+  const std::vector<int> key = tune_key(h, P0, max_len_sum);
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) return it->second.lanes;
+  }
+  if (!may_tune || todo < kTuneMinPairs) return default_lanes(P0, bucket);
+  const int nc = metric_components(P0.metric);
+  const int64_t sample = std::min(todo, kTuneSample);
+  TuneEntry t{default_lanes(P0, bucket), {0.f, 0.f, 0.f}, sample};
+  float best = 0.f;
+  const int cands[3] = {8, 16, 32};
+  for (int ci = 0; ci < 3; ++ci) {
+    if (bucket > 0 && cands[ci] == 8) continue;
+    float m = 0.f;
+    for (int rep = 0; rep < 2; ++rep) {
+      AlignParams P = P0;
+      Round r = first_round(P, nc, max_len_sum, cands[ci]);
+      if (launch_round(h, P, r, sample, nullptr, st) != WFA_OK) return default_lanes(P0, bucket);
+      if (cudaStreamSynchronize(st) != cudaSuccess) return default_lanes(P0, bucket);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+      m = rep == 0 ? ms : std::min(m, ms);
+    }
+    t.ms[ci] = m;
+    if (best == 0.f || m < best) { best = m; t.lanes = cands[ci]; }
+  }
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  g_tune[key] = t;
+  return t.lanes;
 }
 
 // Runs every pair of a device-resident batch, escalating scratch for pairs
@@ -501,7 +627,8 @@ static int run_device_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t
   if (P.compute_alignment && (!d_cigars || !b->cigar_off))
     return fail(h, WFA_ERR_ARGUMENT, "CIGAR output buffers are required in alignment scope");
   const int nc = metric_components(P.metric);
-  Round r = first_round(P, nc, max_len_sum);
+  const int lanes = choose_lanes(h, P, max_len_sum, b->num_pairs, st, true);
+  Round r = first_round(P, nc, max_len_sum, lanes);
   int64_t todo = b->num_pairs;
   const int64_t* list = nullptr;
   h->last_kernel_ms = 0.0;
@@ -509,6 +636,7 @@ static int run_device_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t
     if (round > 8) return fail(h, WFA_ERR_OOM, "alignment needs more scratch than available");
     int e = launch_round(h, P, r, todo, list, st);
     if (e != WFA_OK) return e;
+    if (round == 0) h->last_lanes = h->launch_lanes;
     int32_t retries = 0;
     CUDA_TRY(h, cudaMemcpyAsync(&retries, P.retry_count, 4, cudaMemcpyDeviceToHost, st), "retry count");
     CUDA_TRY(h, cudaStreamSynchronize(st), "kernel");
@@ -690,7 +818,9 @@ static int run_noalloc_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_
   int32_t* retry = base + 2;
   int32_t* fill = base + 4;
   int64_t* list = reinterpret_cast<int64_t*>(base + kNaHeaderWords);
-  Round r = first_round(P, nc, max_len_sum);
+  // Whole warps per pair, and no spill ring: a row wider than the shared
+  // memory slot re-runs the pair with the ring in its slice.
+  Round r = first_round(P, nc, max_len_sum, 32, false);
   if (P.compute_alignment) {
     const int hnc = P.piggyback ? nc : 1;
     r.cfg.hist_scores = 256 * hnc;
@@ -701,32 +831,19 @@ static int run_noalloc_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_
   const int64_t* lst = nullptr;
   h->last_kernel_ms = 0.0;
   for (;;) {
-    P.seq_smem_words = kSeqSmemWords;
-    P.ring_smem = r.ring_smem ? 1 : 0;
-    P.wmax = r.cfg.wmax;
-    const SmemLayout L = smem_layout(P.scope, nc, r.ring_smem ? r.cfg.wmax : 0, P.seq_smem_words);
+    int64_t warp_words = 0;
+    const SmemLayout L = round_layout(P, r, nc, &warp_words);
     if (L.total > 200 * 1024) return fail(h, WFA_ERR_UNSUPPORTED, "wavefront ring too large");
-    const int key = cls * 4 + (P.format == WFA_SEQ_PACKED2) * 2 + (needs_general(P) ? 1 : 0);
-    if (key != h->occ_key || L.total != h->occ_smem) {
-      h->occ_val = occupancy_blocks_per_sm(P, cls, L.total);
-      h->occ_key = key;
-      h->occ_smem = L.total;
-    }
-    int64_t ring_words = r.ring_smem ? 0 : (((int64_t)P.scope * nc * r.cfg.wmax + 3) & ~(int64_t)3);
-    int64_t warp_words = ring_words + (int64_t)r.cfg.hist_scores * 4 + r.cfg.hist_words + r.cfg.dom_words;
-    warp_words = std::max<int64_t>((warp_words + 63) & ~(int64_t)63, 64);
+    const int occ = round_occupancy(h, P, cls, r.lanes, L.total);
     const int64_t fit_blocks = kNaSliceWords / (warp_words * kWarpsPerBlock);
     if (fit_blocks < 1)
       return fail(h, WFA_ERR_OOM, "an alignment needs more scratch than the fixed no-allocation "
                                   "array holds (use wfa_batch_align_device)");
-    int64_t warps = std::min<int64_t>((int64_t)h->num_sms * h->occ_val * kWarpsPerBlock, todo);
+    int64_t warps = std::min<int64_t>((int64_t)h->num_sms * occ * kWarpsPerBlock, todo);
     int64_t blocks = std::min<int64_t>((std::max<int64_t>(warps, 1) + kWarpsPerBlock - 1) / kWarpsPerBlock,
                                        fit_blocks);
     P.scratch = base + kNaSliceOff;
     P.warp_words = warp_words;
-    P.hist_scores = r.cfg.hist_scores;
-    P.hist_words = r.cfg.hist_words;
-    P.dom_words = r.cfg.dom_words;
     P.work_counter = work;
     P.retry_count = retry;
     P.pair_list = lst;
@@ -734,7 +851,7 @@ static int run_noalloc_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_
     CUDA_TRY(h, cudaMemsetAsync(base, 0, 16, st), "memset");
     CUDA_TRY(h, cudaEventRecord(h->ev0, st), "event");
     CUDA_TRY(h, cudaGetLastError(), "an earlier CUDA call of this thread");
-    CUDA_TRY(h, launch_unialign(P, cls, (int)blocks, L.total, st), "kernel launch");
+    CUDA_TRY(h, launch_unialign(P, cls, r.lanes, (int)blocks, L.total, st), "kernel launch");
     CUDA_TRY(h, cudaEventRecord(h->ev1, st), "event");
     h->launches++;
     int32_t retries = 0;
@@ -1069,6 +1186,34 @@ int wfa_last_error(const wfa_aligner_t* h) { return h ? h->last_err : WFA_ERR_AR
 const char* wfa_last_error_string(const wfa_aligner_t* h) { return h ? h->err_str.c_str() : "null handle"; }
 int64_t wfa_kernel_launches(const wfa_aligner_t* h) { return h ? h->launches : 0; }
 int64_t wfa_last_rerun_pairs(const wfa_aligner_t* h) { return h ? h->last_reruns : 0; }
+int wfa_set_lanes_per_pair(wfa_aligner_t* h, int32_t lanes) {
+  if (!h || !(lanes == 0 || lanes == 8 || lanes == 16 || lanes == 32)) return WFA_ERR_ARGUMENT;
+  h->lanes_forced = lanes;
+  return WFA_OK;
+}
+int32_t wfa_last_lanes_per_pair(const wfa_aligner_t* h) { return h ? h->last_lanes : 0; }
+int32_t wfa_autotune_report(char* out, int32_t cap) {
+  std::string r;
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    char line[256];
+    for (const auto& kv : g_tune) {
+      const std::vector<int>& k = kv.first;
+      const TuneEntry& t = kv.second;
+      std::snprintf(line, sizeof line,
+                    "device %d class %d format %d cigar %d bucket %d: lanes %d (sample %lld pairs; "
+                    "ms 8:%.3f 16:%.3f 32:%.3f)\n",
+                    k[0], k[1], k[2], k[3], k[4], t.lanes, (long long)t.sample, t.ms[0], t.ms[1], t.ms[2]);
+      r += line;
+    }
+  }
+  if (out && cap > 0) {
+    int32_t c = std::min<int32_t>((int32_t)r.size(), cap - 1);
+    std::memcpy(out, r.data(), (size_t)c);
+    out[c] = 0;
+  }
+  return (int32_t)r.size();
+}
 double wfa_last_kernel_ms(const wfa_aligner_t* h) { return h ? h->last_kernel_ms : 0.0; }
 
 static int batch_common(wfa_aligner_t* h, const wfa_batch_t* b) {
@@ -1317,9 +1462,14 @@ int wfa_batch_align(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* result
     fill_params(h, &cb, P);
     P.results = dres + a;
     P.cigars = aln ? h->cigars.as<uint8_t>() : nullptr;
-    Round rd = first_round(P, metric_components(P.metric), I.max_len_sum);
+    // Lanes per pair: the tuned choice of a device batch of this kind, if
+    // one ran in this process, else the bucket's default (chunks are not
+    // timed here: the pipeline would wait on them).
+    const int lanes = choose_lanes(h, P, I.max_len_sum, cn, sc, false);
+    Round rd = first_round(P, metric_components(P.metric), I.max_len_sum, lanes);
     int e2 = launch_round(h, P, rd, cn, nullptr, sc, dctr + 2 * ci);
     if (e2 != WFA_OK) return e2;
+    if (ci == 0) h->last_lanes = h->launch_lanes;
     PIPE_TRY(cudaEventRecord(ev_k[(size_t)ci], sc), "event");
     cudaEvent_t ready = ev_k[(size_t)ci];
     if (aln) {

@@ -54,6 +54,11 @@ struct AlignParams {
   int32_t* scratch;
   int64_t warp_words;  // ints per warp slice
   int32_t wmax;        // ring slot width (cells)
+  // Compact ring of the unidirectional aligner: slots per lane group (0: the
+  // full [scope][components] ring) and the width of the device-memory ring
+  // that takes rows wider than wmax (0: none).
+  int32_t ring_slots;
+  int32_t wspill;
   int32_t wmax_base;   // BiWFA base-case ring slot width (cells)
   int32_t ring_smem;   // 1: ring cells in shared memory (else in the scratch slice)
   int32_t seq_smem_words;  // per sequence staged in shared memory (0: none)
@@ -64,5 +69,37 @@ struct AlignParams {
   unsigned long long* work_counter;
   int32_t* retry_count;
 };
+
+// Score step of the unidirectional aligner: scores that are not multiples
+// of it hold no wavefront (the gcd of the recurrences' score offsets and, with
+// begin-free seeds of a match reward, of the seed scores).  The same rule as
+// PairAligner::score_step_gcd, for sizing the compact ring on the host.
+#if defined(__CUDACC__)
+__host__ __device__
+#endif
+inline int score_gcd(int a, int b) {
+  a = a < 0 ? -a : a;
+  b = b < 0 ? -b : b;
+  while (b) { int t = a % b; a = b; b = t; }
+  return a;
+}
+#if defined(__CUDACC__)
+__host__ __device__
+#endif
+inline int compact_ring_slots(const AlignParams& P, int cls) {
+  int g;
+  if (cls == kEditClass) g = 1;
+  else if (cls == kLinearClass) g = score_gcd(P.mismatch, P.o1);
+  else g = score_gcd(score_gcd(P.mismatch, P.o1 + P.e1), P.e1);
+  if (cls == kAffine2pClass) g = score_gcd(score_gcd(g, P.o2 + P.e2), P.e2);
+  const bool ef = P.span == WFA_SPAN_ENDSFREE;
+  const int p0 = P.extension ? 0 : P.p0, t0 = P.extension ? 0 : P.t0;
+  if (ef && P.match != 0 && (p0 > 0 || t0 > 0)) g = score_gcd(g, -P.match);
+  if (g < 1) g = 1;
+  int slots = (P.scope - 1) / g + 1;
+  if (cls >= kAffineClass) slots += 2 * (P.e1 / g + 1);
+  if (cls == kAffine2pClass) slots += 2 * (P.e2 / g + 1);
+  return slots;
+}
 
 }  // namespace wfab

@@ -10,25 +10,49 @@ constexpr int kWarpsPerBlock = 4;
 constexpr int kMinBlocksPerSM = 6;  // register budget: 65536 / (6 * 128) = 85 per thread
 constexpr int kDescBytes = 32;      // sizeof(WfD)
 
-// Per-block dynamic shared memory: descriptor rings, staged sequences and
-// (optionally) ring cells, each as kWarpsPerBlock per-warp slices.
+// Per-block dynamic shared memory of the unidirectional kernel: descriptor
+// rings, staged sequences and (optionally) ring cells, each as one slice per
+// lane group (`groups` groups per block).
 struct SmemLayout {
-  size_t desc_bytes, seq_bytes, ring_bytes;  // per warp
+  size_t desc_bytes, seq_bytes, ring_bytes;  // per group
   size_t desc_off, seq_off, ring_off, total;  // per block
 };
 #if defined(__CUDACC__)
 __host__ __device__
 #endif
-inline SmemLayout smem_layout(int scope, int nc, int ring_wmax, int seq_words) {
+inline SmemLayout smem_layout(int scope, int nc, int cell_slots, int ring_wmax, int seq_words,
+                              int groups) {
   SmemLayout L;
   L.desc_bytes = (size_t)scope * nc * kDescBytes;
   L.seq_bytes = (size_t)2 * seq_words * 4;
-  L.ring_bytes = (size_t)scope * nc * ring_wmax * 4;
+  L.ring_bytes = (size_t)cell_slots * ring_wmax * 4;
   L.desc_off = 0;
-  L.seq_off = L.desc_off + kWarpsPerBlock * L.desc_bytes;
-  L.ring_off = L.seq_off + kWarpsPerBlock * L.seq_bytes;
-  L.total = L.ring_off + kWarpsPerBlock * L.ring_bytes;
+  L.seq_off = L.desc_off + (size_t)groups * L.desc_bytes;
+  L.ring_off = L.seq_off + (size_t)groups * L.seq_bytes;
+  L.total = L.ring_off + (size_t)groups * L.ring_bytes;
   return L;
+}
+
+// Cell slots of a lane group's ring: the compact ring's, or one per score and
+// component.
+#if defined(__CUDACC__)
+__host__ __device__
+#endif
+inline int cell_slots(const AlignParams& P, int nc) {
+  return P.ring_slots > 0 ? P.ring_slots : P.scope * nc;
+}
+
+// Words at the start of a lane group's scratch slice taken by ring cells:
+// the whole ring when its cells are not in shared memory, else the spill
+// ring of the compact layout (if any).  A multiple of 4 (16-byte records
+// follow).
+#if defined(__CUDACC__)
+__host__ __device__
+#endif
+inline int64_t slice_ring_words(const AlignParams& P, int nc) {
+  const int64_t slots = cell_slots(P, nc);
+  int64_t w = P.ring_smem ? (P.ring_slots > 0 ? slots * P.wspill : 0) : slots * P.wmax;
+  return (w + 3) & ~(int64_t)3;
 }
 
 // BiWFA per-warp scratch slice (int32 word offsets).  seq_len_sum is the
@@ -61,8 +85,9 @@ inline BiLayout bi_layout(int scope, int nc, int wmax, int wmax_base, int hist_s
 
 bool needs_general(const AlignParams& P);
 cudaError_t launch_biwfa(const AlignParams& P, int cls, int blocks, size_t smem, cudaStream_t st);
-cudaError_t launch_unialign(const AlignParams& P, int metric_class, int blocks, size_t smem,
+// Lanes per pair: 8, 16 or 32 (groups of 32 / lanes pairs per warp).
+cudaError_t launch_unialign(const AlignParams& P, int metric_class, int lanes, int blocks, size_t smem,
                             cudaStream_t st);
-int occupancy_blocks_per_sm(const AlignParams& P, int metric_class, size_t smem);
+int occupancy_blocks_per_sm(const AlignParams& P, int metric_class, int lanes, size_t smem);
 
 }  // namespace wfab
