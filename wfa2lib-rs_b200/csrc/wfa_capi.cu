@@ -98,6 +98,7 @@ struct wfa_aligner {
   int num_sms = 148;
   DevBuf seq, poff, plen, toff, tlen, coff, results, cigars, dense, scratch, counters, pairlist;
   DevBuf chunkinfo;               // per-chunk counters and dense CIGAR ranges
+  DevBuf order;                   // cost ordering: keys, histograms, pair lists
   int64_t* hinfo = nullptr;       // pinned host copy of the chunk info
   size_t hinfo_cap = 0;
   int64_t launches = 0;
@@ -619,7 +620,8 @@ static int choose_lanes(wfa_aligner_t* h, const AlignParams& P0, int32_t max_len
 // Runs every pair of a device-resident batch, escalating scratch for pairs
 // that need more.  Synchronises `st` to read the retry count.
 static int run_device_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* d_results,
-                            uint8_t* d_cigars, cudaStream_t st, int32_t max_len_sum) {
+                            uint8_t* d_cigars, cudaStream_t st, int32_t max_len_sum,
+                            const int64_t* first_list = nullptr) {
   AlignParams P;
   fill_params(h, b, P);
   P.results = d_results;
@@ -630,7 +632,7 @@ static int run_device_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t
   const int lanes = choose_lanes(h, P, max_len_sum, b->num_pairs, st, true);
   Round r = first_round(P, nc, max_len_sum, lanes);
   int64_t todo = b->num_pairs;
-  const int64_t* list = nullptr;
+  const int64_t* list = first_list;
   h->last_kernel_ms = 0.0;
   for (int round = 0; todo > 0; ++round) {
     if (round > 8) return fail(h, WFA_ERR_OOM, "alignment needs more scratch than available");
@@ -774,9 +776,44 @@ static int run_biwfa_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t*
 }
 
 static int run_batch_kind(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* d_results,
-                          uint8_t* d_cigars, cudaStream_t st, int32_t max_len_sum) {
+                          uint8_t* d_cigars, cudaStream_t st, int32_t max_len_sum,
+                          const int64_t* first_list = nullptr) {
   if (b->span == WFA_SPAN_BIWFA) return run_biwfa_batch(h, b, d_results, d_cigars, st, max_len_sum);
-  return run_device_batch(h, b, d_results, d_cigars, st, max_len_sum);
+  return run_device_batch(h, b, d_results, d_cigars, st, max_len_sum, first_list);
+}
+
+// Cost ordering (wfa_order.cu) for lean batches of short pairs: the lane
+// groups of a warp then get pairs of similar cost.  Batches below
+// kSortMinPairs run in input order.
+static constexpr int64_t kSortMinPairs = 16384;
+
+static bool orders_batch(const wfa_aligner_t* h, const wfa_batch_t* b) {
+  if (b->span == WFA_SPAN_BIWFA || b->num_pairs < kSortMinPairs) return false;
+  AlignParams P;
+  fill_params(h, b, P);
+  return !needs_general(P);
+}
+
+// Layout of h->order for n pairs and `parts` separately ordered ranges:
+// keys (u16), pair lists (i64), then per range kOrderStride ints: a
+// histogram and a fill counter array (kOrderBins each) and a longest-pair
+// word.
+static constexpr int64_t kOrderStride = 2 * kOrderBins + 32;
+struct OrderBufs {
+  uint16_t* keys;
+  int64_t* list;
+  int32_t* hist;  // [parts][kOrderStride]
+};
+static int order_bufs(wfa_aligner_t* h, int64_t n, int64_t parts, OrderBufs* o) {
+  const size_t keys = ((size_t)n * 2 + 15) & ~(size_t)15;
+  const size_t list = (size_t)n * 8;
+  const size_t hist = (size_t)parts * kOrderStride * 4;
+  CUDA_TRY(h, h->order.ensure(keys + list + hist), "ordering buffers");
+  char* base = h->order.as<char>();
+  o->keys = reinterpret_cast<uint16_t*>(base);
+  o->list = reinterpret_cast<int64_t*>(base + keys);
+  o->hist = reinterpret_cast<int32_t*>(base + keys + list);
+  return WFA_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -926,7 +963,8 @@ wfa_aligner_t* wfa_aligner_create(wfa_metric_t metric, const wfa_penalties_t* pe
     return nullptr;
   }
   for (DevBuf* b : {&h->seq, &h->poff, &h->plen, &h->toff, &h->tlen, &h->coff, &h->results,
-                    &h->cigars, &h->dense, &h->scratch, &h->counters, &h->pairlist, &h->chunkinfo})
+                    &h->cigars, &h->dense, &h->scratch, &h->counters, &h->pairlist, &h->chunkinfo,
+                    &h->order})
     b->st = h->stream;
   if (event_pool(h, 32) != cudaSuccess) {
     wfa_aligner_destroy(h);
@@ -951,7 +989,8 @@ void wfa_aligner_destroy(wfa_aligner_t* h) {
   for (cudaStream_t x : {h->stream, h->s_in, h->s_out, h->s_cig})
     if (x) cudaStreamSynchronize(x);
   for (DevBuf* b : {&h->seq, &h->poff, &h->plen, &h->toff, &h->tlen, &h->coff, &h->results,
-                    &h->cigars, &h->dense, &h->scratch, &h->counters, &h->pairlist, &h->chunkinfo})
+                    &h->cigars, &h->dense, &h->scratch, &h->counters, &h->pairlist, &h->chunkinfo,
+                    &h->order})
     b->release();
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->pinned) cudaFreeHost(h->pinned);
@@ -1241,13 +1280,31 @@ int wfa_batch_align_device(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t*
   CUDA_TRY(h, h->counters.ensure(64), "counters");
   int32_t* d_max = reinterpret_cast<int32_t*>(h->counters.as<char>() + 32);
   CUDA_TRY(h, cudaMemsetAsync(d_max, 0, 4, st), "memset");
-  max_lengths<<<256, 256, 0, st>>>(b->p_len, b->t_len, b->num_pairs, d_max);
+  const bool order = orders_batch(h, b);
+  OrderBufs ob{};
+  if (order) {
+    // The longest pair and the cost keys in one pass over the batch.
+    if (int e = order_bufs(h, b->num_pairs, 1, &ob)) return e;
+    CUDA_TRY(h, cudaMemsetAsync(ob.hist, 0, kOrderStride * 4, st), "memset");
+    CUDA_TRY(h, launch_order_count(static_cast<const uint8_t*>(b->seq), b->format == WFA_SEQ_PACKED2,
+                                   b->p_off, b->p_len, b->t_off, b->t_len, b->num_pairs, h->num_sms, d_max,
+                                   ob.keys, ob.hist, st), "cost keys");
+  } else {
+    max_lengths<<<256, 256, 0, st>>>(b->p_len, b->t_len, b->num_pairs, d_max);
+    CUDA_TRY(h, cudaGetLastError(), "max lengths");
+  }
   h->launches++;
-  CUDA_TRY(h, cudaGetLastError(), "max lengths");
   int32_t mx = 0;
   CUDA_TRY(h, cudaMemcpyAsync(&mx, d_max, 4, cudaMemcpyDeviceToHost, st), "D2H");
   CUDA_TRY(h, cudaStreamSynchronize(st), "max lengths");
-  return run_batch_kind(h, b, results, cigars, st, mx);
+  const int64_t* first = nullptr;
+  if (order && length_bucket(mx) <= 2) {
+    CUDA_TRY(h, launch_order_scatter(ob.keys, b->num_pairs, ob.hist, ob.hist + kOrderBins, ob.list,
+                                     h->num_sms, st), "cost order");
+    h->launches++;
+    first = ob.list;
+  }
+  return run_batch_kind(h, b, results, cigars, st, mx, first);
 }
 
 // The device-buffer batch on the fixed array of wfa_noalloc.cu: no cudaMalloc,
@@ -1421,6 +1478,14 @@ int wfa_batch_align(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* result
   long long* dtile = reinterpret_cast<long long*>(dtotal + 1);           // scan tile sums
   int64_t* hinfo = h->hinfo;                                            // [chunk][begin, end, retry, -]
   h->last_kernel_ms = 0.0;
+  // Cost ordering within each chunk (lean batches of short pairs).
+  const bool order = orders_batch(h, b);
+  OrderBufs ob{};
+  if (order) {
+    if (int e = order_bufs(h, n, nchunks, &ob)) return e;
+    if (cudaMemsetAsync(ob.hist, 0, (size_t)nchunks * kOrderStride * 4, sc) != cudaSuccess)
+      return fail(h, WFA_ERR_CUDA, "memset");
+  }
 
 #define PIPE_TRY(expr, what)                                                                      \
   do {                                                                                            \
@@ -1467,7 +1532,18 @@ int wfa_batch_align(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* result
     // timed here: the pipeline would wait on them).
     const int lanes = choose_lanes(h, P, I.max_len_sum, cn, sc, false);
     Round rd = first_round(P, metric_components(P.metric), I.max_len_sum, lanes);
-    int e2 = launch_round(h, P, rd, cn, nullptr, sc, dctr + 2 * ci);
+    const int64_t* clist = nullptr;
+    if (order && cn >= kSortMinPairs && length_bucket(I.max_len_sum) <= 2) {
+      int32_t* hst = ob.hist + kOrderStride * ci;
+      int32_t* dmx = hst + 2 * kOrderBins;  // the chunk's longest pair (known here already)
+      PIPE_TRY(launch_order_count(dseq, packed, dpo + a, dpl + a, dto + a, dtl + a, cn, h->num_sms, dmx,
+                                  ob.keys + a, hst, sc), "cost keys");
+      PIPE_TRY(launch_order_scatter(ob.keys + a, cn, hst, hst + kOrderBins, ob.list + a, h->num_sms, sc),
+               "cost order");
+      h->launches += 2;
+      clist = ob.list + a;
+    }
+    int e2 = launch_round(h, P, rd, cn, clist, sc, dctr + 2 * ci);
     if (e2 != WFA_OK) return e2;
     if (ci == 0) h->last_lanes = h->launch_lanes;
     PIPE_TRY(cudaEventRecord(ev_k[(size_t)ci], sc), "event");

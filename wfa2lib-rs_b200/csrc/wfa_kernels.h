@@ -83,6 +83,19 @@ inline BiLayout bi_layout(int scope, int nc, int wmax, int wmax_base, int hist_s
   return L;
 }
 
+// Cost ordering of a batch (wfa_order.cu): order_count computes each pair's
+// 4-mer profile distance key, the key histogram (kOrderBins bins, highest
+// key first) and the longest n + m; order_scatter writes the pair indices
+// in bin order into a list for the kernel's work queue.  hist and fill
+// (kOrderBins ints each) start zeroed.
+constexpr int kOrderBins = 1024;
+size_t order_count_smem();
+cudaError_t launch_order_count(const uint8_t* seq, int packed, const int64_t* p_off, const int32_t* p_len,
+                               const int64_t* t_off, const int32_t* t_len, int64_t n, int num_sms,
+                               int32_t* max_len_sum, uint16_t* keys, int32_t* hist, cudaStream_t st);
+cudaError_t launch_order_scatter(const uint16_t* keys, int64_t n, const int32_t* hist, int32_t* fill,
+                                 int64_t* list, int num_sms, cudaStream_t st);
+
 bool needs_general(const AlignParams& P);
 cudaError_t launch_biwfa(const AlignParams& P, int cls, int blocks, size_t smem, cudaStream_t st);
 // Lanes per pair: 8, 16 or 32 (groups of 32 / lanes pairs per warp).

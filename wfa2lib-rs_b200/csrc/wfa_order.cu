@@ -1,0 +1,157 @@
+// wfa_order.cu -- cost ordering of a batch for the lane-group kernel.
+//
+// The lane groups of a warp align their pairs side by side, and a warp is as
+// slow as its costliest pair, so pairs of similar cost should share warps.
+// The persistent kernel hands out pairs in list order, four consecutive
+// entries to the four groups of a warp, so the list is ordered by an
+// estimate of each pair's cost, highest first (which also starts the longest
+// work first).  The estimate is the 4-mer profile distance of the two
+// sequences, sum over the 256 4-mers x of |count_P(x) - count_T(x)|: every
+// edit changes at most eight 4-mer counts, and on the short-read batch the
+// distance follows the alignment score closely (correlation about 0.93).
+// The order only decides which pairs run together; results do not depend
+// on it.
+#include <cub/block/block_scan.cuh>
+
+#include <algorithm>
+
+#include "wfa_kernels.h"
+
+namespace wfab {
+
+constexpr int kCountBlock = 128;   // threads (pairs in flight) per counting block
+constexpr int kProfileBases = 4096;  // bases of each sequence the estimate reads
+
+// 2-bit code of base j of a sequence (packed: its code; ASCII: bits 1-2 of
+// the byte, enough to tell A, C, G and T apart for an estimate).
+struct CodeReader {
+  const uint8_t* seq;
+  bool packed;
+  int64_t off;
+  __device__ __forceinline__ uint32_t operator()(int j) const {
+    if (packed) {
+      const uint32_t w = reinterpret_cast<const uint32_t*>(seq)[off + (j >> 4)];
+      return (w >> (2 * (j & 15))) & 3u;
+    }
+    return ((uint32_t)seq[off + j] >> 1) & 3u;
+  }
+};
+
+// Per pair: the longest n + m of the batch (atomicMax into *max_len_sum),
+// the estimate key (keys[i], at most kOrderBins - 1) and the batch's key
+// histogram (bin kOrderBins - 1 - key, so that bins ascend as costs fall).
+__global__ void __launch_bounds__(kCountBlock) order_count(const uint8_t* seq, int packed,
+                                                            const int64_t* p_off, const int32_t* p_len,
+                                                            const int64_t* t_off, const int32_t* t_len,
+                                                            int64_t n, int32_t* max_len_sum,
+                                                            uint16_t* keys, int32_t* hist) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  int16_t* prof = reinterpret_cast<int16_t*>(smem);  // [256][kCountBlock]
+  int32_t* bins = reinterpret_cast<int32_t*>(smem + 256 * kCountBlock * 2);
+  const int tid = threadIdx.x;
+  for (int b = tid; b < kOrderBins; b += kCountBlock) bins[b] = 0;
+  for (int x = 0; x < 256; ++x) prof[x * kCountBlock + tid] = 0;
+  __syncthreads();
+  int32_t mx = 0;
+  for (int64_t i = (int64_t)blockIdx.x * kCountBlock + tid; i < n; i += (int64_t)gridDim.x * kCountBlock) {
+    const int32_t pn = p_len[i], tn = t_len[i];
+    mx = max(mx, pn + tn);
+    for (int s = 0; s < 2; ++s) {
+      const CodeReader rd{seq, packed != 0, s == 0 ? p_off[i] : t_off[i]};
+      const int len = min(s == 0 ? pn : tn, kProfileBases);
+      const int16_t d = s == 0 ? 1 : -1;
+      uint32_t km = 0;
+      for (int j = 0; j < len; ++j) {
+        km = ((km << 2) | rd(j)) & 0xFFu;
+        if (j >= 3) prof[km * kCountBlock + tid] += d;
+      }
+    }
+    int32_t l1 = 0;
+    for (int x = 0; x < 256; ++x) {
+      const int16_t v = prof[x * kCountBlock + tid];
+      l1 += v < 0 ? -v : v;
+      prof[x * kCountBlock + tid] = 0;
+    }
+    const int key = min(l1, kOrderBins - 1);
+    keys[i] = (uint16_t)key;
+    atomicAdd(&bins[kOrderBins - 1 - key], 1);
+  }
+  mx = __reduce_max_sync(0xffffffffu, mx);
+  if ((tid & 31) == 0) atomicMax(max_len_sum, mx);
+  __syncthreads();
+  for (int b = tid; b < kOrderBins; b += kCountBlock)
+    if (bins[b]) atomicAdd(&hist[b], bins[b]);
+}
+
+constexpr int kScatterBlock = 256, kScatterItems = 8;
+constexpr int kScatterTile = kScatterBlock * kScatterItems;
+
+// list[] = the pair indices 0..n-1 in ascending bin order (falling cost).
+// Each block scans the histogram, then places a tile of pairs at a time:
+// ranks within the tile from shared-memory counters, one global reservation
+// per (tile, bin) in fill[].
+__global__ void __launch_bounds__(kScatterBlock) order_scatter(const uint16_t* keys, int64_t n,
+                                                               const int32_t* hist, int32_t* fill,
+                                                               int64_t* list) {
+  using Scan = cub::BlockScan<int32_t, kScatterBlock>;
+  __shared__ typename Scan::TempStorage scan_tmp;
+  __shared__ int32_t start[kOrderBins];  // exclusive scan of hist
+  __shared__ int32_t tcount[kOrderBins];  // this tile's pairs per bin, then their base
+  constexpr int kPer = kOrderBins / kScatterBlock;
+  int32_t v[kPer];
+  for (int j = 0; j < kPer; ++j) v[j] = hist[threadIdx.x * kPer + j];
+  Scan(scan_tmp).ExclusiveSum(v, v);
+  for (int j = 0; j < kPer; ++j) start[threadIdx.x * kPer + j] = v[j];
+  for (int64_t t0 = (int64_t)blockIdx.x * kScatterTile; t0 < n; t0 += (int64_t)gridDim.x * kScatterTile) {
+    for (int b = threadIdx.x; b < kOrderBins; b += kScatterBlock) tcount[b] = 0;
+    __syncthreads();
+    int32_t bin[kScatterItems], rank[kScatterItems];
+    for (int k = 0; k < kScatterItems; ++k) {
+      const int64_t i = t0 + (int64_t)k * kScatterBlock + threadIdx.x;
+      bin[k] = i < n ? kOrderBins - 1 - keys[i] : -1;
+      rank[k] = bin[k] >= 0 ? atomicAdd(&tcount[bin[k]], 1) : 0;
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < kOrderBins; b += kScatterBlock)
+      if (tcount[b]) tcount[b] = start[b] + atomicAdd(&fill[b], tcount[b]);
+    __syncthreads();
+    for (int k = 0; k < kScatterItems; ++k) {
+      const int64_t i = t0 + (int64_t)k * kScatterBlock + threadIdx.x;
+      if (bin[k] >= 0) list[tcount[bin[k]] + rank[k]] = i;
+    }
+    __syncthreads();
+  }
+}
+
+static cudaError_t allow_count_smem() {
+  static bool done = false;
+  if (done) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(order_count, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)order_count_smem());
+  if (e == cudaSuccess) done = true;
+  return e;
+}
+
+size_t order_count_smem() { return (size_t)256 * kCountBlock * 2 + (size_t)kOrderBins * 4; }
+
+cudaError_t launch_order_count(const uint8_t* seq, int packed, const int64_t* p_off, const int32_t* p_len,
+                               const int64_t* t_off, const int32_t* t_len, int64_t n, int num_sms,
+                               int32_t* max_len_sum, uint16_t* keys, int32_t* hist, cudaStream_t st) {
+  cudaError_t e = allow_count_smem();
+  if (e != cudaSuccess) return e;
+  const int64_t want = (n + kCountBlock - 1) / kCountBlock;
+  const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)num_sms * 3));
+  order_count<<<blocks, kCountBlock, order_count_smem(), st>>>(seq, packed, p_off, p_len, t_off, t_len, n,
+                                                               max_len_sum, keys, hist);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_order_scatter(const uint16_t* keys, int64_t n, const int32_t* hist, int32_t* fill,
+                                 int64_t* list, int num_sms, cudaStream_t st) {
+  const int64_t tiles = (n + kScatterTile - 1) / kScatterTile;
+  const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)num_sms * 8));
+  order_scatter<<<blocks, kScatterBlock, 0, st>>>(keys, n, hist, fill, list);
+  return cudaGetLastError();
+}
+
+}  // namespace wfab
