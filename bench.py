@@ -371,6 +371,9 @@ def run_gpu(args):
         t1 = time.perf_counter()
         if i >= e2e_warm:
             e2e_ms.append((t1 - t0) * 1000)
+    e2e_kernel_ms = a.last_kernel_ms()
+    e2e_reruns = a.last_rerun_pairs()
+    e2e_lanes = a.last_lanes_per_pair()
     e2e_total = sum(e2e_ms)
     if world > 1:
         t = torch.tensor([e2e_total], device=dev)
@@ -402,7 +405,8 @@ def run_gpu(args):
             "gcups": world * cells * args.steps / (total_ms / 1000.0) / 1e9,
             "e2e": {"value": e2e_value, "unit": "pairs/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "api": "wfa_batch_align (pinned host buffers)",
-                    "steps": e2e_steps},
+                    "steps": e2e_steps, "kernel_ms": e2e_kernel_ms, "rerun_pairs": int(e2e_reruns),
+                    "lanes_per_pair": e2e_lanes},
             "plain": {"value": plain_value, "unit": "pairs/s", "pairs": plain_n,
                       "api": {0: "wfa_align_end2end", 1: "wfa_align_endsfree",
                               2: "wfa_align_biwfa"}[span] + ", one pair per call"},

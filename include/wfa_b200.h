@@ -348,7 +348,7 @@ WFA_API int64_t wfa_kernel_launches(const wfa_aligner_t* h);
 WFA_API int64_t wfa_last_rerun_pairs(const wfa_aligner_t* h);
 
 /* Lanes per pair of the unidirectional kernel for end-to-end alignments
- * without a heuristic: 8, 16 or 32 (a lane group of that width aligns one
+ * without a heuristic: 4, 8, 16 or 32 (a lane group of that width aligns one
  * pair; 32 / lanes pairs share a warp), or 0 (the default) for the
  * autotuned choice.  The first device batch of each kind (device, metric,
  * encoding, score-only or CIGAR, length bucket n + m <= 384 / 1024 / 2048)

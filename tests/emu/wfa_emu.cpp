@@ -52,7 +52,7 @@ static bool run_lane(const AlignParams& P, const Workspace& ws, int64_t i) {
 template <int CLS>
 static bool run_pair(const AlignParams& P, int64_t i) {
   constexpr int NC = CLS == kAffine2pClass ? 5 : CLS == kAffineClass ? 3 : 1;
-  std::vector<WfD> ring((size_t)P.scope * NC);
+  std::vector<WfD> ring((size_t)P.desc_depth * NC);
   std::vector<int32_t> ringv((size_t)P.ring_slots * P.wmax, 0x5A5A5A5A);
   std::vector<int32_t> ringg((size_t)P.ring_slots * P.wspill, 0x5A5A5A5A);
   std::vector<int4> hist((size_t)P.hist_scores, int4{0, -1, 0, 0});
@@ -113,6 +113,7 @@ extern "C" int64_t wfa_emu_batch(int metric, const int32_t* pen6, int compute_al
   P.hist_scores = hist_scores;
   P.hist_words = hist_words;
   P.ring_slots = compact_ring_slots(P, metric_class(metric));
+  P.desc_depth = compact_desc_depth(P, metric_class(metric));
   int32_t max_len_sum = 0;
   for (int64_t i = 0; i < num_pairs; ++i) max_len_sum = std::max(max_len_sum, p_len[i] + t_len[i]);
   const int nc = metric == WFA_METRIC_GAP_AFFINE_2P ? 5 : metric == WFA_METRIC_GAP_AFFINE ? 3 : 1;

@@ -328,7 +328,7 @@ def test_config2_sample_packed(pkg):
     assert np.array_equal(got, hashes)
 
 
-@pytest.mark.parametrize("lanes", [8, 16, 32])
+@pytest.mark.parametrize("lanes", [4, 8, 16, 32])
 @pytest.mark.parametrize("metric,pen", PENS)
 def test_lane_group_widths(pkg, metric, pen, lanes):
     """Every lane-group width of the end-to-end kernel, every metric, both
@@ -350,8 +350,8 @@ def test_lane_group_widths(pkg, metric, pen, lanes):
                 res, cig = a.align_batch(words, pwo, ps.p_len, two, ps.t_len, packed=True)
             else:
                 res, cig = a.align_batch(ps.buf, ps.p_off, ps.p_len, ps.t_off, ps.t_len)
-            # (a scope too large for narrow groups' rings runs wider groups)
-            assert a.last_lanes_per_pair() == lanes or (lanes < 32 and metric == 4 and pen[0] < 0)
+            # (rings too large for a block of narrow groups run wider groups)
+            assert a.last_lanes_per_pair() >= lanes
             a.close()
             assert np.array_equal(res["score"], scores), (compute, packed)
             assert np.array_equal(res["status"], status), (compute, packed)

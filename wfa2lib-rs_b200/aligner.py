@@ -273,7 +273,7 @@ class WavefrontAligner:
         return self._L.wfa_last_rerun_pairs(self._h)
 
     def set_lanes_per_pair(self, lanes):
-        """8, 16 or 32 lanes per pair for end-to-end alignments without a
+        """4, 8, 16 or 32 lanes per pair for end-to-end alignments without a
         heuristic, or 0 for the autotuned choice (the default)."""
         return self._check(self._L.wfa_set_lanes_per_pair(self._h, lanes))
 

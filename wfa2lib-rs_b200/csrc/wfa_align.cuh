@@ -119,15 +119,15 @@ struct Warp {
 #endif
 };
 
-// A group of LW lanes that aligns one pair: LW = 32 is the whole warp; 8 or
-// 16 put 4 or 2 pairs in a warp (short pairs, whose wavefronts are a few
-// diagonals wide).  The groups of a warp run the same code on different
+// A group of LW lanes that aligns one pair: LW = 32 is the whole warp; 4, 8
+// or 16 put 8, 4 or 2 pairs in a warp (short pairs, whose wavefronts are a
+// few diagonals wide).  The groups of a warp run the same code on different
 // pairs; every collective names only the group's own lanes.  In the
 // emulation builds the emulated warp is the group.
 #if defined(WFA_CUDA_WARP)
 template <int LW>
 struct Lanes {
-  static_assert(LW == 8 || LW == 16 || LW == 32, "lane group width");
+  static_assert(LW == 4 || LW == 8 || LW == 16 || LW == 32, "lane group width");
   static WFA_D unsigned mask() {
     return LW == 32 ? 0xffffffffu : ((1u << LW) - 1u) << ((threadIdx.x & 31) & ~(LW - 1));
   }
@@ -356,15 +356,23 @@ struct PairAligner {
   WFA_D bool ef() const { return GEN && endsfree; }
 
   // ---- slots --------------------------------------------------------------
-  // Ring index of score t (cscore - scope < t <= cscore), kept without a
-  // division: cidx == cscore % scope is advanced with the score loop.
+  // Descriptor ring index of score t (cscore - scope < t <= cscore), kept
+  // without a division: cidx == (cscore >> gshift) % dscope is advanced with
+  // the score loop.  With the compact layout and a power-of-two score step
+  // (gshift > 0) only scores that are multiples of it have slots, and t must
+  // be one of them; otherwise every score has one (dscope == scope).
+  int32_t gshift = 0, dscope = 0;
   WFA_D int sidx(int t) const {
-    int i = cidx - (cscore - t);
-    return i < 0 ? i + scope : i;
+    int i = cidx - ((cscore - t) >> gshift);
+    i = i < 0 ? i + dscope : i;
+#if !(defined(__CUDACC__) && !defined(WFA_EMU))
+    if (i < 0 || i >= dscope || ((cscore - t) & ((1 << gshift) - 1))) std::abort();  // emulation-only check
+#endif
+    return i;
   }
   WFA_D void advance() {
     ++cscore;
-    cidx = cidx + 1 == scope ? 0 : cidx + 1;
+    if ((cscore & ((1 << gshift) - 1)) == 0) cidx = cidx + 1 == dscope ? 0 : cidx + 1;
   }
   WFA_D WfD& slot(int c, int s) { return ws.ring[sidx(s) * NC + c]; }
   // Slot (c, s) holds a live wavefront: present and not null (flags are
@@ -403,6 +411,9 @@ struct PairAligner {
     } else {
       idx = (int64_t)sidx(s) * NC + c;
     }
+#if !(defined(__CUDACC__) && !defined(WFA_EMU))
+    if (compact && idx >= P.ring_slots) std::abort();  // emulation-only check
+#endif
     if (w <= wmax) return ws.ringv + idx * wmax;
     if (compact && ws.ringg && w <= P.wspill) return ws.ringg + idx * P.wspill;
     retry = true;
@@ -584,11 +595,16 @@ struct PairAligner {
     cidx = 0;
     gstep = score_step_gcd();
     gphase = 0;
+    gshift = 0;
+    dscope = scope;
     if (compact) {
       compact_depths();
+      gshift = score_shift(gstep);
+      dscope = ((scope - 1) >> gshift) + 1;
+      if (P.desc_depth && dscope > P.desc_depth) retry = true;
       if (retry) return;
     }
-    for (int i = lane; i < scope * NC; i += LW) ws.ring[i] = wf_none();
+    for (int i = lane; i < dscope * NC; i += LW) ws.ring[i] = wf_none();
     G::sync();
     hist_lo = -(n + scope + 2);
     hist_hi = m + scope + 2;
@@ -1370,6 +1386,8 @@ struct PairAligner {
     cidx = 0;
     gstep = score_step_gcd();
     gphase = 0;
+    gshift = 0;
+    dscope = scope;
     for (int i = lane; i < scope * NC; i += LW) ws.ring[i] = wf_none();
     G::sync();
     hist_lo = -(n + scope + 2);

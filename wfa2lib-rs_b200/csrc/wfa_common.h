@@ -59,6 +59,10 @@ struct AlignParams {
   // that takes rows wider than wmax (0: none).
   int32_t ring_slots;
   int32_t wspill;
+  // Depth (scores) of the descriptor ring of the unidirectional aligner: the
+  // scope, or with the compact layout and a power-of-two score step the
+  // scores of the scope that can hold a wavefront (0: the scope).
+  int32_t desc_depth;
   int32_t wmax_base;   // BiWFA base-case ring slot width (cells)
   int32_t ring_smem;   // 1: ring cells in shared memory (else in the scratch slice)
   int32_t seq_smem_words;  // per sequence staged in shared memory (0: none)
@@ -86,7 +90,7 @@ inline int score_gcd(int a, int b) {
 #if defined(__CUDACC__)
 __host__ __device__
 #endif
-inline int compact_ring_slots(const AlignParams& P, int cls) {
+inline int score_step(const AlignParams& P, int cls) {
   int g;
   if (cls == kEditClass) g = 1;
   else if (cls == kLinearClass) g = score_gcd(P.mismatch, P.o1);
@@ -95,7 +99,29 @@ inline int compact_ring_slots(const AlignParams& P, int cls) {
   const bool ef = P.span == WFA_SPAN_ENDSFREE;
   const int p0 = P.extension ? 0 : P.p0, t0 = P.extension ? 0 : P.t0;
   if (ef && P.match != 0 && (p0 > 0 || t0 > 0)) g = score_gcd(g, -P.match);
-  if (g < 1) g = 1;
+  return g < 1 ? 1 : g;
+}
+// log2 of a power-of-two score step, else 0 (the descriptor ring then keeps
+// one slot per score).
+#if defined(__CUDACC__)
+__host__ __device__
+#endif
+inline int score_shift(int g) {
+  int k = 0;
+  while ((1 << k) < g) ++k;
+  return (1 << k) == g ? k : 0;
+}
+#if defined(__CUDACC__)
+__host__ __device__
+#endif
+inline int compact_desc_depth(const AlignParams& P, int cls) {
+  return ((P.scope - 1) >> score_shift(score_step(P, cls))) + 1;
+}
+#if defined(__CUDACC__)
+__host__ __device__
+#endif
+inline int compact_ring_slots(const AlignParams& P, int cls) {
+  const int g = score_step(P, cls);
   int slots = (P.scope - 1) / g + 1;
   if (cls >= kAffineClass) slots += 2 * (P.e1 / g + 1);
   if (cls == kAffine2pClass) slots += 2 * (P.e2 / g + 1);

@@ -1,20 +1,22 @@
 // wfa_kernels.cu -- dispatch of the unidirectional kernel to its
-// instantiations (wfa_kernels_lean8/16/32.cu, wfa_kernels_gen.cu).
+// instantiations (wfa_kernels_lean4/8/16/32.cu, wfa_kernels_gen.cu).
 #include "wfa_kernels.h"
 
 namespace wfab {
 
+cudaError_t lean_w4_launch(const AlignParams& P, int cls, int blocks, size_t smem, cudaStream_t st);
 cudaError_t lean_w8_launch(const AlignParams& P, int cls, int blocks, size_t smem, cudaStream_t st);
 cudaError_t lean_w16_launch(const AlignParams& P, int cls, int blocks, size_t smem, cudaStream_t st);
 cudaError_t lean_w32_launch(const AlignParams& P, int cls, int blocks, size_t smem, cudaStream_t st);
 cudaError_t general_launch(const AlignParams& P, int cls, int blocks, size_t smem, cudaStream_t st);
+int lean_w4_occupancy(const AlignParams& P, int cls, size_t smem);
 int lean_w8_occupancy(const AlignParams& P, int cls, size_t smem);
 int lean_w16_occupancy(const AlignParams& P, int cls, size_t smem);
 int lean_w32_occupancy(const AlignParams& P, int cls, size_t smem);
 int general_occupancy(const AlignParams& P, int cls, size_t smem);
 
 // The lean instantiation runs end-to-end high-memory (or score-only)
-// alignments without a heuristic, with 8, 16 or 32 lanes per pair;
+// alignments without a heuristic, with 4, 8, 16 or 32 lanes per pair;
 // everything else (ends-free, heuristics, the med/low piggyback backtrace)
 // runs the general one on whole warps.
 bool needs_general(const AlignParams& P) {
@@ -24,6 +26,7 @@ bool needs_general(const AlignParams& P) {
 cudaError_t launch_unialign(const AlignParams& P, int metric_class, int lanes, int blocks, size_t smem,
                             cudaStream_t st) {
   if (needs_general(P)) return general_launch(P, metric_class, blocks, smem, st);
+  if (lanes == 4) return lean_w4_launch(P, metric_class, blocks, smem, st);
   if (lanes == 8) return lean_w8_launch(P, metric_class, blocks, smem, st);
   if (lanes == 16) return lean_w16_launch(P, metric_class, blocks, smem, st);
   return lean_w32_launch(P, metric_class, blocks, smem, st);
@@ -31,6 +34,7 @@ cudaError_t launch_unialign(const AlignParams& P, int metric_class, int lanes, i
 
 int occupancy_blocks_per_sm(const AlignParams& P, int metric_class, int lanes, size_t smem) {
   if (needs_general(P)) return general_occupancy(P, metric_class, smem);
+  if (lanes == 4) return lean_w4_occupancy(P, metric_class, smem);
   if (lanes == 8) return lean_w8_occupancy(P, metric_class, smem);
   if (lanes == 16) return lean_w16_occupancy(P, metric_class, smem);
   return lean_w32_occupancy(P, metric_class, smem);

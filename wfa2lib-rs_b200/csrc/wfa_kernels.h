@@ -20,10 +20,10 @@ struct SmemLayout {
 #if defined(__CUDACC__)
 __host__ __device__
 #endif
-inline SmemLayout smem_layout(int scope, int nc, int cell_slots, int ring_wmax, int seq_words,
+inline SmemLayout smem_layout(int desc_depth, int nc, int cell_slots, int ring_wmax, int seq_words,
                               int groups) {
   SmemLayout L;
-  L.desc_bytes = (size_t)scope * nc * kDescBytes;
+  L.desc_bytes = (size_t)desc_depth * nc * kDescBytes;
   L.seq_bytes = (size_t)2 * seq_words * 4;
   L.ring_bytes = (size_t)cell_slots * ring_wmax * 4;
   L.desc_off = 0;
@@ -98,7 +98,7 @@ cudaError_t launch_order_scatter(const uint16_t* keys, int64_t n, const int32_t*
 
 bool needs_general(const AlignParams& P);
 cudaError_t launch_biwfa(const AlignParams& P, int cls, int blocks, size_t smem, cudaStream_t st);
-// Lanes per pair: 8, 16 or 32 (groups of 32 / lanes pairs per warp).
+// Lanes per pair: 4, 8, 16 or 32 (32 / lanes pairs per warp).
 cudaError_t launch_unialign(const AlignParams& P, int metric_class, int lanes, int blocks, size_t smem,
                             cudaStream_t st);
 int occupancy_blocks_per_sm(const AlignParams& P, int metric_class, int lanes, size_t smem);

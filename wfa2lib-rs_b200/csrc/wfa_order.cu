@@ -21,56 +21,68 @@ namespace wfab {
 
 constexpr int kCountBlock = 128;   // threads (pairs in flight) per counting block
 constexpr int kProfileBases = 4096;  // bases of each sequence the estimate reads
-
-// 2-bit code of base j of a sequence (packed: its code; ASCII: bits 1-2 of
-// the byte, enough to tell A, C, G and T apart for an estimate).
-struct CodeReader {
-  const uint8_t* seq;
-  bool packed;
-  int64_t off;
-  __device__ __forceinline__ uint32_t operator()(int j) const {
-    if (packed) {
-      const uint32_t w = reinterpret_cast<const uint32_t*>(seq)[off + (j >> 4)];
-      return (w >> (2 * (j & 15))) & 3u;
-    }
-    return ((uint32_t)seq[off + j] >> 1) & 3u;
-  }
-};
+// (2-bit codes: packed input as stored; ASCII bytes by their bits 1-2, which
+// tell A, C, G and T apart -- enough for an estimate.)
 
 // Per pair: the longest n + m of the batch (atomicMax into *max_len_sum),
 // the estimate key (keys[i], at most kOrderBins - 1) and the batch's key
 // histogram (bin kOrderBins - 1 - key, so that bins ascend as costs fall).
+// Each thread profiles its own pairs in a column of shared memory: two
+// 16-bit counters per word, biased by kBias so that the at most
+// kProfileBases increments or decrements of a counter never carry into its
+// neighbour, updated with atomic adds whose results are not used (no update
+// waits for the previous one).
+constexpr uint32_t kBias = 0x4000;
 __global__ void __launch_bounds__(kCountBlock) order_count(const uint8_t* seq, int packed,
                                                             const int64_t* p_off, const int32_t* p_len,
                                                             const int64_t* t_off, const int32_t* t_len,
                                                             int64_t n, int32_t* max_len_sum,
                                                             uint16_t* keys, int32_t* hist) {
   extern __shared__ __align__(16) uint8_t smem[];
-  int16_t* prof = reinterpret_cast<int16_t*>(smem);  // [256][kCountBlock]
-  int32_t* bins = reinterpret_cast<int32_t*>(smem + 256 * kCountBlock * 2);
+  uint32_t* prof = reinterpret_cast<uint32_t*>(smem);  // [128 word][kCountBlock]: 4-mers 2w, 2w+1
+  int32_t* bins = reinterpret_cast<int32_t*>(smem + 128 * kCountBlock * 4);
   const int tid = threadIdx.x;
+  constexpr uint32_t kBiased = kBias | (kBias << 16);
   for (int b = tid; b < kOrderBins; b += kCountBlock) bins[b] = 0;
-  for (int x = 0; x < 256; ++x) prof[x * kCountBlock + tid] = 0;
+  for (int x = 0; x < 128; ++x) prof[x * kCountBlock + tid] = kBiased;
   __syncthreads();
   int32_t mx = 0;
   for (int64_t i = (int64_t)blockIdx.x * kCountBlock + tid; i < n; i += (int64_t)gridDim.x * kCountBlock) {
     const int32_t pn = p_len[i], tn = t_len[i];
     mx = max(mx, pn + tn);
     for (int s = 0; s < 2; ++s) {
-      const CodeReader rd{seq, packed != 0, s == 0 ? p_off[i] : t_off[i]};
+      const int64_t off = s == 0 ? p_off[i] : t_off[i];
       const int len = min(s == 0 ? pn : tn, kProfileBases);
-      const int16_t d = s == 0 ? 1 : -1;
+      // +1 or -1 on the low or the high half (as 32-bit adds: neither half
+      // ever wraps, so -1 never borrows from the other half)
+      const uint32_t dlo = s == 0 ? 1u : 0xFFFFFFFFu, dhi = s == 0 ? 1u << 16 : 0xFFFF0000u;
       uint32_t km = 0;
-      for (int j = 0; j < len; ++j) {
-        km = ((km << 2) | rd(j)) & 0xFFu;
-        if (j >= 3) prof[km * kCountBlock + tid] += d;
+      // Bases in chunks of 16: one 32-bit load of 2-bit codes (packed) or
+      // 16 byte loads (ASCII), then the chunk's 4-mers from registers.
+      for (int j0 = 0; j0 < len; j0 += 16) {
+        uint32_t codes = 0;
+        if (packed) {
+          codes = reinterpret_cast<const uint32_t*>(seq)[off + (j0 >> 4)];
+        } else {
+          const int lim = min(16, len - j0);
+          for (int b = 0; b < lim; ++b) codes |= (((uint32_t)seq[off + j0 + b] >> 1) & 3u) << (2 * b);
+        }
+        const int lim = min(16, len - j0);
+#pragma unroll
+        for (int b = 0; b < 16; ++b) {
+          if (b < lim) {
+            km = ((km << 2) | ((codes >> (2 * b)) & 3u)) & 0xFFu;
+            if (j0 + b >= 3) atomicAdd(&prof[(km >> 1) * kCountBlock + tid], (km & 1) ? dhi : dlo);
+          }
+        }
       }
     }
     int32_t l1 = 0;
-    for (int x = 0; x < 256; ++x) {
-      const int16_t v = prof[x * kCountBlock + tid];
-      l1 += v < 0 ? -v : v;
-      prof[x * kCountBlock + tid] = 0;
+    for (int x = 0; x < 128; ++x) {
+      const uint32_t w = prof[x * kCountBlock + tid];
+      const int32_t lo = (int32_t)(w & 0xFFFFu) - (int32_t)kBias, hi = (int32_t)(w >> 16) - (int32_t)kBias;
+      l1 += (lo < 0 ? -lo : lo) + (hi < 0 ? -hi : hi);
+      prof[x * kCountBlock + tid] = kBiased;
     }
     const int key = min(l1, kOrderBins - 1);
     keys[i] = (uint16_t)key;
@@ -132,7 +144,7 @@ static cudaError_t allow_count_smem() {
   return e;
 }
 
-size_t order_count_smem() { return (size_t)256 * kCountBlock * 2 + (size_t)kOrderBins * 4; }
+size_t order_count_smem() { return (size_t)128 * kCountBlock * 4 + (size_t)kOrderBins * 4; }
 
 cudaError_t launch_order_count(const uint8_t* seq, int packed, const int64_t* p_off, const int32_t* p_len,
                                const int64_t* t_off, const int32_t* t_len, int64_t n, int num_sms,

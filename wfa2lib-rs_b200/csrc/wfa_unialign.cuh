@@ -92,7 +92,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (min_blocks<CLS, GEN>()))
   const int64_t ggroup = (int64_t)blockIdx.x * kGroups + gib;
   constexpr int NC = CLS == kAffine2pClass ? 5 : CLS == kAffineClass ? 3 : 1;
   const int slots = cell_slots(P, NC);
-  const SmemLayout L = smem_layout(P.scope, NC, slots, P.ring_smem ? P.wmax : 0, P.seq_smem_words, kGroups);
+  const SmemLayout L = smem_layout(P.desc_depth ? P.desc_depth : P.scope, NC, slots, P.ring_smem ? P.wmax : 0,
+                                   P.seq_smem_words, kGroups);
   Workspace ws;
   ws.ring = reinterpret_cast<WfD*>(smem + L.desc_off + (size_t)gib * L.desc_bytes);
   uint32_t* sseq = reinterpret_cast<uint32_t*>(smem + L.seq_off + (size_t)gib * L.seq_bytes);
