@@ -359,6 +359,11 @@ WFA_API int64_t wfa_last_rerun_pairs(const wfa_aligner_t* h);
 WFA_API int wfa_set_lanes_per_pair(wfa_aligner_t* h, int32_t lanes);
 /* Lanes per pair the handle's last batch ran with (first round). */
 WFA_API int32_t wfa_last_lanes_per_pair(const wfa_aligner_t* h);
+/* Device memory (bytes) one pair in flight used in the handle's last
+ * unidirectional launch: its lane group's scratch slice (ring cells beyond
+ * shared memory, the high-memory M history or the med/low backtrace
+ * buffer).  No counterpart in the reference. */
+WFA_API int64_t wfa_last_slice_bytes(const wfa_aligner_t* h);
 /* The autotuner's choices so far, one line per kind with the candidates'
  * sample times, into out (NUL-terminated, at most cap bytes); returns the
  * full length. */

@@ -35,6 +35,7 @@ def lib(fast=False):
     L.wfo_set_alignment_scope.argtypes = [vp, ctypes.c_int]
     L.wfo_set_memory_mode.argtypes = [vp, ctypes.c_int]
     L.wfo_set_compat.argtypes = [vp, ctypes.c_int]
+    L.wfo_set_piggyback_literal.argtypes = [vp, ctypes.c_int]
     L.wfo_set_heuristic.argtypes = [vp, ctypes.c_int, i32, i32, i32]
     L.wfo_set_max_alignment_steps.argtypes = [vp, i32]
     L.wfo_set_alignment_free_ends.argtypes = [vp, i32, i32, i32, i32]
@@ -88,6 +89,11 @@ class OracleAligner:
 
     def set_memory_mode(self, mode):
         self.L.wfo_set_memory_mode(self.h, {"high": 0, "med": 1, "low": 2}.get(mode, mode))
+
+    def set_piggyback_literal(self, on):
+        """Med/low: the reference's per-cell packed-CIGAR path (True, the
+        default) or the picks re-made from the kept offsets (False)."""
+        self.L.wfo_set_piggyback_literal(self.h, int(bool(on)))
 
     def set_compat(self, compat):
         """'c' (reproduce C's known bugs, the default) or 'corrected'."""

@@ -321,6 +321,36 @@ struct Wavefront {
   // reference keeps it) and the begin-free seeds placed in this wavefront.
   int32_t wr_lo = 1, wr_hi = 0;
   std::vector<int32_t> seeds;
+  // The piggyback kernels' per-cell backtrace (src/wavefront.rs:64-77,
+  // 529-580): the packed CIGAR (up to 16 operations, src/pcigar.rs) and the
+  // index of the backtrace-buffer block it continues; and the occupancy the
+  // offload tracks (bt_occupancy_max).  Sized with the offsets when an
+  // aligner runs the literal piggyback path, else empty.
+  std::vector<uint32_t> pc, pvb;
+  int32_t occ = 0;
+  bool has_bt() const { return !pc.empty(); }
+  void ensure_bt() {  // fresh arrays are zeroed (alloc_zeroed, :283-301)
+    if (pc.size() != mem.size()) { pc.assign(mem.size(), 0); pvb.assign(mem.size(), 0); }
+  }
+  uint32_t get_pc(int32_t k) const { WFO_ASSERT(allocated(k)); return pc[(size_t)(k - base_k)]; }
+  uint32_t get_pv(int32_t k) const { WFO_ASSERT(allocated(k)); return pvb[(size_t)(k - base_k)]; }
+  void set_bt(int32_t k, uint32_t c, uint32_t v) {
+    WFO_ASSERT(allocated(k));
+    pc[(size_t)(k - base_k)] = c;
+    pvb[(size_t)(k - base_k)] = v;
+  }
+  // zero_bt, :570-580: zeroed backtraces count as written.
+  void zero_bt(int32_t k, int32_t count) {
+    if (!has_bt() || count <= 0) return;
+    mark_written(k, k + count - 1);
+    for (int32_t i = 0; i < count; ++i) set_bt(k + i, 0, 0);
+  }
+  // bt_or_zero, :410-416
+  void bt_or_zero(int32_t k, uint32_t& c, uint32_t& v) const {
+    if (!written(k)) { c = 0; v = 0; return; }
+    c = get_pc(k);
+    v = get_pv(k);
+  }
   void mark_written(int32_t l, int32_t h) {
     if (l > h) return;
     if (wr_lo > wr_hi) { wr_lo = l; wr_hi = h; }
@@ -350,14 +380,17 @@ struct Wavefront {
 #else
     mem.resize((size_t)n);
 #endif
+    if (has_bt()) { pc.assign((size_t)n, 0); pvb.assign((size_t)n, 0); }
   }
   void init(int32_t min_lo, int32_t /*max_hi*/) {  // :307
     null = false; lo = 1; hi = -1; base_k = min_lo; init_min = 0; init_max = 0;
-    wr_lo = 1; wr_hi = 0; seeds.clear();
+    wr_lo = 1; wr_hi = 0; seeds.clear(); occ = 0;
   }
   void init_null(int32_t min_lo, int32_t max_hi) {  // :331
-    null = true; lo = 1; hi = -1; base_k = min_lo; wr_lo = 1; wr_hi = 0; seeds.clear();
+    null = true; lo = 1; hi = -1; base_k = min_lo; wr_lo = 1; wr_hi = 0; seeds.clear(); occ = 0;
     for (int32_t i = 0; i < max_hi - min_lo + 1; ++i) mem[(size_t)i] = OFFSET_NULL;
+    if (has_bt())
+      for (int32_t i = 0; i < max_hi - min_lo + 1; ++i) { pc[(size_t)i] = 0; pvb[(size_t)i] = 0; }
     init_min = min_lo; init_max = max_hi;
   }
   void init_victim(int32_t min_lo, int32_t max_hi) { init(min_lo, max_hi); null = true; }
@@ -366,19 +399,21 @@ struct Wavefront {
     mark_written(l, h);
   }
   void clear_init_range() { init_min = lo; init_max = hi; }  // :375
-  void set_null_cell_if_allocated(int32_t k) { if (allocated(k)) set(k, OFFSET_NULL); }  // :405
+  void set_null_cell_if_allocated(int32_t k) {  // :395-405
+    if (allocated(k)) { set(k, OFFSET_NULL); zero_bt(k, 1); }
+  }
   void init_ends_lower(int32_t min_lo) {  // :422
     if (init_min <= min_lo) return;
     int32_t min_init = std::min(init_min, lo);
     int32_t start = std::max(min_lo, base_k);
-    if (start < min_init) fill_null(start, min_init - start);
+    if (start < min_init) { fill_null(start, min_init - start); zero_bt(start, min_init - start); }
     init_min = start;
   }
   void init_ends_higher(int32_t max_hi) {  // :443
     if (init_max >= max_hi) return;
     int32_t max_init = std::max(init_max, hi);
     int32_t end = std::min(max_hi, base_k + alloc - 1);
-    if (end > max_init) fill_null(max_init + 1, end - max_init);
+    if (end > max_init) { fill_null(max_init + 1, end - max_init); zero_bt(max_init + 1, end - max_init); }
     init_max = end;
   }
 };
@@ -568,6 +603,51 @@ static bool heuristic_cutoff(const Heuristic& hs, HeurState& st, Wavefront& wf,
 // ---------------------------------------------------------------------------
 // Components: src/components.rs (flat or modular per-score arrays)
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// The piggyback backtrace of med/low memory, as the reference runs it:
+// packed CIGARs (src/pcigar.rs:13-199) and the backtrace buffer
+// (src/bt_buffer.rs:34-327).  Block indices are plain vector positions (the
+// reference's segments are storage detail), and the buffer is never
+// compacted here: compaction (:238-327) renumbers blocks without changing
+// any chain's content, so results do not depend on it.
+// ---------------------------------------------------------------------------
+constexpr uint32_t PCIGAR_DELETION = 1, PCIGAR_MISMATCH = 2, PCIGAR_INSERTION = 3;
+constexpr uint32_t PCIGAR_FULL_MASK = 0x40000000u, PCIGAR_ALMOST_FULL_MASK = 0x10000000u,
+                   PCIGAR_HALF_FULL_MASK = 0x00010000u;
+constexpr int32_t PCIGAR_MAX_LENGTH = 16;
+constexpr uint32_t BT_BLOCK_IDX_NULL = 0xFFFFFFFFu;
+static inline uint32_t pcigar_push(uint32_t pc, uint32_t op) { return (pc << 2) | op; }
+static inline int32_t pcigar_free_slots(uint32_t pc) {  // :77-84
+  return pc ? __builtin_clz(pc) / 2 : PCIGAR_MAX_LENGTH;
+}
+
+struct BtBuffer {
+  std::vector<std::pair<uint32_t, uint32_t>> blocks;  // {pcigar, prev}
+  std::vector<std::pair<int32_t, int32_t>> init_pos;  // {v, h}
+  std::vector<uint32_t> packed;                       // traceback: end first
+  void clear() { blocks.clear(); init_pos.clear(); }
+  uint32_t store_block(uint32_t pc, uint32_t prev) {  // :112-131
+    blocks.emplace_back(pc, prev);
+    return (uint32_t)blocks.size() - 1;
+  }
+  uint32_t init_block(int32_t v, int32_t h) {  // :134-139
+    init_pos.emplace_back(v, h);
+    return store_block((uint32_t)init_pos.size() - 1, BT_BLOCK_IDX_NULL);
+  }
+  // traceback_from, :196-212: the pcigars back to the initial block (end
+  // first); returns the initial block's pcigar (an index of init_pos).
+  uint32_t traceback_from(uint32_t pc, uint32_t prev) {
+    packed.clear();
+    while (prev != BT_BLOCK_IDX_NULL) {
+      packed.push_back(pc);
+      const auto& b = blocks[prev];
+      pc = b.first;
+      prev = b.second;
+    }
+    return pc;
+  }
+};
+
 struct Components {
   bool modular = false;
   size_t num_wavefronts = 0, scope = 0;
@@ -783,6 +863,14 @@ class Aligner {
   HeurState hstate;
   int memory_mode = 0;
   bool piggyback = false;  // med/low memory with an alignment (the piggyback backtrace)
+  // Med/low run either as the reference does (bt_literal: every cell carries
+  // its packed CIGAR and block index, offloaded to `bt`) or by re-making the
+  // kernels' picks from the kept offsets after the end cell is found
+  // (backtrace_piggyback_rederived); both give the same CIGARs.
+  bool bt_literal = true;
+  BtBuffer bt;
+  uint32_t zdrop_bt_pc = 0, zdrop_bt_pv = BT_BLOCK_IDX_NULL;  // zdrop_best_bt, :186
+  bool lit() const { return piggyback && bt_literal; }
   // Compat (src/aligner.rs:53-94): 0 C (reproduce C's known bugs), 1 Corrected.
   int compat = 0;
   // Corrected-mode ends-free end candidate (EndsfreeCandidate, :96-107): the
@@ -791,6 +879,7 @@ class Aligner {
     bool has = false;
     int32_t total = 0;
     Pos pos;
+    uint32_t bt_pc = 0, bt_pv = BT_BLOCK_IDX_NULL;  // its cell's backtrace (med/low)
   };
   Candidate best;
   // Corrected-mode begin-free dominance pruning (:172-186): per component,
@@ -818,6 +907,7 @@ class Aligner {
       w = pool.back().get();
       w->reallocate(len);
     }
+    if (lit()) w->ensure_bt();
     w->init(lo, hi);
     return w;
   }
@@ -873,10 +963,14 @@ class Aligner {
 
   // The seed's backtrace starts at (v, h) = (offset - k, offset) (set_bt_init,
   // src/aligner.rs:213-225, and :3425-3434).
-  void endsfree_init_offset(Wavefront& wf, int32_t k, int32_t /*v*/, int32_t h) {
+  void endsfree_init_offset(Wavefront& wf, int32_t k, int32_t v, int32_t h) {
     wf.set(k, h);
     if (piggyback) { wf.seeds.push_back(k); wf.mark_written(k, k); }
+    if (lit()) set_bt_init(wf, k, v, h);
   }
+  // set_bt_init, src/aligner.rs:213-225: an empty pcigar continuing a new
+  // initial block at (v, h).
+  void set_bt_init(Wavefront& wf, int32_t k, int32_t v, int32_t h) { wf.set_bt(k, 0, bt.init_block(v, h)); }
 
   // endsfree_init, src/aligner.rs:3426-3452
   void endsfree_init(Wavefront& wf, int32_t k) {
@@ -972,12 +1066,25 @@ class Aligner {
     if (pen.match_ == 0 && span == SPAN_ENDSFREE) { lo0 = -p0; hi0 = t0; }
     int32_t alo, ahi;
     output_alloc_range(0, lo0, hi0, alo, ahi);
+    if (lit()) {
+      bt.clear();
+      comps.null_wf.ensure_bt();
+      zdrop_bt_pc = 0;
+      zdrop_bt_pv = BT_BLOCK_IDX_NULL;
+    }
     Wavefront* wf = allocate(alo, ahi);
     wf->set(0, 0);
     wf->set_limits(0, 0);
+    if (lit()) set_bt_init(*wf, 0, 0, 0);
     if (span == SPAN_ENDSFREE && pen.match_ == 0) {
-      for (int32_t h = 1; h <= t0; ++h) wf->set(h, h);
-      for (int32_t v = 1; v <= p0; ++v) wf->set(-v, 0);
+      for (int32_t h = 1; h <= t0; ++h) {
+        wf->set(h, h);
+        if (lit()) set_bt_init(*wf, h, 0, h);
+      }
+      for (int32_t v = 1; v <= p0; ++v) {
+        wf->set(-v, 0);
+        if (lit()) set_bt_init(*wf, -v, v, 0);
+      }
       wf->lo = -p0; wf->hi = t0; wf->init_min = -p0; wf->init_max = t0;
       if (piggyback) wf->mark_written(-p0, t0);
     }
@@ -1073,7 +1180,12 @@ class Aligner {
     size_t need = (size_t)(comps.alloc_hi + 2 - sbase + 1);
     if (scratch.size() < need) scratch.assign(need, 0);
     int32_t lo_base = m->lo, hi_base = m->hi;
+    const int32_t max_wf_score_base = hstate.max_wf_score;
     bool z = heuristic_cutoff(heur, hstate, *m, scratch, sbase, plen(), tlen(), drop, score);
+    // Corrected med/low keep the backtrace of a new Z-drop best cell, which
+    // the end backtrace needs after its wavefront is gone (:1677-1688).
+    if (compat == 1 && lit() && hstate.max_wf_score == score && max_wf_score_base != score)
+      m->bt_or_zero(hstate.max_sw_score_k, zdrop_bt_pc, zdrop_bt_pv);
     if (z) {
       end_pos = Pos{hstate.max_wf_score, hstate.max_sw_score_k, hstate.max_sw_score_offset};
       return true;
@@ -1236,6 +1348,7 @@ class Aligner {
           best.has = true;
           best.total = total;
           best.pos = Pos{score, k, off};
+          if (lit()) m->bt_or_zero(k, best.bt_pc, best.bt_pv);  // :1155-1160
           if (prune && total > score) endsfree_prune(score, total);
         }
       }
@@ -1255,6 +1368,110 @@ class Aligner {
       return true;
     }
     return false;
+  }
+
+  // --- the piggyback kernels' per-cell backtraces, src/compute/piggyback.rs --
+  // Every cell copies (pcigar, prev) from the input its kernel picked and
+  // pushes the operation: edit/linear cells pick misms over del over ins
+  // (later checks win ties, :197-228), indel del over ins (:249-273); a gap
+  // cell picks its extension over the M opening on a tie (`gap`, :146-170)
+  // and affine M picks misms, else D2, D1, I2, I1, pushing an X (the gap
+  // close) on the chosen chain (:364-392, 483-527).
+  void bt_edit_cells(const Wavefront& wi, const Wavefront& wx, const Wavefront& wd, Wavefront& out,
+                     int32_t lo, int32_t hi, bool indel) {
+    for (int32_t k = lo; k <= hi; ++k) {
+      const int32_t ins = wrap_add(wi.get(k - 1), 1), del = wd.get(k + 1);
+      uint32_t pc, pv;
+      if (indel) {
+        const bool d = std::max(del, ins) == del;
+        pc = d ? pcigar_push(wd.get_pc(k + 1), PCIGAR_DELETION) : pcigar_push(wi.get_pc(k - 1), PCIGAR_INSERTION);
+        pv = d ? wd.get_pv(k + 1) : wi.get_pv(k - 1);
+      } else {
+        const int32_t misms = wrap_add(wx.get(k), 1);
+        const int32_t mx = std::max(del, std::max(ins, misms));
+        const bool d = mx == del, x = mx == misms;
+        pc = x ? pcigar_push(wx.get_pc(k), PCIGAR_MISMATCH)
+               : d ? pcigar_push(wd.get_pc(k + 1), PCIGAR_DELETION)
+                   : pcigar_push(wi.get_pc(k - 1), PCIGAR_INSERTION);
+        pv = x ? wx.get_pv(k) : d ? wd.get_pv(k + 1) : wi.get_pv(k - 1);
+      }
+      out.set_bt(k, pc, pv);
+    }
+  }
+  struct GapPick {
+    int32_t off;
+    uint32_t pc, pv;
+  };
+  // `gap` (:146-170): the M opening at kk or the extension at kk, the
+  // extension on a tie.
+  static GapPick gap_pick(const Wavefront& open, const Wavefront& ext, int32_t kk) {
+    const int32_t o = open.get(kk), e = ext.get(kk);
+    return e >= o ? GapPick{e, ext.get_pc(kk), ext.get_pv(kk)} : GapPick{o, open.get_pc(kk), open.get_pv(kk)};
+  }
+  void bt_affine_cells(const Wavefront& wmm, const Wavefront& wo1, const Wavefront& wi1,
+                       const Wavefront& wd1, const Wavefront* wo2, const Wavefront* wi2,
+                       const Wavefront* wd2, Wavefront& mc, Wavefront& ic, Wavefront& dc,
+                       Wavefront* i2c, Wavefront* d2c, int32_t lo, int32_t hi) {
+    const bool two = i2c != nullptr;
+    for (int32_t k = lo; k <= hi; ++k) {
+      GapPick i1 = gap_pick(wo1, wi1, k - 1), d1 = gap_pick(wo1, wd1, k + 1);
+      i1.off = wrap_add(i1.off, 1);
+      i1.pc = pcigar_push(i1.pc, PCIGAR_INSERTION);
+      d1.pc = pcigar_push(d1.pc, PCIGAR_DELETION);
+      ic.set_bt(k, i1.pc, i1.pv);
+      dc.set_bt(k, d1.pc, d1.pv);
+      const int32_t misms = wrap_add(wmm.get(k), 1);
+      uint32_t pc, pv;
+      int32_t mx;
+      if (!two) {
+        mx = std::max(d1.off, std::max(misms, i1.off));
+        const bool d = mx == d1.off;
+        pc = d ? d1.pc : i1.pc;
+        pv = d ? d1.pv : i1.pv;
+      } else {
+        GapPick i2 = gap_pick(*wo2, *wi2, k - 1), d2 = gap_pick(*wo2, *wd2, k + 1);
+        i2.off = wrap_add(i2.off, 1);
+        i2.pc = pcigar_push(i2.pc, PCIGAR_INSERTION);
+        d2.pc = pcigar_push(d2.pc, PCIGAR_DELETION);
+        i2c->set_bt(k, i2.pc, i2.pv);
+        d2c->set_bt(k, d2.pc, d2.pv);
+        mx = std::max(std::max(std::max(i1.off, i2.off), std::max(d1.off, d2.off)), misms);
+        const bool s2 = mx == i2.off, t1 = mx == d1.off, t2 = mx == d2.off;
+        pc = t2 ? d2.pc : t1 ? d1.pc : s2 ? i2.pc : i1.pc;
+        pv = t2 ? d2.pv : t1 ? d1.pv : s2 ? i2.pv : i1.pv;
+      }
+      const bool x = mx == misms;
+      mc.set_bt(k, pcigar_push(x ? wmm.get_pc(k) : pc, PCIGAR_MISMATCH), x ? wmm.get_pv(k) : pv);
+    }
+  }
+
+  // --- offloading, C's wavefront_backtrace_offload.c (piggyback.rs:530-705) --
+  // Every live cell's pcigar at or above `mask` moves into a new block, the
+  // cell continuing from it.
+  void offload_selective(Wavefront& wf, int32_t lo, int32_t hi, uint32_t mask) {
+    for (int32_t k = lo; k <= hi; ++k) {
+      const uint32_t pc = wf.get_pc(k);
+      if (wf.get(k) >= 0 && pc >= mask) wf.set_bt(k, 0, bt.store_block(pc, wf.get_pv(k)));
+    }
+  }
+  int32_t offload_blocks_linear(Wavefront& wf, int32_t lo, int32_t hi) {  // :557-569
+    const bool low = memory_mode == 2;
+    offload_selective(wf, lo, hi, low ? PCIGAR_FULL_MASK : PCIGAR_HALF_FULL_MASK);
+    return low ? PCIGAR_MAX_LENGTH - 1 : PCIGAR_MAX_LENGTH / 2;
+  }
+  int32_t offload_blocks_affine(Wavefront& wf, int32_t lo, int32_t hi) {  // :573-585
+    const bool low = memory_mode == 2;
+    offload_selective(wf, lo, hi, low ? PCIGAR_ALMOST_FULL_MASK : PCIGAR_HALF_FULL_MASK);
+    return low ? PCIGAR_MAX_LENGTH - 2 : PCIGAR_MAX_LENGTH / 2;
+  }
+  static int32_t occ_of(const Wavefront* w) { return is_null_wf(w) ? 0 : w->occ; }
+  static int32_t occ_gap(const Wavefront* open, const Wavefront* ext) {  // :611-620
+    int32_t o = is_null_wf(open) ? 0 : open->occ + 1;
+    if (!is_null_wf(ext)) o = std::max(o, ext->occ + 1);
+    return o;
+  }
+  void offload_component(Wavefront* wf, int32_t lo, int32_t hi) {  // :622-632
+    if (wf && !wf->null && wf->occ >= PCIGAR_MAX_LENGTH - 1) wf->occ = offload_blocks_affine(*wf, lo, hi);
   }
 
   // --- compute steps --------------------------------------------------------
@@ -1283,6 +1500,11 @@ class Aligner {
       else mx = std::max(del, std::max(ins, prev->get(k)) + 1);
       if ((uint32_t)mx > (uint32_t)m || (uint32_t)(mx - k) > (uint32_t)n) mx = OFFSET_NULL;
       cur->set(k, mx);
+    }
+    if (lit()) {
+      bt_edit_cells(*prev, *prev, *prev, *cur, lo, hi, indel);
+      // C offloads edit/indel every PCIGAR_MAX_LENGTH scores (:1848-1852).
+      if (score % PCIGAR_MAX_LENGTH == 0) offload_blocks_linear(*cur, lo, hi);
     }
     comps.set(CM, score, cur);
     trim_ends(n, m, *cur);
@@ -1329,6 +1551,12 @@ class Aligner {
       int32_t mx = std::max(del, std::max(ins, mi));
       if ((uint32_t)mx > (uint32_t)m || (uint32_t)(mx - k) > (uint32_t)n) mx = OFFSET_NULL;
       cur->set(k, mx);
+    }
+    if (lit()) {
+      bt_edit_cells(wg, wm, wg, *cur, lo, hi, false);
+      // offload_linear (:590-607)
+      cur->occ = std::max(occ_of(gap), occ_of(misms)) + 1;
+      if (!cur->null && cur->occ >= PCIGAR_MAX_LENGTH) cur->occ = offload_blocks_linear(*cur, lo, hi);
     }
     comps.set(CM, score, cur);
     if (endsfree_begin_k(score, bk)) endsfree_init(*cur, bk);
@@ -1433,6 +1661,30 @@ class Aligner {
       mc->set(k, mx);
       ic->set(k, i1);
       dc->set(k, d1);
+    }
+    if (lit()) {
+      const bool full = two && !affine_kernel;
+      bt_affine_cells(wmm, wo1, wi1, wd1, full ? &wo2 : nullptr, full ? &wi2 : nullptr,
+                      full ? &wd2 : nullptr, *mc, *ic, *dc, full ? i2c : nullptr, full ? d2c : nullptr,
+                      lo, hi);
+      // offload_affine / offload_affine2p (:635-705): occupancies from the
+      // inputs, then every output component near full is offloaded.
+      const int32_t o_i1 = occ_gap(m_open1, i1e), o_d1 = occ_gap(m_open1, d1e);
+      int32_t o_m = std::max(occ_of(m_misms), std::max(o_i1, o_d1));
+      int32_t o_i2 = 0, o_d2 = 0;
+      if (full) {
+        o_i2 = occ_gap(m_open2, i2e);
+        o_d2 = occ_gap(m_open2, d2e);
+        o_m = std::max(o_m, std::max(o_i2, o_d2));
+      }
+      ic->occ = o_i1;
+      dc->occ = o_d1;
+      mc->occ = o_m + 1;
+      if (full) { i2c->occ = o_i2; d2c->occ = o_d2; }
+      offload_component(mc, lo, hi);
+      offload_component(ic, lo, hi);
+      offload_component(dc, lo, hi);
+      if (full) { offload_component(i2c, lo, hi); offload_component(d2c, lo, hi); }
     }
     if (two && comps.modular) {
       if (!i2c) free_wf(comps.arr[CI2][out]);
@@ -1718,6 +1970,10 @@ class Aligner {
     // dead).  Corrected: every mode backtraces the best cell at the score it
     // was found at (med/low from the backtrace kept then; every score's
     // cells are kept here, so that is the cell's own chain).
+    if (compat == 1 && lit()) {
+      backtrace_piggyback_bt(zdrop_bt_pc, zdrop_bt_pv, end_pos.score, end_pos.k, end_pos.offset);
+      return;
+    }
     int32_t from = compat == 1 ? end_pos.score
                    : (!piggyback && end_pos.score >= 0) ? end_pos.score : score;
     backtrace_from(from, end_pos.k, end_pos.offset);
@@ -1785,9 +2041,78 @@ class Aligner {
     }
   }
 
-  // backtrace_piggyback + backtrace_piggyback_bt, src/aligner.rs:1443-1485:
-  // the chain of M cell (score, k) back to its begin position, unpacked.
+  // backtrace_piggyback, src/aligner.rs:1443-1459: the end cell's chain.
   void backtrace_piggyback(int32_t score, int32_t k, int32_t offset) {
+    if (!bt_literal) { backtrace_piggyback_rederived(score, k, offset); return; }
+    const Wavefront* m = comps.get(CM, score);
+    if (!m || !m->allocated(k)) { cigar.begin = 0; cigar.end = 0; return; }
+    uint32_t c, v;
+    m->bt_or_zero(k, c, v);
+    backtrace_piggyback_bt(c, v, score, k, offset);
+  }
+  // backtrace_piggyback_bt, :1463-1486: the blocks back to the initial one
+  // (traceback_from), unpacked from the initial position.
+  void backtrace_piggyback_bt(uint32_t pc, uint32_t pv, int32_t score, int32_t k, int32_t offset) {
+    const uint32_t init = bt.traceback_from(pc, pv);
+    const auto ip = bt.init_pos[init];
+    unpack_packed(bt.packed, ip.first, ip.second, offset - k, offset);
+    cigar.score = score;
+  }
+  // unpack_piggyback, :232-311, on packed blocks (end first): begin-free I
+  // then D, each block's operations from its first, matches re-extended
+  // before each (only in M when affine, where an X after I/D is the gap
+  // close and is dropped), matches to the end cell (a negative count moves
+  // back), then I and D to the sequence ends.
+  void unpack_packed(const std::vector<uint32_t>& packed, int32_t v, int32_t h, int32_t end_v,
+                     int32_t end_h) {
+    const int32_t n = plen(), m = tlen();
+    const bool affine = pen.metric == AFFINE || pen.metric == AFFINE2P;
+    int64_t p = 0;
+    auto put = [&](uint8_t op) { cigar.ops[(size_t)p++] = op; };
+    for (int32_t i = 0; i < h; ++i) put('I');
+    for (int32_t i = 0; i < v; ++i) put('D');
+    bool in_m = true;
+    for (size_t b = packed.size(); b-- > 0;) {
+      uint32_t pcig = packed[b];
+      int32_t length = PCIGAR_MAX_LENGTH;
+      if (pcig < PCIGAR_FULL_MASK) {
+        const int32_t fr = pcigar_free_slots(pcig);
+        length -= fr;
+        pcig = fr >= 16 ? 0u : pcig << (2 * fr);
+      }
+      for (int32_t j = 0; j < length; ++j) {
+        if (in_m || !affine) {
+          while (v < n && h < m && seq.cmp(v, h)) { put('M'); ++v; ++h; }
+        }
+        const uint32_t op = pcig >> 30;
+        pcig <<= 2;
+        uint8_t ch;
+        int32_t dv, dh;
+        bool mm;
+        if (op == PCIGAR_DELETION) { ch = 'D'; dv = 1; dh = 0; mm = false; }
+        else if (op == PCIGAR_MISMATCH) { ch = 'X'; dv = 1; dh = 1; mm = true; }
+        else if (op == PCIGAR_INSERTION) { ch = 'I'; dv = 0; dh = 1; mm = false; }
+        else { ch = '?'; dv = 0; dh = 0; mm = true; }
+        if (affine && !in_m && ch == 'X') { in_m = true; continue; }
+        put(ch);
+        v += dv;
+        h += dh;
+        in_m = mm;
+      }
+    }
+    const int32_t nm = std::min(end_v - v, end_h - h);
+    for (int32_t i = 0; i < nm; ++i) put('M');
+    v += nm;
+    h += nm;
+    while (h < m) { put('I'); ++h; }
+    while (v < n) { put('D'); ++v; }
+    cigar.begin = 0;
+    cigar.end = p;
+  }
+
+  // The same chain re-made from the kept offsets: each step applies the
+  // kernels' tie order to the stored predecessors (piggyback_pred).
+  void backtrace_piggyback_rederived(int32_t score, int32_t k, int32_t offset) {
     const Wavefront* m = comps.get(CM, score);
     if (!m || !m->allocated(k)) { cigar.begin = 0; cigar.end = 0; return; }
     std::vector<uint8_t> back;
@@ -1990,7 +2315,8 @@ class Aligner {
       if (cand) result = best.total;
       if (scope == SCOPE_ALIGNMENT && (status == END_REACHED || end_pos.offset != OFFSET_NULL)) {
         if (cand) {
-          backtrace_from(best.pos.score, best.pos.k, best.pos.offset);
+          if (lit()) backtrace_piggyback_bt(best.bt_pc, best.bt_pv, best.pos.score, best.pos.k, best.pos.offset);
+          else backtrace_from(best.pos.score, best.pos.k, best.pos.offset);
           cigar.score = best.total;
         } else if (unreachable) {
           backtrace_zdrop_end(score);
@@ -2269,6 +2595,7 @@ void wfo_destroy(void* h) { delete static_cast<Aligner*>(h); }
 void wfo_set_alignment_scope(void* h, int a) { static_cast<Aligner*>(h)->scope = a ? SCOPE_ALIGNMENT : SCOPE_SCORE; }
 void wfo_set_memory_mode(void* h, int mode) { static_cast<Aligner*>(h)->memory_mode = mode; }
 void wfo_set_compat(void* h, int compat) { static_cast<Aligner*>(h)->compat = compat; }
+void wfo_set_piggyback_literal(void* h, int on) { static_cast<Aligner*>(h)->bt_literal = on != 0; }
 void wfo_set_heuristic(void* h, int kind, int32_t p0, int32_t p1, int32_t p2) {
   Heuristic& hs = static_cast<Aligner*>(h)->heur;
   hs.kind = kind; hs.p0 = p0; hs.p1 = p1; hs.p2 = p2;

@@ -42,6 +42,12 @@ void wfo_destroy(void* h);
 void wfo_set_alignment_scope(void* h, int compute_alignment);
 void wfo_set_memory_mode(void* h, int mode);
 void wfo_set_compat(void* h, int compat);  // 0 C, 1 Corrected (src/aligner.rs:53-94)
+/* Med/low with an alignment: 1 (default) runs the reference's piggyback
+ * path as it is (per-cell packed CIGARs and backtrace-buffer blocks,
+ * src/compute/piggyback.rs, src/bt_buffer.rs); 0 re-makes the kernels' picks
+ * from the kept offsets after the end cell is found (the design the GPU
+ * library uses).  Both give the same results. */
+void wfo_set_piggyback_literal(void* h, int on);
 void wfo_set_heuristic(void* h, int kind, int32_t p0, int32_t p1, int32_t p2);
 void wfo_set_max_alignment_steps(void* h, int32_t steps);
 void wfo_set_alignment_free_ends(void* h, int32_t p0, int32_t pf, int32_t t0, int32_t tf);

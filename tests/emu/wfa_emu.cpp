@@ -24,42 +24,50 @@ EmuWarp* g_emu_warp = nullptr;
 }  // namespace wfab
 #endif
 
-template <int CLS, bool GEN>
+template <int CLS, bool GEN, bool PB>
 static bool run_lane_g(const AlignParams& P, const Workspace& ws, int64_t i) {
   if (P.format == WFA_SEQ_PACKED2) {
     const uint32_t* w = reinterpret_cast<const uint32_t*>(P.seq);
     SeqPacked sp{w + P.p_off[i], P.p_len[i], (P.p_len[i] + 15) >> 4};
     SeqPacked st{w + P.t_off[i], P.t_len[i], (P.t_len[i] + 15) >> 4};
-    return align_one<CLS, SeqPacked, GEN>(P, ws, i, sp, st);
+    return align_one<CLS, SeqPacked, GEN, WFA_WARP, PB>(P, ws, i, sp, st);
   }
   SeqAscii sp{P.seq + P.p_off[i], P.p_len[i]};
   SeqAscii st{P.seq + P.t_off[i], P.t_len[i]};
-  return align_one<CLS, SeqAscii, GEN>(P, ws, i, sp, st);
+  return align_one<CLS, SeqAscii, GEN, WFA_WARP, PB>(P, ws, i, sp, st);
 }
 
 // Same dispatch as the kernel launcher: the lean instantiation for
-// end-to-end alignments without a heuristic, the general one otherwise.
+// end-to-end alignments without a heuristic, the med/low one for med/low
+// with an alignment, the general one otherwise.
 template <int CLS>
 static bool run_lane(const AlignParams& P, const Workspace& ws, int64_t i) {
-  if (P.span == WFA_SPAN_END2END && P.hkind == WFA_HEURISTIC_NONE && !P.piggyback)
-    return run_lane_g<CLS, false>(P, ws, i);
-  return run_lane_g<CLS, true>(P, ws, i);
+  if (P.piggyback && P.compute_alignment) return run_lane_g<CLS, true, true>(P, ws, i);
+  if (P.span == WFA_SPAN_END2END && P.hkind == WFA_HEURISTIC_NONE)
+    return run_lane_g<CLS, false, false>(P, ws, i);
+  return run_lane_g<CLS, true, false>(P, ws, i);
 }
 
 // The kernel's compact ring: P.ring_slots slots of P.wmax cells (narrow, as
 // the shared-memory slots are), rows wider than that in the spill ring of
 // P.wspill cells per slot -- both paths run in every emulated alignment.
+// Med/low: the ring as wide as any wavefront, with the pcigar and block
+// arrays after the offsets, and the backtrace buffer.
 template <int CLS>
 static bool run_pair(const AlignParams& P, int64_t i) {
   constexpr int NC = CLS == kAffine2pClass ? 5 : CLS == kAffineClass ? 3 : 1;
+  const size_t arrays = P.piggyback ? 3 : 1;
   std::vector<WfD> ring((size_t)P.desc_depth * NC);
-  std::vector<int32_t> ringv((size_t)P.ring_slots * P.wmax, 0x5A5A5A5A);
+  std::vector<int32_t> ringv(arrays * P.ring_slots * P.wmax, 0x5A5A5A5A);
   std::vector<int32_t> ringg((size_t)P.ring_slots * P.wspill, 0x5A5A5A5A);
   std::vector<int4> hist((size_t)P.hist_scores, int4{0, -1, 0, 0});
   std::vector<int32_t> harena((size_t)P.hist_words, 0x5A5A5A5A);
   std::vector<int32_t> dom((size_t)P.dom_words, 0x5A5A5A5A);
+  std::vector<uint2> bt((size_t)P.bt_cap, uint2{0x5A5A5A5A, 0x5A5A5A5A});
+  std::vector<int2> btinit((size_t)P.bt_init_cap, int2{0x5A5A5A5A, 0x5A5A5A5A});
+  std::vector<uint32_t> btmark(2 * (((size_t)P.bt_cap + 31) / 32) + 1, 0x5A5A5A5A);
   Workspace ws{ring.data(), ringv.data(), hist.data(), harena.data(),
-               P.dom_words ? dom.data() : nullptr, ringg.data()};
+               P.dom_words ? dom.data() : nullptr, ringg.data(), bt.data(), btinit.data(), btmark.data()};
 #ifdef WFA_EMU_THREADS
   EmuWarp warp;
   g_emu_warp = &warp;
@@ -86,7 +94,7 @@ extern "C" int64_t wfa_emu_batch(int metric, const int32_t* pen6, int compute_al
                                  const int32_t* t_len, int64_t num_pairs, const int64_t* cigar_off,
                                  uint8_t* cigars, wfa_result_t* results, int32_t wmax,
                                  int32_t hist_scores, int64_t hist_words, int piggyback,
-                                 int compat) {
+                                 int compat, int64_t bt_limit, int32_t bt_cap, int32_t bt_probe) {
   AlignParams P;
   std::memset(&P, 0, sizeof P);
   wfa_penalties_t u = {pen6[0], pen6[1], pen6[2], pen6[3], pen6[4], pen6[5]};
@@ -116,6 +124,16 @@ extern "C" int64_t wfa_emu_batch(int metric, const int32_t* pen6, int compute_al
   P.desc_depth = compact_desc_depth(P, metric_class(metric));
   int32_t max_len_sum = 0;
   for (int64_t i = 0; i < num_pairs; ++i) max_len_sum = std::max(max_len_sum, p_len[i] + t_len[i]);
+  if (P.piggyback && P.compute_alignment) {
+    P.wmax = wmax;  // no spill ring: the ring holds offsets, pcigars and block indices
+    P.wspill = 0;
+    P.hist_scores = 0;
+    P.hist_words = 0;
+    P.bt_cap = bt_cap;
+    P.bt_init_cap = max_len_sum + 8;
+    P.bt_limit = bt_limit;
+    P.bt_probe = bt_probe;
+  }
   const int nc = metric == WFA_METRIC_GAP_AFFINE_2P ? 5 : metric == WFA_METRIC_GAP_AFFINE ? 3 : 1;
   P.dom_words = (int64_t)nc * (max_len_sum + 2 * P.scope + 5);
   int64_t retries = 0;

@@ -31,10 +31,14 @@ def _p(a):
 
 def run(metric, pen, pairs, compute_alignment=True, span=0, extension=0, free=None, heuristic=0,
         hparams=(0, 0, 0), max_steps=2**31 - 1, packed=False, wmax=4096, hist_scores=1 << 16,
-        hist_words=1 << 22, lanes=None, piggyback=False, compat=0):
+        hist_words=1 << 22, lanes=None, piggyback=False, compat=0, bt_limit=256 << 20,
+        bt_cap=1 << 20, bt_probe=6000):
     """pairs: list of (bytes, bytes).  Returns (results, list of cigar strings).
-    piggyback: med/low memory with an alignment (the piggyback backtrace);
-    compat: 0 C, 1 Corrected."""
+    piggyback: med/low memory with an alignment (the piggyback backtrace):
+    True or "med", or "low"; compat: 0 C, 1 Corrected; bt_limit: bytes of
+    backtrace blocks above which the buffer is compacted (max_memory_compact);
+    bt_cap: blocks of the backtrace buffer; bt_probe: scores between
+    compaction probes (the library's is the reference's 6000)."""
     n = len(pairs)
     if packed:
         words, p_off, t_off, p_len, t_len = [], [], [], [], []
@@ -73,7 +77,8 @@ def run(metric, pen, pairs, compute_alignment=True, span=0, extension=0, free=No
                         _p(seq), ctypes.c_int64(seq.nbytes), _p(p_off), _p(p_len), _p(t_off),
                         _p(t_len), ctypes.c_int64(n), _p(c_off), _p(cig), _p(res),
                         ctypes.c_int32(wmax), ctypes.c_int32(hist_scores), ctypes.c_int64(hist_words),
-                        int(piggyback), int(compat))
+                        2 if piggyback == "low" else int(bool(piggyback)), int(compat),
+                        ctypes.c_int64(bt_limit), ctypes.c_int32(bt_cap), ctypes.c_int32(bt_probe))
     assert r >= 0
     cigars = []
     for i in range(n):

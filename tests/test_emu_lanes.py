@@ -56,7 +56,7 @@ def test_32_lanes_memory_modes_and_corrected(metric, pen, span, free, memory, co
         fr = [min(free[0], min(len(p) for p, _ in pairs)), min(free[1], min(len(p) for p, _ in pairs)),
               min(free[2], min(len(t) for _, t in pairs)), min(free[3], min(len(t) for _, t in pairs))]
     res, cig = emu_lib.run(metric, pen, pairs, span=span, free=fr, lanes=32,
-                           piggyback=memory != "high", compat=compat)
+                           piggyback=memory if memory != "high" else False, compat=compat)
     for i, (p, t) in enumerate(pairs):
         s, st, ops, ep, _ = oracle_run(metric, pen, p, t, True, span, fr, 0, [0, 0, 0],
                                        memory=memory, compat=compat)

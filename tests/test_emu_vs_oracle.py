@@ -43,7 +43,7 @@ def compare(metric, pen, pairs, compute=True, span=0, free=None, hk=0, hp=(0, 0,
             extension=False, packed=False, memory="high", compat=0):
     res, cig = emu_lib.run(metric, pen, pairs, compute_alignment=compute, span=span or int(extension),
                            extension=int(extension), free=free, heuristic=hk, hparams=hp,
-                           packed=packed, piggyback=compute and memory != "high", compat=compat)
+                           packed=packed, piggyback=memory if compute and memory != "high" else False, compat=compat)
     for i, (p, t) in enumerate(pairs):
         s, st, ops, ep, (cs, ev, eh) = oracle_run(metric, pen, p, t, compute, span, free, hk, hp,
                                                   extension, memory, compat)
@@ -212,7 +212,7 @@ def test_golden_cli_cases(golden):
                 span = 1
             res, cig = emu_lib.run(metric, pen, [(pb, tb)], compute_alignment=not so, span=span,
                                    extension=ext, free=free, heuristic=hk, hparams=hp[:3],
-                                   piggyback=not so and case["memory"] != "high",
+                                   piggyback=case["memory"] if not so and case["memory"] != "high" else False,
                                    compat=int(case.get("no_c_compat", False)))
             orig = (pen + [0] * 6)[:6]
             lines.append(cli_format.line(metric, orig, so, False, res[0], cig[0], len(pb), len(tb),
@@ -220,3 +220,40 @@ def test_golden_cli_cases(golden):
         assert lines == case["expected"], case["name"]
         checked += 1
     assert checked >= 20
+
+
+# Med/low on the configurations where the kernels' picks depend on values a
+# later step changes (a heuristic emptying I/D of the same score; C-mode
+# Z-drop ends read on a dead cell), and with the backtrace buffer compacted
+# every few scores under a tiny limit: the oracle, which never compacts,
+# must still agree on every pair (compaction keeps every live chain whole).
+@pytest.mark.parametrize("memory", ["med", "low"])
+def test_piggyback_picks_and_compaction(memory):
+    import random
+    rng = random.Random(4242)
+    pairs = []
+    for _ in range(30):
+        n = rng.randint(40, 400)
+        p = bytes(rng.choice(b"ACGT") for _ in range(n))
+        t = bytearray()
+        for c in p:
+            u = rng.random()
+            if u < 0.05: t += bytes([rng.choice(b"ACGT")])
+            elif u < 0.10: t += bytes([rng.choice(b"ACGT"), c])
+            elif u < 0.15: pass
+            else: t.append(c)
+        pairs.append((p, bytes(t)))
+    cases = [(3, [-3, 5, 3, 2], 1, 5, (-8, 8, 1)), (4, [-1, 4, 6, 2, 24, 1], 0, 3, (20, 1, 0)),
+             (4, [-1, 4, 6, 2, 24, 1], 1, 5, (-8, 8, 1)), (3, [0, 4, 6, 2], 0, 0, (0, 0, 0)),
+             (1, None, 0, 0, (0, 0, 0)), (2, [0, 4, 2], 1, 1, (10, 50, 1))]
+    for metric, pen, span, hk, hp in cases:
+        for probe, limit in ((6000, 256 << 20), (3, 64)):
+            for p, t in pairs:
+                free = [len(p) // 5, len(p) // 5, len(t) // 5, len(t) // 5] if span else None
+                res, cig = emu_lib.run(metric, pen, [(p, t)], span=span, free=free, heuristic=hk,
+                                       hparams=hp, piggyback=memory, bt_limit=limit, bt_probe=probe,
+                                       bt_cap=1 << 16)
+                s, st, ops, ep, cg = oracle_run(metric, pen, p, t, True, span, free, hk, list(hp),
+                                                memory=memory)
+                assert (int(res["score"][0]), int(res["status"][0]), cig[0]) == (s, st, ops), \
+                    (metric, pen, span, hk, probe, len(p))

@@ -239,6 +239,84 @@ def test_corrected_reference_cases(pkg, golden):
     assert got == {x["cigar_affine_score"]}
 
 
+def test_med_low_picks_fixed_at_compute_time(pkg):
+    """Med/low where a later step changes what a kernel read: banded-adaptive
+    cutoffs emptying I/D of the score M was just computed from (ends-free,
+    match reward), and C-mode Z-drop ends read on a dead cell."""
+    r = random.Random(4242)
+    pairs = []
+    for _ in range(40):
+        n = r.randint(40, 400)
+        p = bytes(r.choice(b"ACGT") for _ in range(n))
+        t = bytearray()
+        for c in p:
+            u = r.random()
+            if u < 0.05: t += bytes([r.choice(b"ACGT")])
+            elif u < 0.10: t += bytes([r.choice(b"ACGT"), c])
+            elif u < 0.15: pass
+            else: t.append(c)
+        pairs.append((p, bytes(t)))
+    for memory in ("med", "low"):
+        for p, t in pairs:
+            free = [len(p) // 5, len(p) // 5, len(t) // 5, len(t) // 5]
+            compare(pkg, 3, [-3, 5, 3, 2], [(p, t)], span=1, free=free, hk=5, hp=(-8, 8, 1), memory=memory)
+            compare(pkg, 4, [-1, 4, 6, 2, 24, 1], [(p, t)], span=1, free=free, hk=5, hp=(-8, 8, 1),
+                    memory=memory)
+        compare(pkg, 4, [-1, 4, 6, 2, 24, 1], pairs, hk=3, hp=(20, 1, 0), memory=memory)
+        compare(pkg, 4, [-1, 4, 6, 2, 24, 1], pairs, extension=True, hk=3, hp=(20, 1, 0), memory=memory)
+
+
+def test_med_low_compaction_and_memory(pkg):
+    """Pairs whose alignments pass score 6000 (the reference's compaction
+    probe) with max_memory_compact at 64 KiB: the backtrace buffer is
+    compacted and every CIGAR still equals the oracle's (which never
+    compacts).  Med/low hold no history, so a pair needs less device memory
+    than in high memory."""
+    r = random.Random(31)
+    pairs = []
+    for n in (7000, 8000):
+        p = bytes(r.choice(b"ACGT") for _ in range(n))
+        t = bytearray()
+        for c in p:
+            u = r.random()
+            if u < 0.08: t += bytes([r.choice(b"ACGT")])
+            elif u < 0.14: t += bytes([r.choice(b"ACGT"), c])
+            elif u < 0.20: pass
+            else: t.append(c)
+        pairs.append((p, bytes(t)))
+    for memory in ("med", "low"):
+        a = pkg.WavefrontAligner(3, [0, 4, 6, 2])
+        a.set_alignment_scope(True)
+        a.set_memory_mode(memory)
+        a.set_max_memory_compact(64 << 10)
+        seq, po, pl, to, tl = pack(pairs)
+        res, cig = a.align_batch(seq, po, pl, to, tl)
+        a.close()
+        for i, (p, t) in enumerate(pairs):
+            o = O.OracleAligner(3, [0, 4, 6, 2])
+            o.set_alignment_scope(True)
+            o.set_memory_mode(memory)
+            s = o.align_end2end(p, t)
+            assert s > 6000
+            rr = res[i]
+            got = cig[rr["cigar_begin"]:rr["cigar_begin"] + rr["cigar_length"]].tobytes()
+            assert (int(rr["score"]), int(rr["status"]), got) == (s, o.status(), o.cigar()[0]), (memory, i)
+    # Device bytes per pair in flight: C4-shaped pairs (0.5-5 kbp cores with
+    # flanks), extension span, CIGAR, med against high memory.
+    from wfa_b200 import synth
+    ps = synth.config4(64, synth.SEED_BASE + 44)
+    sizes = {}
+    for memory in ("high", "med"):
+        a = pkg.WavefrontAligner(3, [0, 4, 6, 2])
+        a.set_alignment_scope(True)
+        a.set_memory_mode(memory)
+        a.set_alignment_extension()
+        a.align_batch(ps.buf, ps.p_off, ps.p_len, ps.t_off, ps.t_len, span=1)
+        sizes[memory] = a.last_slice_bytes()
+        a.close()
+    assert 0 < sizes["med"] < sizes["high"], sizes
+
+
 def test_med_low_long_pairs(pkg):
     """Pairs long enough to outgrow the first history size re-run and match."""
     r = random.Random(29)

@@ -115,6 +115,7 @@ def lib():
         "wfa_last_rerun_pairs": (i64, [vp]),
         "wfa_set_lanes_per_pair": (ctypes.c_int, [vp, i32]),
         "wfa_last_lanes_per_pair": (i32, [vp]),
+        "wfa_last_slice_bytes": (i64, [vp]),
         "wfa_autotune_report": (i32, [ctypes.c_char_p, i32]),
         "wfa_last_kernel_ms": (ctypes.c_double, [vp]),
         "wfa_cigar_rle": (i32, [vp, i32, ctypes.c_char_p, i32]),
@@ -279,6 +280,10 @@ class WavefrontAligner:
 
     def last_lanes_per_pair(self):
         return self._L.wfa_last_lanes_per_pair(self._h)
+
+    def last_slice_bytes(self):
+        """Device bytes one pair in flight used in the last launch."""
+        return self._L.wfa_last_slice_bytes(self._h)
 
     # --- batches ---
     def align_batch(self, seq, p_off, p_len, t_off, t_len, packed=False, span=SPAN_END2END,

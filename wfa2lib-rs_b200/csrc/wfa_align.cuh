@@ -38,6 +38,8 @@
 #include <cstdlib>
 #ifndef __CUDACC__
 struct int4 { int x, y, z, w; };
+struct int2 { int x, y; };
+struct uint2 { unsigned x, y; };
 #endif
 #define WFA_D inline
 #define WFA_DN inline
@@ -87,6 +89,19 @@ struct Warp {
   static int min(int v) { return reduce(v, false); }
   static int max(int v) { return reduce(v, true); }
   static unsigned any(bool p) { return (unsigned)reduce(p ? 1 : 0, true); }
+  // Lanes below this one with p set; *total: lanes with p set.
+  static int rank(bool p, int* total) {
+    EmuWarp* w = g_emu_warp;
+    w->red[g_emu_lane] = p ? 1 : 0;
+    w->bar.arrive_and_wait();
+    int below = 0, all = 0;
+    for (int i = 0; i < WFA_WARP; ++i) { all += w->red[i]; if (i < g_emu_lane) below += w->red[i]; }
+    w->bar.arrive_and_wait();
+    *total = all;
+    return below;
+  }
+  static uint32_t atomic_or(uint32_t* a, uint32_t v) { return __atomic_fetch_or(a, v, __ATOMIC_RELAXED); }
+  static int popc(uint32_t x) { return __builtin_popcount(x); }
   static uint32_t ffs(uint32_t x) { return x ? (uint32_t)__builtin_ctz(x) + 1 : 0; }
   static uint32_t clz(uint32_t x) { return x ? (uint32_t)__builtin_clz(x) : 32; }
   static uint32_t funnel(uint32_t lo, uint32_t hi, uint32_t s) {
@@ -100,6 +115,7 @@ struct Warp {
   static WFA_D int max(int v) { return __reduce_max_sync(0xffffffffu, v); }
   static WFA_D unsigned any(bool p) { return __ballot_sync(0xffffffffu, p); }
   static WFA_D void sync() { __syncwarp(); }
+  static WFA_D int popc(uint32_t x) { return __popc(x); }
   static WFA_D uint32_t ffs(uint32_t x) { return (uint32_t)__ffs((int)x); }
   static WFA_D uint32_t clz(uint32_t x) { return (uint32_t)__clz((int)x); }
   static WFA_D uint32_t funnel(uint32_t lo, uint32_t hi, uint32_t s) { return __funnelshift_r(lo, hi, s); }
@@ -108,6 +124,9 @@ struct Warp {
   static int min(int v) { return v; }
   static int max(int v) { return v; }
   static unsigned any(bool p) { return p ? 1u : 0u; }
+  static int rank(bool p, int* total) { *total = p ? 1 : 0; return 0; }
+  static uint32_t atomic_or(uint32_t* a, uint32_t v) { uint32_t o = *a; *a = o | v; return o; }
+  static int popc(uint32_t x) { return __builtin_popcount(x); }
   static void sync() {}
   static uint32_t ffs(uint32_t x) { return x ? (uint32_t)__builtin_ctz(x) + 1 : 0; }
   static uint32_t clz(uint32_t x) { return x ? (uint32_t)__builtin_clz(x) : 32; }
@@ -136,6 +155,14 @@ struct Lanes {
   static WFA_D int max(int v) { return __reduce_max_sync(mask(), v); }
   static WFA_D unsigned any(bool p) { return __ballot_sync(mask(), p) & mask(); }
   static WFA_D void sync() { __syncwarp(mask()); }
+  // Lanes of the group below this one with p set; *total: the group's lanes
+  // with p set.
+  static WFA_D int rank(bool p, int* total) {
+    const unsigned b = __ballot_sync(mask(), p) & mask();
+    *total = __popc(b);
+    return __popc(b & ((1u << (threadIdx.x & 31)) - 1u));
+  }
+  static WFA_D uint32_t atomic_or(uint32_t* a, uint32_t v) { return atomicOr(a, v); }
 };
 #else
 template <int LW>
@@ -226,6 +253,13 @@ WFA_D int lcp_bwd(const S& P, int v, const S& T, int h, int R) {
 // Wavefront descriptors
 // ---------------------------------------------------------------------------
 constexpr int kPresent = 1, kNullFlag = 2;
+// Packed CIGARs of the med/low (piggyback) backtrace, src/pcigar.rs:13-35:
+// up to 16 two-bit operations per u32, pushed at the low end.
+constexpr uint32_t kPcDel = 1, kPcMisms = 2, kPcIns = 3;
+constexpr uint32_t kPcFullMask = 0x40000000u, kPcAlmostFullMask = 0x10000000u, kPcHalfFullMask = 0x00010000u;
+constexpr int kPcMaxLength = 16;
+constexpr uint32_t kBtNull = 0xFFFFFFFFu;  // BT_BLOCK_IDX_NULL, src/bt_buffer.rs:11
+WFA_D uint32_t pc_push(uint32_t pc, uint32_t op) { return (pc << 2) | op; }
 constexpr int32_t kAdUnknown = INT32_MAX / 4, kAdNone = INT32_MIN / 4;
 constexpr int CM = 0, CI1 = 1, CD1 = 2, CI2 = 3, CD2 = 4;
 
@@ -273,6 +307,11 @@ struct Workspace {
   int32_t* harena;  // M history cells
   int32_t* dom;     // Corrected-mode dominance array (NC x diagonals), or null
   int32_t* ringg;   // compact ring: rows wider than the ring's slots (device memory), or null
+  // Med/low: the backtrace buffer (blocks {pcigar, prev}), the initial
+  // positions of its chains ({v, h}) and the mark bitmap of its compaction.
+  uint2* bt;
+  int2* btinit;
+  uint32_t* btmark;
 };
 
 // GEN = false compiles the common configuration only (end-to-end, no
@@ -281,7 +320,9 @@ struct Workspace {
 // compute and of the BiWFA extend: their loads are all issued before any
 // result is stored, so a lane keeps UNR cells' loads in flight (wide
 // wavefronts of long pairs, whose cells live in device memory).
-template <int CLS, class S, bool GEN = true, int UNR = 1, int LW = WFA_WARP>
+// PB: the med/low (piggyback) code is compiled in (a separate kernel: it
+// would otherwise cost the other general alignments registers).
+template <int CLS, class S, bool GEN = true, int UNR = 1, int LW = WFA_WARP, bool PB = false>
 struct PairAligner {
   using G = Lanes<LW>;
   static constexpr int NC = CLS == kAffine2pClass ? 5 : CLS == kAffineClass ? 3 : 1;
@@ -320,11 +361,20 @@ struct PairAligner {
   // steps store null slots (BiWFA's overlap scans read every ring slot).
   int32_t hist_nc;
   bool keep_null_slots;
-  // Med/low memory with an alignment (the piggyback backtrace), and the
-  // begin-free seeds endsfree_init placed at the current score (bit 0 text
-  // seed at +k, bit 1 pattern seed at -k), stored with M's history record.
+  // Med/low memory with an alignment: the piggyback backtrace as the
+  // reference runs it (src/compute/piggyback.rs).  Every cell of every
+  // component carries a packed CIGAR and the index of the backtrace-buffer
+  // block it continues, stored pcoff and 2 * pcoff words after the cell's
+  // offset in the same ring slot; full packed CIGARs move into the buffer
+  // (ws.bt, bt_used of P.bt_cap blocks) and chains start at initial blocks
+  // whose positions are in ws.btinit.  There is no history: med/low needs
+  // only the ring and the buffer.  The occupancy the offload tracks
+  // (bt_occupancy_max) rides in a wavefront's descriptor, in adub.
   bool pgb = false;
-  int32_t seed_flags = 0;
+  int64_t pcoff = 0;
+  int32_t bt_used = 0, bi_used = 0;
+  int32_t mL = 1, mH = 0;  // the cells the current score's M kernel wrote
+  uint32_t cand_pc = 0, cand_pv = kBtNull, zd_pc = 0, zd_pv = kBtNull;
   // Compat::Corrected ends-free with a match reward (src/aligner.rs:1104-1345):
   // the end candidate (the best cell reaching a free end so far, its total
   // score) and the begin-free dominance array (ws.dom, NC x diagonals from
@@ -366,7 +416,7 @@ struct PairAligner {
     int i = cidx - ((cscore - t) >> gshift);
     i = i < 0 ? i + dscope : i;
 #if !(defined(__CUDACC__) && !defined(WFA_EMU))
-    if (i < 0 || i >= dscope || ((cscore - t) & ((1 << gshift) - 1))) std::abort();  // emulation-only check
+    if (i < 0 || i >= dscope) std::abort();  // emulation-only check
 #endif
     return i;
   }
@@ -414,10 +464,98 @@ struct PairAligner {
 #if !(defined(__CUDACC__) && !defined(WFA_EMU))
     if (compact && idx >= P.ring_slots) std::abort();  // emulation-only check
 #endif
-    if (w <= wmax) return ws.ringv + idx * wmax;
+    if (w <= wmax) {
+      int32_t* base = ws.ringv + idx * wmax;
+      if (PB && pgb && c == CM) { mbase = base; mL = L; mH = H; }
+      return base;
+    }
     if (compact && ws.ringg && w <= P.wspill) return ws.ringg + idx * P.wspill;
     retry = true;
     return nullptr;
+  }
+
+  // ---- med/low: packed CIGARs and the backtrace buffer -----------------------
+  int32_t* mbase = nullptr;  // the current score's M slot (cells from mL)
+  WFA_D uint32_t* pcs(int32_t* v) const { return reinterpret_cast<uint32_t*>(v + pcoff); }
+  WFA_D uint32_t* pvs(int32_t* v) const { return reinterpret_cast<uint32_t*>(v + 2 * pcoff); }
+  // (pcigar, prev) of cell k as the kernels read it: zero outside the
+  // initialised range (init_ends zeroes them, src/wavefront.rs:422-457, and
+  // the null wavefront holds zeroes).
+  WFA_D uint32_t rpc(const WfD& d, int k) const { return (k >= d.a && k <= d.b) ? pcs(d.vals)[k - d.a] : 0u; }
+  WFA_D uint32_t rpv(const WfD& d, int k) const { return (k >= d.a && k <= d.b) ? pvs(d.vals)[k - d.a] : 0u; }
+  // bt_occupancy_max of an input (0 if absent or null).
+  WFA_D int32_t occ_of(const WfD& d) const { return d.flags == kPresent ? d.adub : 0; }
+  // bt_or_zero (src/wavefront.rs:410-416) on the current score's M: the
+  // cells its kernel wrote (mL..mH), else zeroes.
+  WFA_D void m_bt(int k, uint32_t& c, uint32_t& v) const {
+    if (mbase && k >= mL && k <= mH) { c = pcs(mbase)[k - mL]; v = pvs(mbase)[k - mL]; }
+    else { c = 0; v = 0; }
+  }
+  // init_block (src/bt_buffer.rs:134-139) for the cell at base[i]: an empty
+  // pcigar continuing a new initial block at (v, h) (set_bt_init,
+  // src/aligner.rs:213-225).  Lane 0 writes.
+  WFA_D void bt_init_cell(int32_t* base, int64_t i, int v, int h) {
+    if (bt_used >= P.bt_cap || bi_used >= P.bt_init_cap) { retry = true; return; }
+    if (lane == 0) {
+      ws.btinit[bi_used] = int2{v, h};
+      ws.bt[bt_used] = uint2{(uint32_t)bi_used, kBtNull};
+      pcs(base)[i] = 0;
+      pvs(base)[i] = (uint32_t)bt_used;
+    }
+    ++bi_used;
+    ++bt_used;
+  }
+  // zero_bt (src/wavefront.rs:570-580) on cells base[i0 .. i1].
+  WFA_D void bt_zero(int32_t* base, int64_t i0, int64_t i1) {
+    for (int64_t i = i0 + lane; i <= i1; i += LW) { pcs(base)[i] = 0; pvs(base)[i] = 0; }
+  }
+  // offload_blocks_selective (src/compute/piggyback.rs:530-555) on output
+  // cells [lo, hi] of a slot whose cells start at L: every live cell whose
+  // pcigar is at or above `mask` moves into a new block (in ascending k, as
+  // the reference numbers them) and continues from it.
+  WFA_D void offload_cells(int32_t* base, int L, int lo, int hi, uint32_t mask) {
+    uint32_t* pc = pcs(base);
+    uint32_t* pv = pvs(base);
+    for (int k0 = lo; k0 <= hi; k0 += LW) {
+      const int k = k0 + lane;
+      bool mv = false;
+      uint32_t c = 0;
+      if (k <= hi) {
+        c = pc[k - L];
+        mv = base[k - L] >= 0 && c >= mask;
+      }
+      int total;
+      const int r = G::rank(mv, &total);
+      if (bt_used + total > P.bt_cap) { retry = true; return; }
+      if (mv) {
+        ws.bt[bt_used + r] = uint2{c, pv[k - L]};
+        pc[k - L] = 0;
+        pv[k - L] = (uint32_t)(bt_used + r);
+      }
+      bt_used += total;
+    }
+    G::sync();
+  }
+  WFA_D bool pb_low() const { return P.piggyback == 2; }
+  // offload_blocks_linear / _affine (:557-585); returns the occupancy left.
+  WFA_D int32_t offload_linear_cells(int32_t* base, int L, int lo, int hi) {
+    offload_cells(base, L, lo, hi, pb_low() ? kPcFullMask : kPcHalfFullMask);
+    return pb_low() ? kPcMaxLength - 1 : kPcMaxLength / 2;
+  }
+  WFA_D int32_t offload_affine_cells(int32_t* base, int L, int lo, int hi) {
+    offload_cells(base, L, lo, hi, pb_low() ? kPcAlmostFullMask : kPcHalfFullMask);
+    return pb_low() ? kPcMaxLength - 2 : kPcMaxLength / 2;
+  }
+  // occupancy of a gap component fed by an M opening and its own extension
+  // (:611-620).
+  WFA_D int32_t occ_gap(const WfD& open, const WfD& ext) const {
+    int32_t o = open.flags == kPresent ? open.adub + 1 : 0;
+    if (ext.flags == kPresent) o = imax(o, ext.adub + 1);
+    return o;
+  }
+  // offload_affine_component (:622-632) for an output with occupancy occ.
+  WFA_D int32_t offload_component(int32_t* base, int L, int lo, int hi, int32_t occ) {
+    return occ >= kPcMaxLength - 1 ? offload_affine_cells(base, L, lo, hi) : occ;
   }
   // Depths of the compact ring for score step gstep (the longest read offset
   // of M is scope - 1; of a gap component its extension penalty).
@@ -431,7 +569,7 @@ struct PairAligner {
   // High memory: once M at score s is final (after its extend step), copy its
   // initialised range to the history arena for the backtrace.
   WFA_D void hist_commit(int s) {
-    if (modular) return;
+    if (modular || (PB && pgb)) return;
     if ((int64_t)(s + 1) * hist_nc > P.hist_scores) { retry = true; return; }
     for (int c = 0; c < hist_nc; ++c) {
       WfD d = slot(c, s);
@@ -442,12 +580,11 @@ struct PairAligner {
         if (hused + w > P.hist_words) { retry = true; return; }
         for (int64_t i = lane; i < w; i += LW) ws.harena[hused + i] = d.vals[i];
         r.z = (int32_t)hused;
-        r.w = GEN && c == CM ? 1 | (seed_flags << 1) : 1;
+        r.w = 1;
         hused += w;
       }
       if (lane == 0) ws.hist[(int64_t)s * hist_nc + c] = r;
     }
-    seed_flags = 0;
     // No sync: the history is read only by the backtrace, which starts with one.
   }
 
@@ -518,24 +655,35 @@ struct PairAligner {
   // and computed over [lo, hi]; returns the new limits through lo/hi.
   WFA_D void endsfree_init(int32_t* base, int L, int& lo, int& hi, int k) {
     G::sync();
+    const bool bt = PB && pgb;  // seeds start chains (endsfree_init_offset, :3421-3434)
     if (t0 >= k) {
       if (hi >= k) {
-        if (base[k - L] <= k) { G::sync(); if (lane == 0) base[k - L] = k; seed_flags |= 1; }
+        if (base[k - L] <= k) {
+          G::sync();
+          if (lane == 0) base[k - L] = k;
+          if (bt) bt_init_cell(base, k - L, 0, k);
+        }
       } else {
         for (int kk = hi + 1 + lane; kk < k; kk += LW) base[kk - L] = kOffsetNull;
+        if (bt) bt_zero(base, hi + 1 - L, k - 1 - L);
         if (lane == 0) base[k - L] = k;
-        seed_flags |= 1;
+        if (bt) bt_init_cell(base, k - L, 0, k);
         hi = k;
       }
     }
     G::sync();
     if (p0 >= k) {
       if (lo <= -k) {
-        if (base[-k - L] <= 0) { G::sync(); if (lane == 0) base[-k - L] = 0; seed_flags |= 2; }
+        if (base[-k - L] <= 0) {
+          G::sync();
+          if (lane == 0) base[-k - L] = 0;
+          if (bt) bt_init_cell(base, -k - L, k, 0);
+        }
       } else {
         if (lane == 0) base[-k - L] = 0;
-        seed_flags |= 2;
+        if (bt) bt_init_cell(base, -k - L, k, 0);
         for (int kk = -k + 1 + lane; kk < lo; kk += LW) base[kk - L] = kOffsetNull;
+        if (bt) bt_zero(base, -k + 1 - L, lo - 1 - L);
         lo = -k;
       }
     }
@@ -553,15 +701,21 @@ struct PairAligner {
     int32_t* v = alloc(CM, s, lo, hi);
     if (retry) return wf_none();
     for (int kk = lo + lane; kk <= hi; kk += LW) v[kk - lo] = kOffsetNull;
+    if (PB && pgb) bt_zero(v, 0, hi - lo);  // set_null_cell (:3454-3456)
     G::sync();
     if (lane == 0) {
       if (text) v[k - lo] = k;
       if (pattern) v[-k - lo] = 0;
     }
-    seed_flags |= (text ? 1 : 0) | (pattern ? 2 : 0);
+    if (PB && pgb) {
+      G::sync();
+      if (text) bt_init_cell(v, k - lo, 0, k);
+      if (pattern) bt_init_cell(v, -k - lo, k, 0);
+    }
     G::sync();
     WfD d;
-    d.vals = v; d.lo = lo; d.hi = hi; d.a = lo; d.b = hi; d.flags = kPresent; d.adub = kAdUnknown;
+    d.vals = v; d.lo = lo; d.hi = hi; d.a = lo; d.b = hi; d.flags = kPresent;
+    d.adub = PB && pgb ? 0 : kAdUnknown;  // a fresh wavefront's occupancy is 0
     return d;
   }
 
@@ -638,10 +792,186 @@ struct PairAligner {
       int32_t val = k == 0 ? 0 : (k > 0 ? k : 0);  // seeds: (h,0) on k=h, (0,v) on k=-v
       v[k - lo0] = val;
     }
+    if (PB && pgb) {
+      // Chains start at (0, 0), then at the text seeds (0, h), then at the
+      // pattern seeds (v, 0) (src/aligner.rs:962-992), numbered in that order.
+      bt_used = 0;
+      bi_used = 0;
+      const int cnt = 1 + (seeds ? t0 + p0 : 0);
+      if (cnt > P.bt_cap || cnt > P.bt_init_cap) { retry = true; return; }
+      for (int i = lane; i < cnt; i += LW) {
+        const int k = i == 0 ? 0 : i <= t0 ? i : -(i - t0);
+        ws.btinit[i] = int2{k < 0 ? -k : 0, k > 0 ? k : 0};
+        ws.bt[i] = uint2{(uint32_t)i, kBtNull};
+        pcs(v)[k - lo0] = 0;
+        pvs(v)[k - lo0] = (uint32_t)i;
+      }
+      bt_used = cnt;
+      bi_used = cnt;
+      cand_pc = 0; cand_pv = kBtNull; zd_pc = 0; zd_pv = kBtNull;
+    }
     G::sync();
     WfD d;
-    d.vals = v; d.lo = lo0; d.hi = hi0; d.a = lo0; d.b = hi0; d.flags = kPresent; d.adub = kAdUnknown;
+    d.vals = v; d.lo = lo0; d.hi = hi0; d.a = lo0; d.b = hi0; d.flags = kPresent;
+    d.adub = PB && pgb ? 0 : kAdUnknown;
     set_m(0, d);
+  }
+
+  // ---- med/low: compaction of the backtrace buffer ----------------------------
+  // compact_bt_buffer (src/components.rs:231-279): keep the blocks reachable
+  // from the live cells (offset >= 0) of the wavefronts still to be read and
+  // from the kept chains (the Corrected candidate and the Z-drop best), move
+  // them down in order, and translate the block indices of those cells and
+  // chains.  The wavefronts still to be read are M of the last dm scores
+  // that can hold one and I/D of the last d1 (d2), which own distinct cell
+  // slots of the compact ring (the reference walks every wavefront of the
+  // scope; the ones it adds are never read again).  The cells are those of
+  // the initialised range, which later kernels read: the reference walks the
+  // limits only, and a heuristic that narrows the limits leaves readable
+  // cells outside them whose chains it would lose.  So compaction never
+  // changes a result here.  ws.btmark: the mark bitmap, then the marked
+  // blocks before each of its words.
+  WFA_D void mark_chain(uint32_t idx) {
+    int32_t guard = 0;
+    while (idx != kBtNull && idx < (uint32_t)bt_used && guard++ <= bt_used) {
+      const uint32_t bit = 1u << (idx & 31);
+      if (G::atomic_or(&ws.btmark[idx >> 5], bit) & bit) return;
+      idx = ws.bt[idx].y;
+    }
+  }
+  WFA_D uint32_t moved_index(uint32_t idx, int nw) const {
+    return ws.btmark[nw + (idx >> 5)] + (uint32_t)Warp::popc(ws.btmark[idx >> 5] & ((1u << (idx & 31)) - 1u));
+  }
+  // The cells of component c at score t (a multiple of the score step back
+  // from the current one) whose chains compaction keeps; apply(pv) per cell.
+  template <class F>
+  WFA_D void live_cells(int c, int t, F&& apply) {
+    if (t < 0) return;
+    const WfD d = slot(c, t);
+    if (!wf_present(d) || d.a > d.b) return;
+    for (int k = d.a + lane; k <= d.b; k += LW)
+      if (d.vals[k - d.a] >= 0) apply(pvs(d.vals)[k - d.a]);
+  }
+  template <class F>
+  WFA_D void each_live_cell(F&& apply) {
+    const int base = cscore - gphase;  // the last score that can hold a wavefront
+    for (int j = 0; j < dm; ++j) live_cells(CM, base - j * gstep, apply);
+    if (AFF)
+      for (int j = 0; j < d1; ++j) {
+        live_cells(CI1, base - j * gstep, apply);
+        live_cells(CD1, base - j * gstep, apply);
+      }
+    if (TWO)
+      for (int j = 0; j < d2; ++j) {
+        live_cells(CI2, base - j * gstep, apply);
+        live_cells(CD2, base - j * gstep, apply);
+      }
+  }
+  WFA_D void compact_bt() {
+    const int nw = (bt_used + 31) >> 5;
+    for (int w = lane; w < nw; w += LW) ws.btmark[w] = 0;
+    G::sync();
+    each_live_cell([&](uint32_t& pv) { mark_chain(pv); });
+    if (lane == 0) {
+      if (c_has) mark_chain(cand_pv);
+      mark_chain(zd_pv);
+    }
+    G::sync();
+    if (lane == 0) {
+      uint32_t run = 0;
+      for (int w = 0; w < nw; ++w) {
+        ws.btmark[nw + w] = run;
+        run += (uint32_t)Warp::popc(ws.btmark[w]);
+      }
+    }
+    G::sync();
+    int32_t kept = 0;
+    for (int i0 = 0; i0 < bt_used; i0 += LW) {
+      const int i = i0 + lane;
+      const bool mk = i < bt_used && (ws.btmark[i >> 5] >> (i & 31) & 1u);
+      uint2 blk = uint2{0, 0};
+      uint32_t to = 0;
+      if (mk) {
+        blk = ws.bt[i];
+        if (blk.y != kBtNull) blk.y = moved_index(blk.y, nw);
+        to = moved_index((uint32_t)i, nw);
+      }
+      int total;
+      G::rank(mk, &total);  // every lane has read its block before any is written
+      if (mk) ws.bt[to] = blk;
+      kept += total;
+      G::sync();
+    }
+    each_live_cell([&](uint32_t& pv) { if (pv != kBtNull) pv = moved_index(pv, nw); });
+    // The kept chains are warp-uniform state: every lane translates them.
+    if (c_has && cand_pv != kBtNull) cand_pv = moved_index(cand_pv, nw);
+    if (zd_pv != kBtNull) zd_pv = moved_index(zd_pv, nw);
+    G::sync();
+    bt_used = kept;
+  }
+
+  // ---- med/low: the piggyback kernels' cells (src/compute/piggyback.rs) ------
+  // Each cell copies (pcigar, prev) from the input its kernel picks and pushes
+  // the operation taken.  Edit/linear (edit_kernel, :194-228): misms over del
+  // over ins on ties; indel (:249-273): del over ins.  wi: insertion input
+  // (cell k - 1), wx: mismatch input (cell k), wd: deletion input (cell k + 1).
+  WFA_D void pb_edit_cell(const WfD& wi, const WfD& wx, const WfD& wd, int32_t* out, int L, int k,
+                          bool indel) {
+    const int32_t ins = rd(wi, k - 1) + 1, del = rd(wd, k + 1);
+    uint32_t c, v;
+    if (indel) {
+      const bool d = imax(del, ins) == del;
+      c = d ? pc_push(rpc(wd, k + 1), kPcDel) : pc_push(rpc(wi, k - 1), kPcIns);
+      v = d ? rpv(wd, k + 1) : rpv(wi, k - 1);
+    } else {
+      const int32_t misms = rd(wx, k) + 1;
+      const int32_t mx = imax(del, imax(ins, misms));
+      const bool d = mx == del, x = mx == misms;
+      c = x ? pc_push(rpc(wx, k), kPcMisms) : d ? pc_push(rpc(wd, k + 1), kPcDel) : pc_push(rpc(wi, k - 1), kPcIns);
+      v = x ? rpv(wx, k) : d ? rpv(wd, k + 1) : rpv(wi, k - 1);
+    }
+    pcs(out)[k - L] = c;
+    pvs(out)[k - L] = v;
+  }
+  // A gap cell (`gap`, :146-170): the extension on a tie with the M opening.
+  struct PbGap {
+    int32_t off;
+    uint32_t c, v;
+  };
+  WFA_D PbGap pb_gap(const WfD& open, const WfD& ext, int kk, uint32_t op, int add) const {
+    const int32_t o = rd(open, kk), e = rd(ext, kk);
+    const bool x = e >= o;
+    return PbGap{(x ? e : o) + add, pc_push(x ? rpc(ext, kk) : rpc(open, kk), op), x ? rpv(ext, kk) : rpv(open, kk)};
+  }
+  // Affine / two-piece affine (affine_kernel :364-392, affine2p_kernel
+  // :483-527): I and D from their gaps; M takes misms, else D2, D1, I2, I1
+  // (later checks win ties) and pushes an X (the gap close) on the chain.
+  WFA_D void pb_affine_cell(const WfD& mm, const WfD& mo1, const WfD& i1e, const WfD& d1e, const WfD& mo2,
+                            const WfD& i2e, const WfD& d2e, bool two, int32_t* om, int L, int32_t* oi1,
+                            int32_t* od1, int32_t* oi2, int32_t* od2, int lo, int k) {
+    const PbGap i1 = pb_gap(mo1, i1e, k - 1, kPcIns, 1), d1 = pb_gap(mo1, d1e, k + 1, kPcDel, 0);
+    pcs(oi1)[k - lo] = i1.c; pvs(oi1)[k - lo] = i1.v;
+    pcs(od1)[k - lo] = d1.c; pvs(od1)[k - lo] = d1.v;
+    const int32_t misms = rd(mm, k) + 1;
+    int32_t mx;
+    uint32_t c, v;
+    if (!two) {
+      mx = imax(d1.off, imax(misms, i1.off));
+      const bool d = mx == d1.off;
+      c = d ? d1.c : i1.c;
+      v = d ? d1.v : i1.v;
+    } else {
+      const PbGap i2 = pb_gap(mo2, i2e, k - 1, kPcIns, 1), d2 = pb_gap(mo2, d2e, k + 1, kPcDel, 0);
+      pcs(oi2)[k - lo] = i2.c; pvs(oi2)[k - lo] = i2.v;
+      pcs(od2)[k - lo] = d2.c; pvs(od2)[k - lo] = d2.v;
+      mx = imax(imax(imax(i1.off, i2.off), imax(d1.off, d2.off)), misms);
+      const bool s2 = mx == i2.off, t1 = mx == d1.off, t2 = mx == d2.off;
+      c = t2 ? d2.c : t1 ? d1.c : s2 ? i2.c : i1.c;
+      v = t2 ? d2.v : t1 ? d1.v : s2 ? i2.v : i1.v;
+    }
+    const bool x = mx == misms;
+    pcs(om)[k - L] = pc_push(x ? rpc(mm, k) : c, kPcMisms);
+    pvs(om)[k - L] = x ? rpv(mm, k) : v;
   }
 
   // ---- compute steps ----------------------------------------------------------
@@ -656,9 +986,12 @@ struct PairAligner {
     // initialised range only; outside it they already read as NULL).
     if (lane == 0) {
       int ks[4] = {prev.lo - 2, prev.lo - 1, prev.hi + 1, prev.hi + 2};
-      int4 hr = modular ? int4{0, -1, 0, 0} : ws.hist[(int64_t)(s - 1) * hist_nc];
+      int4 hr = modular || (PB && pgb) ? int4{0, -1, 0, 0} : ws.hist[(int64_t)(s - 1) * hist_nc];
       for (int i = 0; i < 4; ++i) {
-        if (ks[i] >= prev.a && ks[i] <= prev.b) prev.vals[ks[i] - prev.a] = kOffsetNull;
+        if (ks[i] >= prev.a && ks[i] <= prev.b) {
+          prev.vals[ks[i] - prev.a] = kOffsetNull;
+          if (PB && pgb) { pcs(prev.vals)[ks[i] - prev.a] = 0; pvs(prev.vals)[ks[i] - prev.a] = 0; }
+        }
         if (hr.w && ks[i] >= hr.x && ks[i] <= hr.y) ws.harena[hr.z + ks[i] - hr.x] = kOffsetNull;
       }
     }
@@ -671,9 +1004,16 @@ struct PairAligner {
       int32_t ins = rd(prev, k - 1), del = rd(prev, k + 1), mx;
       if (indel) mx = imax(del, ins + 1);
       else mx = imax(del, imax(ins, rd(prev, k)) + 1);
+      if (PB && pgb) pb_edit_cell(prev, prev, prev, out, lo, k, indel);
       if (!cell_in_bounds(mx, k, n, m)) mx = kOffsetNull;
       out[k - lo] = mx;
       if (mx != kOffsetNull) { vmin = imin(vmin, k); vmax = imax(vmax, k); }
+    }
+    // C offloads edit/indel every PCIGAR_MAX_LENGTH scores (src/aligner.rs:1848-1852).
+    if (PB && pgb && s % kPcMaxLength == 0) {
+      G::sync();
+      offload_linear_cells(out, lo, lo, hi);
+      if (retry) return;
     }
     vmin = G::min(vmin);
     vmax = G::max(vmax);
@@ -703,22 +1043,33 @@ struct PairAligner {
     int L = bf ? imin(lo, -bk) : lo, H = bf ? imax(hi, bk) : hi;
     int32_t* out = alloc(CM, s, L, H);
     if (retry) return;
+    int32_t lin_occ = 0;
     int vmin = INT_MAX, vmax = INT_MIN;
     for (int k = lo + lane; k <= hi; k += LW) {
       int32_t a = rd(mi, k) + 1, ins = rd(gp, k - 1) + 1, del = rd(gp, k + 1);
       int32_t mx = imax(del, imax(ins, a));
+      if (PB && pgb) pb_edit_cell(gp, mi, gp, out, L, k, false);
       if (!cell_in_bounds(mx, k, n, m)) mx = kOffsetNull;
       out[k - L] = mx;
       if (mx != kOffsetNull) { vmin = imin(vmin, k); vmax = imax(vmax, k); }
     }
+    if (PB && pgb) {  // offload_linear (src/compute/piggyback.rs:590-607)
+      G::sync();
+      lin_occ = imax(occ_of(gp), occ_of(mi)) + 1;
+      if (lin_occ >= kPcMaxLength) lin_occ = offload_linear_cells(out, L, lo, hi);
+      if (retry) return;
+    }
+    WfD r;
     if (bf) {
       endsfree_init(out, L, lo, hi, bk);
-      set_m(s, trim_pass(out, L, lo, hi));
+      r = trim_pass(out, L, lo, hi);
     } else {
       vmin = G::min(vmin);
       vmax = G::max(vmax);
-      set_m(s, finish(out, L, lo, hi, vmin, vmax));
+      r = finish(out, L, lo, hi, vmin, vmax);
     }
+    if (PB && pgb) r.adub = lin_occ;
+    set_m(s, r);
   }
 
   // compute_affine_step (src/aligner.rs:2006-2193) and compute_affine2p_step
@@ -821,6 +1172,8 @@ struct PairAligner {
           if (cell_in_bounds(i2, k, n, m)) { mn_i2 = imin(mn_i2, k); mx_i2 = imax(mx_i2, k); }
           if (cell_in_bounds(d2, k, n, m)) { mn_d2 = imin(mn_d2, k); mx_d2 = imax(mx_d2, k); }
         }
+        if (PB && pgb)
+          pb_affine_cell(mm, mo1, i1e, d1e, mo2, i2e, d2e, two, om, L, oi1, od1, oi2, od2, lo, k);
         if (!cell_in_bounds(mx, k, n, m)) mx = kOffsetNull;
         om[k - L] = mx;
         oi1[k - lo] = i1;
@@ -830,10 +1183,36 @@ struct PairAligner {
         if (cell_in_bounds(d1, k, n, m)) { mn_d1 = imin(mn_d1, k); mx_d1 = imax(mx_d1, k); }
       }
     }
+    // Med/low: occupancies and offload (offload_affine / offload_affine2p,
+    // src/compute/piggyback.rs:635-705), before the trims as the reference.
+    int32_t o_m = 0, o_i1 = 0, o_d1 = 0, o_i2 = 0, o_d2 = 0;
+    if (PB && pgb) {
+      G::sync();
+      o_i1 = occ_gap(mo1, i1e);
+      o_d1 = occ_gap(mo1, d1e);
+      o_m = imax(occ_of(mm), imax(o_i1, o_d1));
+      if (two) {
+        o_i2 = occ_gap(mo2, i2e);
+        o_d2 = occ_gap(mo2, d2e);
+        o_m = imax(o_m, imax(o_i2, o_d2));
+      }
+      o_m = offload_component(om, L, lo, hi, o_m + 1);
+      o_i1 = offload_component(oi1, lo, lo, hi, o_i1);
+      o_d1 = offload_component(od1, lo, lo, hi, o_d1);
+      if (two) {
+        o_i2 = offload_component(oi2, lo, lo, hi, o_i2);
+        o_d2 = offload_component(od2, lo, lo, hi, o_d2);
+      }
+      if (retry) return;
+    }
     mn_i1 = G::min(mn_i1); mx_i1 = G::max(mx_i1);
     mn_d1 = G::min(mn_d1); mx_d1 = G::max(mx_d1);
-    put_ns(CI1, s, finish(oi1, lo, lo, hi, mn_i1, mx_i1));
-    put_ns(CD1, s, finish(od1, lo, lo, hi, mn_d1, mx_d1));
+    WfD r = finish(oi1, lo, lo, hi, mn_i1, mx_i1);
+    if (PB && pgb) r.adub = o_i1;
+    put_ns(CI1, s, r);
+    r = finish(od1, lo, lo, hi, mn_d1, mx_d1);
+    if (PB && pgb) r.adub = o_d1;
+    put_ns(CD1, s, r);
     if (TWO) {
       if (affine_kernel) {
         put_ns(CI2, s, wf_none());
@@ -841,18 +1220,24 @@ struct PairAligner {
       } else {
         mn_i2 = G::min(mn_i2); mx_i2 = G::max(mx_i2);
         mn_d2 = G::min(mn_d2); mx_d2 = G::max(mx_d2);
-        put_ns(CI2, s, finish(oi2, lo, lo, hi, mn_i2, mx_i2));
-        put_ns(CD2, s, finish(od2, lo, lo, hi, mn_d2, mx_d2));
+        r = finish(oi2, lo, lo, hi, mn_i2, mx_i2);
+        if (PB && pgb) r.adub = o_i2;
+        put_ns(CI2, s, r);
+        r = finish(od2, lo, lo, hi, mn_d2, mx_d2);
+        if (PB && pgb) r.adub = o_d2;
+        put_ns(CD2, s, r);
       }
     }
     if (bf) {
       int mlo = lo, mhi = hi;
       endsfree_init(om, L, mlo, mhi, bk);
-      set_m(s, trim_pass(om, L, mlo, mhi));
+      r = trim_pass(om, L, mlo, mhi);
     } else {
       mn_m = G::min(mn_m); mx_m = G::max(mx_m);
-      set_m(s, finish(om, L, lo, hi, mn_m, mx_m));
+      r = finish(om, L, lo, hi, mn_m, mx_m);
     }
+    if (PB && pgb) r.adub = o_m;
+    set_m(s, r);
   }
 
 
@@ -1001,6 +1386,7 @@ struct PairAligner {
   }
 
   WFA_D void compute_step(int s) {
+    if (PB && pgb) mbase = nullptr;  // set again if this score allocates an M
     if (CLS == kEditClass) compute_edit(s);
     else if (CLS == kLinearClass) compute_linear(s);
     else compute_affine(s);
@@ -1126,6 +1512,7 @@ struct PairAligner {
         const int total = score + (-P.match) * left;
         if (!c_has || total < c_total) {
           c_has = true; c_total = total; c_score = score; c_k = k; c_off = off;
+          if (pgb) m_bt(k, cand_pc, cand_pv);  // the candidate's chain (src/aligner.rs:1155-1160)
           if (prune && total > score) ef_prune(score, total);
         }
       }
@@ -1322,7 +1709,11 @@ struct PairAligner {
     WfD d = slot(CM, score);
     if (hk() == WFA_HEURISTIC_BANDED_STATIC && d.lo >= hp0 && d.hi <= hp1) return false;
     int lo_base = d.lo, hi_base = d.hi;
+    const int32_t max_wf_base = hs.max_wf_score;
     bool z = heuristic_cutoff(d, score);
+    // Corrected med/low keep the chain of a new Z-drop best cell (src/aligner.rs:1677-1688).
+    if (PB && pgb && P.compat == WFA_COMPAT_CORRECTED && hs.max_wf_score == score && max_wf_base != score)
+      m_bt(hs.max_sw_k, zd_pc, zd_pv);
     if (z) {
       end_score = hs.max_wf_score; end_k = hs.max_sw_k; end_off = hs.max_sw_off;
       return true;
@@ -1716,68 +2107,6 @@ struct PairAligner {
     run('I', h);
   }
 
-  // ---- med/low: the piggyback backtrace ----------------------------------------
-  // The reference's med/low kernels (src/compute/piggyback.rs) carry each
-  // cell's backtrace along, copied from the predecessor the kernel picked;
-  // here every component's history is kept and the same picks are re-made
-  // from it, walking back from the end cell.
-  //
-  // Offset of (c, s, k) as the compute kernels read it (absent wavefronts
-  // and cells outside the stored range read as NULL).
-  WFA_D int32_t pv(int c, int s, int k) const {
-    if (s < 0) return kOffsetNull;
-    int4 r = ws.hist[(int64_t)s * hist_nc + c];
-    if (!(r.w & 1) || k < r.x || k > r.y) return kOffsetNull;
-    return ws.harena[r.z + (k - r.x)];
-  }
-  // The begin-free seed endsfree_init placed at M cell (s, k).
-  WFA_D bool pb_seed(int s, int k) const {
-    if (P.match >= 0 || s <= 0) return false;
-    int fl = ws.hist[(int64_t)s * hist_nc + CM].w >> 1;
-    if (!fl) return false;
-    int bk = s / (-P.match);
-    return ((fl & 1) && k == bk) || ((fl & 2) && k == -bk);
-  }
-  struct PbStep {
-    uint8_t op;
-    int c, s, k;
-  };
-  // The predecessor cell (c, s, k)'s kernel copied its backtrace from, and
-  // the operation it pushed (src/compute/piggyback.rs:172-528): edit and
-  // linear take misms over del over ins, indel del over ins; a gap cell
-  // takes its extension over the M opening on a tie (:146-170); affine M
-  // takes misms, else D2, D1, I2, I1, pushing an X (the gap close) on top of
-  // the gap's chain.
-  WFA_D PbStep pb_pred(int c, int s, int k) const {
-    if (!AFF) {
-      const int gs = s - P.o1;
-      const int32_t ins = pv(CM, gs, k - 1) + 1, del = pv(CM, gs, k + 1);
-      if (P.metric == WFA_METRIC_INDEL)
-        return imax(del, ins) == del ? PbStep{'D', CM, gs, k + 1} : PbStep{'I', CM, gs, k - 1};
-      const int ms = s - P.mismatch;
-      const int32_t misms = pv(CM, ms, k) + 1;
-      const int32_t mx = imax(del, imax(ins, misms));
-      if (mx == misms) return PbStep{'X', CM, ms, k};
-      return mx == del ? PbStep{'D', CM, gs, k + 1} : PbStep{'I', CM, gs, k - 1};
-    }
-    if (c != CM) {
-      const bool ins = c == CI1 || c == CI2, p2 = c == CI2 || c == CD2;
-      const int o = p2 ? P.o2 : P.o1, e = p2 ? P.e2 : P.e1;
-      const int kk = ins ? k - 1 : k + 1;
-      const uint8_t op = ins ? 'I' : 'D';
-      const int32_t open = pv(CM, s - o - e, kk), ext = pv(c, s - e, kk);
-      return ext >= open ? PbStep{op, c, s - e, kk} : PbStep{op, CM, s - o - e, kk};
-    }
-    const int32_t i1 = pv(CI1, s, k), d1 = pv(CD1, s, k);
-    const int32_t i2 = TWO ? pv(CI2, s, k) : kOffsetNull, d2 = TWO ? pv(CD2, s, k) : kOffsetNull;
-    const int32_t misms = pv(CM, s - P.mismatch, k) + 1;
-    const int32_t mx = imax(imax(misms, imax(i1, d1)), imax(i2, d2));
-    if (mx == misms) return PbStep{'X', CM, s - P.mismatch, k};
-    if (TWO && mx == d2) return PbStep{'X', CD2, s, k};
-    if (mx == d1) return PbStep{'X', CD1, s, k};
-    if (TWO && mx == i2) return PbStep{'X', CI2, s, k};
-    return PbStep{'X', CI1, s, k};
-  }
   // Forward CIGAR writes of the unpack: at most `limit` (exclusive) -- the
   // chain operations not yet read sit above it in the same slot.
   WFA_D bool fwd(int64_t& p, int64_t limit, uint8_t op, int cnt) {
@@ -1787,72 +2116,110 @@ struct PairAligner {
     p += cnt;
     return true;
   }
-  // backtrace_piggyback + backtrace_piggyback_bt (src/aligner.rs:1443-1485)
-  // and unpack_piggyback (:232-311): the chain of M cell (score, k) back to
-  // its begin -- score 0, or a begin-free seed at (0, k) / (-k, 0) -- then
-  // unpacked forwards: begin-free I/D, the operations with matches
-  // re-extended before each one (only in M when affine, where an X after I/D
-  // is the gap close and is dropped), matches to the end cell, I/D to the
-  // sequence ends.  The chain is stored backwards from the slot's end and
-  // read in order while the CIGAR is written from the slot's start.
-  WFA_D void backtrace_piggyback(int score, int k, int offset) {
-    cg_begin = 0;
-    cg_end = 0;
-    if (score < 0) return;
-    {
-      int4 r = ws.hist[(int64_t)score * hist_nc + CM];
-      if (!(r.w & 1) || k < r.x || k > r.y) return;  // no such end cell: no CIGAR
-    }
-    int64_t rd = cg_cap;
-    int c = CM, s = score, kk = k, bv = 0, bh = 0;
-    // A dead cell ends the chain with the zero backtrace (no operations, from
-    // (0, 0)): the kernels never build it from a live predecessor.
-    while (pv(c, s, kk) >= 0) {
-      if (c == CM && (s == 0 || pb_seed(s, kk))) {
-        bv = kk < 0 ? -kk : 0;
-        bh = kk > 0 ? kk : 0;
-        break;
-      }
-      const PbStep st = pb_pred(c, s, kk);
-      if (rd == 0) { status = WFA_STATUS_OOM; return; }
-      --rd;
-      if (lane == 0) cg[rd] = st.op;
-      c = st.c; s = st.s; kk = st.k;
-    }
-    G::sync();
+  // ---- med/low: the chain of packed CIGARs -------------------------------------
+  // backtrace_piggyback_bt (src/aligner.rs:1463-1486): traceback_from
+  // (src/bt_buffer.rs:196-212) collects the chain's packed CIGARs back to
+  // its initial block; unpack_piggyback (src/aligner.rs:232-311) then spells
+  // them from the first.  The end cell's own packed CIGAR stays in a
+  // register; the offloaded blocks (each of at least 9 operations: only
+  // packed CIGARs at least half full are offloaded) are stored 4 bytes each
+  // backwards from the end of the pair's CIGAR slot and read from the first
+  // while the CIGAR is written forwards from the slot's start: at most
+  // 2 (n + m) / 9 blocks take less than the (n + m + 1) bytes the CIGAR
+  // leaves free, so the unread blocks always lie above the write point.
+  WFA_D uint32_t cg_word(int64_t i) const {
+    return (uint32_t)cg[i] | ((uint32_t)cg[i + 1] << 8) | ((uint32_t)cg[i + 2] << 16) | ((uint32_t)cg[i + 3] << 24);
+  }
+  // The operations of one packed CIGAR, matches re-extended before each
+  // (only in M when affine, where an X after I/D is the gap close and is
+  // dropped); writes below `limit`.
+  WFA_D bool unpack_block(uint32_t pcig, int64_t& p, int64_t limit, int& v, int& h, bool& in_m) {
     const bool affine = AFF;
-    int64_t p = 0;
-    int v = bv, h = bh;
-    if (!fwd(p, rd, 'I', h) || !fwd(p, rd, 'D', v)) return;
-    bool in_m = true;
-    for (int64_t i = rd; i < cg_cap; ++i) {
-      const uint8_t op = cg[i];
-      G::sync();  // every lane has read cg[i] before it may be overwritten
+    int length = kPcMaxLength;
+    if (pcig < kPcFullMask) {
+      const int fr = pcig ? (int)Warp::clz(pcig) / 2 : kPcMaxLength;
+      length -= fr;
+      pcig = fr >= kPcMaxLength ? 0u : pcig << (2 * fr);
+    }
+    for (int j = 0; j < length; ++j) {
       if (in_m || !affine) {
         const int nm = lcp_fwd(pat, v, txt, h, imax(0, imin(n - v, m - h)));
-        if (!fwd(p, i + 1, 'M', nm)) return;
+        if (!fwd(p, limit, 'M', nm)) return false;
         v += nm;
         h += nm;
       }
-      if (affine && !in_m && op == 'X') { in_m = true; continue; }
-      if (!fwd(p, i + 1, op, 1)) return;
-      if (op == 'D') { ++v; in_m = false; }
-      else if (op == 'I') { ++h; in_m = false; }
-      else { ++v; ++h; in_m = true; }
+      const uint32_t op = pcig >> 30;
+      pcig <<= 2;
+      const uint8_t ch = op == kPcDel ? 'D' : op == kPcMisms ? 'X' : op == kPcIns ? 'I' : '?';
+      if (affine && !in_m && ch == 'X') { in_m = true; continue; }
+      if (!fwd(p, limit, ch, 1)) return false;
+      v += (op == kPcDel || op == kPcMisms) ? 1 : 0;
+      h += (op == kPcIns || op == kPcMisms) ? 1 : 0;
+      in_m = op == kPcMisms || op == 0;
     }
+    return true;
+  }
+  WFA_D void backtrace_pb(uint32_t pc, uint32_t pv, int score, int k, int offset) {
+    cg_begin = 0;
+    cg_end = 0;
+    cg_score = score;
+    const uint32_t end_pc = pc;
+    int64_t rdp = cg_cap;
+    int32_t guard = 0;
+    uint32_t init = 0;
+    for (;;) {
+      if (pv == kBtNull || ++guard > bt_used + 1) { status = WFA_STATUS_OOM; return; }
+      const uint2 blk = ws.bt[pv];
+      if (blk.y == kBtNull) { init = blk.x; break; }  // the initial block: its position's index
+      if (rdp < 4) { status = WFA_STATUS_OOM; return; }
+      rdp -= 4;
+      if (lane == 0)
+        for (int b = 0; b < 4; ++b) cg[rdp + b] = (uint8_t)(blk.x >> (8 * b));
+      pv = blk.y;
+    }
+    G::sync();
+    const int2 ip = ws.btinit[init];
+    int64_t p = 0;
+    int v = ip.x, h = ip.y;
+    if (!fwd(p, rdp, 'I', h) || !fwd(p, rdp, 'D', v)) return;
+    bool in_m = true;
+    for (int64_t b = rdp; b < cg_cap; b += 4) {
+      const uint32_t pcig = cg_word(b);
+      G::sync();  // every lane has read the block before it may be overwritten
+      if (!unpack_block(pcig, p, b + 4, v, h, in_m)) return;
+    }
+    if (!unpack_block(end_pc, p, cg_cap, v, h, in_m)) return;
+    // As the reference, a negative count (end behind the unpacked position) moves back.
     const int nm = imin(offset - k - v, offset - h);
     if (!fwd(p, cg_cap, 'M', nm)) return;
-    v += nm;  // as the reference: a negative count moves back
+    v += nm;
     h += nm;
     if (!fwd(p, cg_cap, 'I', m - h) || !fwd(p, cg_cap, 'D', n - v)) return;
     cg_end = p;
   }
+  // The end cell of the current score's M (backtrace_piggyback,
+  // src/aligner.rs:1443-1459): no CIGAR without an M at that score.
+  WFA_D void backtrace_pb_current(int score, int k, int offset) {
+    if (!mbase) { cg_begin = 0; cg_end = 0; cg_score = score; return; }
+    uint32_t c, v;
+    m_bt(k, c, v);
+    backtrace_pb(c, v, score, k, offset);
+  }
+  // The Z-drop end (backtrace_zdrop_end, :1393-1411).
+  WFA_D void backtrace_zdrop(int score) {
+    if (PB && pgb && P.compat == WFA_COMPAT_CORRECTED) {
+      G::sync();
+      backtrace_pb(zd_pc, zd_pv, end_score, end_k, end_off);
+      G::sync();
+      return;
+    }
+    backtrace_from(zdrop_from(score), end_k, end_off);
+  }
 
   WFA_D void backtrace_from(int score, int k, int offset) {  // src/aligner.rs:1414-1436
     G::sync();
-    if (GEN && pgb) {
-      backtrace_piggyback(score, k, offset);
-      cg_score = score;
+    if (PB && pgb) {
+      backtrace_pb_current(score, k, offset);
       G::sync();
       return;
     }
@@ -2015,7 +2382,7 @@ struct PairAligner {
   // reads every mode at the best cell's score.
   WFA_D int zdrop_from(int score) const {
     if (GEN && P.compat == WFA_COMPAT_CORRECTED) return end_score;
-    return end_score >= 0 && !(GEN && pgb) ? end_score : score;
+    return end_score >= 0 && !(PB && pgb) ? end_score : score;
   }
 
   // ---- one pair: align_end2end_span (src/aligner.rs:638-698) and
@@ -2050,7 +2417,7 @@ struct PairAligner {
           done = !(GEN && corr && c_has) && num_null_steps > scope;
           if (done) status = WFA_STATUS_END_UNREACHABLE;
         }
-        if (!modular) {
+        if (!modular && !(PB && pgb)) {
           if ((int64_t)(score + 1) * hist_nc > P.hist_scores) { retry = true; break; }
           if (lane == 0)
             for (int c = 0; c < hist_nc; ++c) ws.hist[(int64_t)score * hist_nc + c] = int4{1, 0, 0, 0};
@@ -2065,10 +2432,21 @@ struct PairAligner {
       gphase = gphase + 1 == gstep ? 0 : gphase + 1;
       if (!has_slot(score)) { status = WFA_STATUS_MAX_STEPS_REACHED; break; }
       const bool computed = gphase == 0;
-      if (computed) compute_step(score);
-      else ++num_null_steps;
+      if (computed) {
+        compute_step(score);
+      } else {
+        ++num_null_steps;
+        if (PB && pgb) mbase = nullptr;
+      }
       if (retry) break;
       if (score >= P.max_steps || score >= hard_limit) { status = WFA_STATUS_MAX_STEPS_REACHED; break; }
+      // probe_bt_buffer (src/aligner.rs:479-513): compact the backtrace
+      // buffer every PROBE_INTERVAL_COMPACT scores while it holds more than
+      // max_memory_compact bytes (8 per block).
+      if (PB && pgb && score % P.bt_probe == 0 && (int64_t)bt_used * 8 > P.bt_limit) {
+        compact_bt();
+        if (retry) break;
+      }
       if (computed) { cur = score; return false; }
     }
     cur = score;
@@ -2098,7 +2476,7 @@ struct PairAligner {
         if (status != WFA_STATUS_OOM) status = WFA_STATUS_COMPLETED;
       } else if (status == WFA_STATUS_END_UNREACHABLE && end_off != kOffsetNull) {
         if (cigar) {
-          backtrace_from(zdrop_from(score), end_k, end_off);
+          backtrace_zdrop(score);
           maxtrim_cigar();
         }
         if (status != WFA_STATUS_OOM) status = WFA_STATUS_PARTIAL;
@@ -2110,9 +2488,17 @@ struct PairAligner {
       const bool cand = GEN && corr && c_has && !unreachable;
       if (cand) result = c_total;
       if (cigar && (status == WFA_STATUS_END_REACHED || end_off != kOffsetNull)) {
-        if (cand) backtrace_from(c_score, c_k, c_off);
-        else if (unreachable) backtrace_from(zdrop_from(score), end_k, end_off);
-        else backtrace_from(score, end_k, end_off);
+        if (cand && PB && pgb) {
+          G::sync();
+          backtrace_pb(cand_pc, cand_pv, c_score, c_k, c_off);
+          G::sync();
+        } else if (cand) {
+          backtrace_from(c_score, c_k, c_off);
+        } else if (unreachable) {
+          backtrace_zdrop(score);
+        } else {
+          backtrace_from(score, end_k, end_off);
+        }
         if (cand) cg_score = c_total;
         if (status == WFA_STATUS_OOM) return result;
         if (P.extension || unreachable) {
@@ -2134,8 +2520,8 @@ struct PairAligner {
 
 // Per-pair set-up of an aligner A (its workspace and lane already set) for
 // pair `pair` of the launch.
-template <int CLS, class S, bool GEN, int LW>
-WFA_D void setup_pair(PairAligner<CLS, S, GEN, 1, LW>& A, const AlignParams& P, int64_t pair, S pat,
+template <int CLS, class S, bool GEN, int LW, bool PB>
+WFA_D void setup_pair(PairAligner<CLS, S, GEN, 1, LW, PB>& A, const AlignParams& P, int64_t pair, S pat,
                       S txt) {
   A.pat = pat;
   A.txt = txt;
@@ -2145,12 +2531,17 @@ WFA_D void setup_pair(PairAligner<CLS, S, GEN, 1, LW>& A, const AlignParams& P, 
   A.wmax = P.wmax;
   A.compact = P.ring_slots > 0;
   A.modular = P.compute_alignment == 0;
-  A.pgb = GEN && !A.modular && P.piggyback != 0;
+  A.pgb = PB && !A.modular && P.piggyback != 0;
   // Med/low components are modular: no score cap.
   A.cap = A.modular || A.pgb ? INT_MAX : imax(A.dims_num(1000, 1000), A.dims_num(A.n, A.m));
   A.endsfree = P.span == WFA_SPAN_ENDSFREE;
   A.hkind = P.hkind; A.hp0 = P.hp0; A.hp1 = P.hp1; A.hp2 = P.hp2;
-  A.hist_nc = A.pgb ? PairAligner<CLS, S, GEN, 1, LW>::NC : 1;
+  A.hist_nc = 1;
+  // Med/low: each cell's pcigar and block index sit ring_slots x wmax and
+  // twice that many words after its offset (the ring lies in the scratch
+  // slice, three arrays of the same shape).
+  A.pcoff = (int64_t)P.ring_slots * P.wmax;
+  A.mbase = nullptr;
   A.keep_null_slots = false;
   A.comp_end = CM;
   if (P.extension) { A.p0 = 0; A.pf = A.n; A.t0 = 0; A.tf = A.m; }
@@ -2165,8 +2556,8 @@ WFA_D void setup_pair(PairAligner<CLS, S, GEN, 1, LW>& A, const AlignParams& P, 
 }
 
 // The result record of an aligned pair (lane 0 of the group writes it).
-template <int CLS, class S, bool GEN, int LW>
-WFA_D void write_result(const PairAligner<CLS, S, GEN, 1, LW>& A, const AlignParams& P, int64_t pair,
+template <int CLS, class S, bool GEN, int LW, bool PB>
+WFA_D void write_result(const PairAligner<CLS, S, GEN, 1, LW, PB>& A, const AlignParams& P, int64_t pair,
                         int32_t score) {
   if (A.lane == 0) {
     wfa_result_t r;
@@ -2187,9 +2578,9 @@ WFA_D void write_result(const PairAligner<CLS, S, GEN, 1, LW>& A, const AlignPar
 
 // Set up and align pair `pair` of the launch with workspace `ws`, writing
 // its result.  Returns true if the pair must be retried with more scratch.
-template <int CLS, class S, bool GEN = true, int LW = WFA_WARP>
+template <int CLS, class S, bool GEN = true, int LW = WFA_WARP, bool PB = false>
 WFA_D bool align_one(const AlignParams& P, const Workspace& ws, int64_t pair, S pat, S txt) {
-  PairAligner<CLS, S, GEN, 1, LW> A(P);
+  PairAligner<CLS, S, GEN, 1, LW, PB> A(P);
   A.ws = ws;
   A.lane = Lanes<LW>::lane();
   setup_pair(A, P, pair, pat, txt);

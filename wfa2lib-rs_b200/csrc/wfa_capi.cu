@@ -63,6 +63,7 @@ struct DevBuf {
 struct ScratchCfg {
   int32_t wmax;
   int32_t ring_slots = 0;  // compact ring slots (0: one per score and component)
+  int32_t bt_cap = 0, bt_init_cap = 0;  // med/low backtrace buffer (blocks, initial positions)
   int32_t hist_scores;
   int64_t hist_words;
   int64_t dom_words = 0;  // Corrected-mode dominance array per warp
@@ -110,6 +111,7 @@ struct wfa_aligner {
   int lanes_forced = 0;  // lanes per pair of the lean kernel (0: autotuned)
   int last_lanes = 0;    // lanes per pair of the last batch's first round
   int launch_lanes = 0;  // lanes per pair of the last launch
+  int64_t last_slice_bytes = 0;  // one lane group's scratch slice in the last launch
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_kernel_ms = 0.0;
   int64_t last_reruns = 0;  // pair re-runs (larger scratch) of the last call
@@ -156,6 +158,7 @@ static cudaError_t host_info(wfa_aligner_t* h, size_t words) {
 struct ChunkInfo {
   int64_t lo = INT64_MAX, hi = 0;
   int32_t max_len_sum = 0;
+  int32_t max_seq = 0;  // longest single sequence
   int64_t slots = 0;
 };
 static void scan_chunks(const wfa_batch_t* b, int64_t n, const std::vector<int64_t>& bnd, bool packed,
@@ -169,7 +172,7 @@ static void scan_chunks(const wfa_batch_t* b, int64_t n, const std::vector<int64
       const int64_t e = std::min(i1, bnd[(size_t)ci + 1]);
       ChunkInfo& c = acc[(size_t)ci];
       int64_t lo = c.lo, hi = c.hi, slots = c.slots;
-      int32_t mx = c.max_len_sum;
+      int32_t mx = c.max_len_sum, ms = c.max_seq;
       for (; i < e; ++i) {
         const int64_t pl = b->p_len[i], tl = b->t_len[i], po = b->p_off[i], to = b->t_off[i];
         const int64_t pe = packed ? (po + (pl + 15) / 16) * 4 : po + pl;
@@ -177,9 +180,10 @@ static void scan_chunks(const wfa_batch_t* b, int64_t n, const std::vector<int64
         lo = std::min(lo, std::min(po, to) * unit);
         hi = std::max(hi, std::max(pe, te));
         mx = std::max<int32_t>(mx, (int32_t)(pl + tl));
+        ms = std::max<int32_t>(ms, (int32_t)std::max(pl, tl));
         slots += 2 * (pl + tl) + 1;
       }
-      c.lo = lo; c.hi = hi; c.slots = slots; c.max_len_sum = mx;
+      c.lo = lo; c.hi = hi; c.slots = slots; c.max_len_sum = mx; c.max_seq = ms;
     }
   };
   const int64_t kPerThread = 131072;
@@ -200,6 +204,7 @@ static void scan_chunks(const wfa_batch_t* b, int64_t n, const std::vector<int64
       c.lo = std::min(c.lo, p.lo);
       c.hi = std::max(c.hi, p.hi);
       c.max_len_sum = std::max(c.max_len_sum, p.max_len_sum);
+      c.max_seq = std::max(c.max_seq, p.max_seq);
       c.slots += p.slots;
     }
     c.lo = c.lo == INT64_MAX ? 0 : (c.lo & ~(int64_t)15);
@@ -351,12 +356,20 @@ static cudaError_t chunk_scan(const int32_t* pl, const int32_t* tl, const wfa_re
   return cudaGetLastError();
 }
 
+// out[0]: the longest n + m of a batch; out[1]: its longest sequence.
 __global__ void max_lengths(const int32_t* pl, const int32_t* tl, int64_t n, int32_t* out) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  int32_t v = 0;
-  for (; i < n; i += (int64_t)gridDim.x * blockDim.x) v = max(v, pl[i] + tl[i]);
+  int32_t v = 0, w = 0;
+  for (; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    v = max(v, pl[i] + tl[i]);
+    w = max(w, max(pl[i], tl[i]));
+  }
   v = __reduce_max_sync(0xffffffffu, v);
-  if ((threadIdx.x & 31) == 0) atomicMax(out, v);
+  w = __reduce_max_sync(0xffffffffu, w);
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(out, v);
+    atomicMax(out + 1, w);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -375,8 +388,11 @@ static void fill_params(const wfa_aligner_t* h, const wfa_batch_t* b, AlignParam
   P.hkind = h->hkind; P.hp0 = h->hp0; P.hp1 = h->hp1; P.hp2 = h->hp2;
   P.compute_alignment = h->scope == WFA_SCOPE_ALIGNMENT;
   // Med/low with an alignment: the piggyback backtrace (BiWFA ignores the mode).
-  P.piggyback = P.compute_alignment && h->memory_mode != WFA_MEMORY_HIGH &&
-                b->span != WFA_SPAN_BIWFA;
+  P.piggyback = P.compute_alignment && h->memory_mode != WFA_MEMORY_HIGH && b->span != WFA_SPAN_BIWFA
+                    ? (h->memory_mode == WFA_MEMORY_LOW ? 2 : 1)
+                    : 0;
+  P.bt_limit = (int64_t)std::min<uint64_t>(h->max_memory_compact, (uint64_t)INT64_MAX);
+  P.bt_probe = kProbeIntervalCompact;
   P.compat = h->compat;
   P.max_steps = h->max_steps;
   P.format = b->format;
@@ -439,7 +455,7 @@ static int32_t max_width(const AlignParams& P, int32_t max_len_sum) {
 static int32_t smem_slot_width(int lanes) { return lanes == 4 ? 16 : lanes == 8 ? 32 : 64; }
 
 static Round first_round(const AlignParams& P, int nc, int32_t max_len_sum, int lanes = 32,
-                         bool spill = true) {
+                         bool spill = true, int32_t max_seq = 0) {
   Round r;
   const int cls = metric_class(P.metric);
   const bool longp = max_len_sum > kLongPair;
@@ -454,14 +470,25 @@ static Round first_round(const AlignParams& P, int nc, int32_t max_len_sum, int 
                          : 0;
   r.ring_smem = !longp;
   r.wspill = 0;
+  if (P.piggyback) {
+    // Med/low keep no history: the ring (offsets, pcigars and block indices,
+    // as wide as any wavefront of the launch) and a backtrace buffer sized
+    // from the lengths, grown when a pair outgrows it.
+    r.ring_smem = false;
+    r.cfg.hist_scores = 0;
+    r.cfg.hist_words = 0;
+    r.cfg.bt_cap = std::max(16384, 16 * (max_len_sum + 3));
+    r.cfg.bt_init_cap = max_len_sum + 8;
+  }
   if (r.ring_smem) {
     const int32_t wsm = smem_slot_width(lanes);
     if (spill && r.cfg.wmax > wsm) r.wspill = r.cfg.wmax;
     r.cfg.wmax = std::min(r.cfg.wmax, wsm);
   }
-  // Each sequence of the launch is at most max_len_sum long.
+  // The longest sequence of the launch (max_seq, else at most max_len_sum).
   const bool packed = P.format == WFA_SEQ_PACKED2;
-  r.seq_words = std::min(kSeqSmemWords, packed ? (max_len_sum + 15) / 16 : (max_len_sum + 3) / 4 + 1);
+  const int32_t ms = max_seq > 0 ? max_seq : max_len_sum;
+  r.seq_words = std::min(kSeqSmemWords, packed ? (ms + 15) / 16 : (ms + 3) / 4 + 1);
   r.seq_words = (r.seq_words + 1) & ~1;
   // Corrected ends-free with begin-free seeds prunes dominated cells against
   // a per-diagonal array over [-(n + scope + 2), m + scope + 2] per component.
@@ -484,6 +511,7 @@ static void next_round(Round& r, const AlignParams& P, int32_t max_len_sum) {
     r.cfg.hist_scores *= 4;
     r.cfg.hist_words *= 4;
   }
+  if (P.piggyback) r.cfg.bt_cap = (int32_t)std::min<int64_t>((int64_t)r.cfg.bt_cap * 4, INT32_MAX / 2);
 }
 
 // Fills the launch fields of P for round r and returns the per-block shared
@@ -498,10 +526,13 @@ static SmemLayout round_layout(AlignParams& P, const Round& r, int nc, int64_t* 
   P.hist_scores = r.cfg.hist_scores;
   P.hist_words = r.cfg.hist_words;
   P.dom_words = r.cfg.dom_words;
+  P.bt_cap = r.cfg.bt_cap;
+  P.bt_init_cap = r.cfg.bt_init_cap;
   const int groups = kWarpsPerBlock * 32 / r.lanes;
   const SmemLayout L = smem_layout(P.desc_depth ? P.desc_depth : P.scope, nc, cell_slots(P, nc),
                                    r.ring_smem ? r.cfg.wmax : 0, r.seq_words, groups);
-  int64_t w = slice_ring_words(P, nc) + (int64_t)r.cfg.hist_scores * 4 + r.cfg.hist_words + r.cfg.dom_words;
+  int64_t w = slice_ring_words(P, nc) + (int64_t)r.cfg.hist_scores * 4 +
+              ((r.cfg.hist_words + r.cfg.dom_words + 3) & ~(int64_t)3) + slice_bt_words(P);
   *group_words = std::max<int64_t>((w + 63) & ~(int64_t)63, 64);
   return L;
 }
@@ -548,6 +579,7 @@ static int launch_round(wfa_aligner_t* h, AlignParams& P, const Round& r0, int64
   CUDA_TRY(h, h->counters.ensure(64), "counters");
   P.scratch = h->scratch.as<int32_t>();
   P.warp_words = group_words;
+  h->last_slice_bytes = group_words * 4;
   P.work_counter = ctr ? ctr : h->counters.as<unsigned long long>();
   P.retry_count = reinterpret_cast<int32_t*>(P.work_counter + 1);
   P.pair_list = list;
@@ -595,7 +627,7 @@ static std::vector<int> tune_key(const wfa_aligner_t* h, const AlignParams& P, i
 // Lanes per pair for a batch of `todo` pairs (0..todo-1 on the device; the
 // samples follow `list`, the batch's cost order, when given).
 static int choose_lanes(wfa_aligner_t* h, const AlignParams& P0, int32_t max_len_sum, int64_t todo,
-                        cudaStream_t st, bool may_tune, const int64_t* list = nullptr) {
+                        cudaStream_t st, bool may_tune, const int64_t* list = nullptr, int32_t max_seq = 0) {
   const int bucket = length_bucket(max_len_sum);
   if (needs_general(P0) || bucket == 3) return 32;
   if (h->lanes_forced) return h->lanes_forced;
@@ -616,7 +648,7 @@ static int choose_lanes(wfa_aligner_t* h, const AlignParams& P0, int32_t max_len
     float m = 0.f;
     for (int rep = 0; rep < 2; ++rep) {
       AlignParams P = P0;
-      Round r = first_round(P, nc, max_len_sum, cands[ci]);
+      Round r = first_round(P, nc, max_len_sum, cands[ci], true, max_seq);
       if (launch_round(h, P, r, sample, list, st) != WFA_OK) return default_lanes(P0, bucket);
       if (h->launch_lanes != cands[ci]) break;  // did not fit: ran wider groups
       if (cudaStreamSynchronize(st) != cudaSuccess) return default_lanes(P0, bucket);
@@ -637,7 +669,7 @@ static int choose_lanes(wfa_aligner_t* h, const AlignParams& P0, int32_t max_len
 // that need more.  Synchronises `st` to read the retry count.
 static int run_device_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* d_results,
                             uint8_t* d_cigars, cudaStream_t st, int32_t max_len_sum,
-                            const int64_t* first_list = nullptr) {
+                            const int64_t* first_list = nullptr, int32_t max_seq = 0) {
   AlignParams P;
   fill_params(h, b, P);
   P.results = d_results;
@@ -645,8 +677,8 @@ static int run_device_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t
   if (P.compute_alignment && (!d_cigars || !b->cigar_off))
     return fail(h, WFA_ERR_ARGUMENT, "CIGAR output buffers are required in alignment scope");
   const int nc = metric_components(P.metric);
-  const int lanes = choose_lanes(h, P, max_len_sum, b->num_pairs, st, true, first_list);
-  Round r = first_round(P, nc, max_len_sum, lanes);
+  const int lanes = choose_lanes(h, P, max_len_sum, b->num_pairs, st, true, first_list, max_seq);
+  Round r = first_round(P, nc, max_len_sum, lanes, true, max_seq);
   int64_t todo = b->num_pairs;
   const int64_t* list = first_list;
   h->last_kernel_ms = 0.0;
@@ -793,9 +825,9 @@ static int run_biwfa_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t*
 
 static int run_batch_kind(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* d_results,
                           uint8_t* d_cigars, cudaStream_t st, int32_t max_len_sum,
-                          const int64_t* first_list = nullptr) {
+                          const int64_t* first_list = nullptr, int32_t max_seq = 0) {
   if (b->span == WFA_SPAN_BIWFA) return run_biwfa_batch(h, b, d_results, d_cigars, st, max_len_sum);
-  return run_device_batch(h, b, d_results, d_cigars, st, max_len_sum, first_list);
+  return run_device_batch(h, b, d_results, d_cigars, st, max_len_sum, first_list, max_seq);
 }
 
 // Cost ordering (wfa_order.cu) for lean batches of short pairs: the lane
@@ -874,10 +906,9 @@ static int run_noalloc_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_
   // Whole warps per pair, and no spill ring: a row wider than the shared
   // memory slot re-runs the pair with the ring in its slice.
   Round r = first_round(P, nc, max_len_sum, 32, false);
-  if (P.compute_alignment) {
-    const int hnc = P.piggyback ? nc : 1;
-    r.cfg.hist_scores = 256 * hnc;
-    r.cfg.hist_words = 4096 * hnc;
+  if (P.compute_alignment && !P.piggyback) {
+    r.cfg.hist_scores = 256;
+    r.cfg.hist_words = 4096;
   }
   int64_t todo = b->num_pairs, pending = 0;
   int grown = 0;
@@ -1248,6 +1279,7 @@ int wfa_set_lanes_per_pair(wfa_aligner_t* h, int32_t lanes) {
   return WFA_OK;
 }
 int32_t wfa_last_lanes_per_pair(const wfa_aligner_t* h) { return h ? h->last_lanes : 0; }
+int64_t wfa_last_slice_bytes(const wfa_aligner_t* h) { return h ? h->last_slice_bytes : 0; }
 int32_t wfa_autotune_report(char* out, int32_t cap) {
   std::string r;
   {
@@ -1297,7 +1329,7 @@ int wfa_batch_align_device(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t*
   cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
   CUDA_TRY(h, h->counters.ensure(64), "counters");
   int32_t* d_max = reinterpret_cast<int32_t*>(h->counters.as<char>() + 32);
-  CUDA_TRY(h, cudaMemsetAsync(d_max, 0, 4, st), "memset");
+  CUDA_TRY(h, cudaMemsetAsync(d_max, 0, 8, st), "memset");
   const bool order = orders_batch(h, b);
   OrderBufs ob{};
   if (order) {
@@ -1319,11 +1351,12 @@ int wfa_batch_align_device(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t*
                                      h->num_sms, st), "cost order");
     h->launches++;
   }
-  int32_t mx = 0;
-  CUDA_TRY(h, cudaMemcpyAsync(&mx, d_max, 4, cudaMemcpyDeviceToHost, st), "D2H");
+  int32_t mxs[2] = {0, 0};
+  CUDA_TRY(h, cudaMemcpyAsync(mxs, d_max, 8, cudaMemcpyDeviceToHost, st), "D2H");
   CUDA_TRY(h, cudaStreamSynchronize(st), "max lengths");
+  const int32_t mx = mxs[0];
   const int64_t* first = order && length_bucket(mx) <= 2 ? ob.list : nullptr;
-  return run_batch_kind(h, b, results, cigars, st, mx, first);
+  return run_batch_kind(h, b, results, cigars, st, mx, first, mxs[1]);
 }
 
 // The device-buffer batch on the fixed array of wfa_noalloc.cu: no cudaMalloc,
@@ -1340,7 +1373,7 @@ int wfa_batch_align_device_noalloc(wfa_aligner_t* h, const wfa_batch_t* b, wfa_r
   int32_t* base = nullptr;
   CUDA_TRY(h, noalloc_scratch(h->device, &base), "address of the no-allocation scratch array");
   cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
-  int32_t* d_max = base + 3;
+  int32_t* d_max = base + 6;  // header words 6, 7: longest n + m, longest sequence
   CUDA_TRY(h, cudaMemsetAsync(base, 0, kNaHeaderWords * 4, st), "memset");
   max_lengths<<<256, 256, 0, st>>>(b->p_len, b->t_len, b->num_pairs, d_max);
   h->launches++;
@@ -1554,7 +1587,7 @@ int wfa_batch_align(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* result
     // one ran in this process, else the bucket's default (chunks are not
     // timed here: the pipeline would wait on them).
     const int lanes = choose_lanes(h, P, I.max_len_sum, cn, sc, false);
-    Round rd = first_round(P, metric_components(P.metric), I.max_len_sum, lanes);
+    Round rd = first_round(P, metric_components(P.metric), I.max_len_sum, lanes, true, I.max_seq);
     const int64_t* clist = nullptr;
     if (order && cn >= kSortMinPairs && length_bucket(I.max_len_sum) <= 2) {
       int32_t* hst = ob.hist + kOrderStride * ci;

@@ -6,6 +6,10 @@
 
 namespace wfab {
 
+// PROBE_INTERVAL_COMPACT (src/aligner.rs:360): scores between the med/low
+// backtrace buffer's compaction probes.
+constexpr int32_t kProbeIntervalCompact = 6000;
+
 // OFFSET_NULL (src/offset.rs:15) and DPMATRIX_DIAGONAL_NULL (:46).
 constexpr int32_t kOffsetNull = INT32_MIN / 2;
 constexpr int32_t kDiagNull = INT32_MAX;
@@ -31,9 +35,14 @@ struct AlignParams {
   // Heuristic (wfa_heuristic_kind_t and its three parameters).
   int32_t hkind, hp0, hp1, hp2;
   int32_t compute_alignment;
-  // 1: med/low memory with an alignment -- the piggyback backtrace (every
-  // component's history, no score cap).
+  // Med/low memory with an alignment -- the piggyback backtrace: 1 med,
+  // 2 low (0: neither).  Its backtrace buffer per lane group: bt_cap blocks,
+  // bt_init_cap initial positions, compacted above bt_limit bytes
+  // (max_memory_compact).
   int32_t piggyback;
+  int32_t bt_cap, bt_init_cap;
+  int64_t bt_limit;
+  int32_t bt_probe;  // scores between compaction probes (PROBE_INTERVAL_COMPACT, 6000)
   // Compat: 0 C (reproduce C's known bugs), 1 Corrected (src/aligner.rs:53-94).
   int32_t compat;
   int32_t max_steps;

@@ -52,7 +52,20 @@ __host__ __device__
 inline int64_t slice_ring_words(const AlignParams& P, int nc) {
   const int64_t slots = cell_slots(P, nc);
   int64_t w = P.ring_smem ? (P.ring_slots > 0 ? slots * P.wspill : 0) : slots * P.wmax;
+  if (P.piggyback && P.compute_alignment && !P.ring_smem) w *= 3;  // offsets, pcigars, block indices
   return (w + 3) & ~(int64_t)3;
+}
+
+// Words of a lane group's med/low backtrace buffer (after the dominance
+// array): blocks (2 words each), initial positions (2 words each), then the
+// compaction bitmap and its word counts.
+#if defined(__CUDACC__)
+__host__ __device__
+#endif
+inline int64_t slice_bt_words(const AlignParams& P) {
+  if (!(P.piggyback && P.compute_alignment)) return 0;
+  const int64_t marks = 2 * (((int64_t)P.bt_cap + 31) / 32);
+  return (2 * (int64_t)P.bt_cap + 2 * (int64_t)P.bt_init_cap + marks + 3) & ~(int64_t)3;
 }
 
 // BiWFA per-warp scratch slice (int32 word offsets).  seq_len_sum is the
@@ -85,7 +98,8 @@ inline BiLayout bi_layout(int scope, int nc, int wmax, int wmax_base, int hist_s
 
 // Cost ordering of a batch (wfa_order.cu): order_count computes each pair's
 // 4-mer profile distance key, the key histogram (kOrderBins bins, highest
-// key first) and the longest n + m; order_scatter writes the pair indices
+// key first), the longest n + m and the longest sequence (two words at
+// max_len_sum); order_scatter writes the pair indices
 // in bin order into a list for the kernel's work queue.  hist and fill
 // (kOrderBins ints each) start zeroed.
 constexpr int kOrderBins = 1024;

@@ -1,5 +1,5 @@
-// wfa_kernels_gen.cu -- general (ends-free, heuristics, med/low, Corrected): the
-// unidirectional kernel's instantiations for ends-free, heuristic, med/low and Corrected alignments (whole warps), in a translation
+// wfa_kernels_gen.cu -- general (ends-free, heuristics, Corrected): the
+// unidirectional kernel's instantiations for ends-free, heuristic and Corrected alignments in high memory or score only (whole warps), in a translation
 // unit of their own so the kernel variants build in parallel.
 #include "wfa_unialign.cuh"
 

@@ -24,7 +24,8 @@ constexpr int kProfileBases = 4096;  // bases of each sequence the estimate read
 // (2-bit codes: packed input as stored; ASCII bytes by their bits 1-2, which
 // tell A, C, G and T apart -- enough for an estimate.)
 
-// Per pair: the longest n + m of the batch (atomicMax into *max_len_sum),
+// Per pair: the longest n + m of the batch and its longest sequence
+// (atomicMax into max_len_sum[0] and [1]),
 // the estimate key (keys[i], at most kOrderBins - 1) and the batch's key
 // histogram (bin kOrderBins - 1 - key, so that bins ascend as costs fall).
 // Each thread profiles its own pairs in a column of shared memory: two
@@ -46,10 +47,11 @@ __global__ void __launch_bounds__(kCountBlock) order_count(const uint8_t* seq, i
   for (int b = tid; b < kOrderBins; b += kCountBlock) bins[b] = 0;
   for (int x = 0; x < 128; ++x) prof[x * kCountBlock + tid] = kBiased;
   __syncthreads();
-  int32_t mx = 0;
+  int32_t mx = 0, ms = 0;
   for (int64_t i = (int64_t)blockIdx.x * kCountBlock + tid; i < n; i += (int64_t)gridDim.x * kCountBlock) {
     const int32_t pn = p_len[i], tn = t_len[i];
     mx = max(mx, pn + tn);
+    ms = max(ms, max(pn, tn));
     for (int s = 0; s < 2; ++s) {
       const int64_t off = s == 0 ? p_off[i] : t_off[i];
       const int len = min(s == 0 ? pn : tn, kProfileBases);
@@ -89,7 +91,11 @@ __global__ void __launch_bounds__(kCountBlock) order_count(const uint8_t* seq, i
     atomicAdd(&bins[kOrderBins - 1 - key], 1);
   }
   mx = __reduce_max_sync(0xffffffffu, mx);
-  if ((tid & 31) == 0) atomicMax(max_len_sum, mx);
+  ms = __reduce_max_sync(0xffffffffu, ms);
+  if ((tid & 31) == 0) {
+    atomicMax(max_len_sum, mx);
+    atomicMax(max_len_sum + 1, ms);
+  }
   __syncthreads();
   for (int b = tid; b < kOrderBins; b += kCountBlock)
     if (bins[b]) atomicAdd(&hist[b], bins[b]);

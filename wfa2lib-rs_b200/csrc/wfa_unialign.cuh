@@ -23,8 +23,10 @@ namespace wfab {
 // Register budget: the lean instantiations of the smaller metrics fit 80
 // registers (6 blocks = 24 warps per SM); the general and two-piece ones keep
 // 128 (4 blocks) rather than spill.
-template <int CLS, bool GEN>
-constexpr int min_blocks() { return (GEN || CLS == kAffine2pClass) ? 4 : kMinBlocksPerSM; }
+// The med/low instantiation carries three arrays per cell and the backtrace
+// buffer: 2 blocks per SM (up to 255 registers) rather than spill.
+template <int CLS, bool GEN, bool PB = false>
+constexpr int min_blocks() { return PB ? 2 : (GEN || CLS == kAffine2pClass) ? 4 : kMinBlocksPerSM; }
 
 // The sequences of pair `pair`, staged in the group's shared memory (2 x sw
 // words) when both fit, else read from device memory.
@@ -80,8 +82,8 @@ WFA_D void mark_retry(const AlignParams& P, int64_t pair, int lane) {
   }
 }
 
-template <int CLS, int ENC, bool GEN, int LW>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, (min_blocks<CLS, GEN>()))
+template <int CLS, int ENC, bool GEN, int LW, bool PB = false>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, (min_blocks<CLS, GEN, PB>()))
     unialign_kernel(const AlignParams P) {
   extern __shared__ __align__(16) uint8_t smem[];
   constexpr int kGroups = kWarpsPerBlock * 32 / LW;  // lane groups (pairs in flight) per block
@@ -105,6 +107,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (min_blocks<CLS, GEN>()))
   ws.hist = reinterpret_cast<int4*>(slice + ring_words);
   ws.harena = slice + ring_words + (int64_t)P.hist_scores * 4;
   ws.dom = P.dom_words ? ws.harena + P.hist_words : nullptr;
+  int32_t* btb = ws.harena + ((P.hist_words + P.dom_words + 3) & ~(int64_t)3);  // 16-byte aligned
+  ws.bt = reinterpret_cast<uint2*>(btb);
+  ws.btinit = reinterpret_cast<int2*>(btb + 2 * (int64_t)P.bt_cap);
+  ws.btmark = reinterpret_cast<uint32_t*>(btb + 2 * (int64_t)P.bt_cap + 2 * (int64_t)P.bt_init_cap);
   const int sw = P.seq_smem_words;
   // Each lane group pulls pairs from the launch's work queue.  The groups of
   // a warp run their pairs side by side (lockstep per pair: the warp's
@@ -115,7 +121,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (min_blocks<CLS, GEN>()))
     if (pair < 0) break;
     S sp, st;
     pair_seqs<LW>(P, pair, sseq, sw, lane, sp, st);
-    if (align_one<CLS, S, GEN, LW>(P, ws, pair, sp, st)) mark_retry<LW>(P, pair, lane);
+    if (align_one<CLS, S, GEN, LW, PB>(P, ws, pair, sp, st)) mark_retry<LW>(P, pair, lane);
     G::sync();
   }
 }
@@ -124,13 +130,13 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (min_blocks<CLS, GEN>()))
 // is only ever raised, under a lock: handles on several host threads launch
 // the same kernels, and lowering it under another thread's launch would make
 // that launch fail.
-template <int CLS, int ENC, bool GEN, int LW>
+template <int CLS, int ENC, bool GEN, int LW, bool PB = false>
 static cudaError_t allow_smem(size_t smem) {
   static size_t configured = 0;
   static std::mutex mu;
   std::lock_guard<std::mutex> lock(mu);
   if (smem > configured) {
-    cudaError_t e = cudaFuncSetAttribute(unialign_kernel<CLS, ENC, GEN, LW>,
+    cudaError_t e = cudaFuncSetAttribute(unialign_kernel<CLS, ENC, GEN, LW, PB>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     configured = smem;
@@ -138,20 +144,20 @@ static cudaError_t allow_smem(size_t smem) {
   return cudaSuccess;
 }
 
-template <int CLS, int ENC, bool GEN, int LW>
+template <int CLS, int ENC, bool GEN, int LW, bool PB = false>
 static cudaError_t launch_t(const AlignParams& P, int blocks, size_t smem, cudaStream_t st) {
-  auto k = unialign_kernel<CLS, ENC, GEN, LW>;
-  cudaError_t e = allow_smem<CLS, ENC, GEN, LW>(smem);
+  auto k = unialign_kernel<CLS, ENC, GEN, LW, PB>;
+  cudaError_t e = allow_smem<CLS, ENC, GEN, LW, PB>(smem);
   if (e != cudaSuccess) return e;
   k<<<blocks, kWarpsPerBlock * 32, smem, st>>>(P);
   return cudaGetLastError();
 }
 
-template <int CLS, int ENC, bool GEN, int LW>
+template <int CLS, int ENC, bool GEN, int LW, bool PB = false>
 static int occ_t(size_t smem) {
   int nb = 0;
-  auto k = unialign_kernel<CLS, ENC, GEN, LW>;
-  if (allow_smem<CLS, ENC, GEN, LW>(smem) != cudaSuccess ||
+  auto k = unialign_kernel<CLS, ENC, GEN, LW, PB>;
+  if (allow_smem<CLS, ENC, GEN, LW, PB>(smem) != cudaSuccess ||
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, kWarpsPerBlock * 32, smem) != cudaSuccess) {
     cudaGetLastError();
     nb = 1;
