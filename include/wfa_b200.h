@@ -82,7 +82,8 @@ enum {
   WFA_ERR_UNSUPPORTED = -3, /* configuration this build does not run on the GPU */
   WFA_ERR_CUDA = -4,        /* CUDA runtime error (see wfa_last_error_string) */
   WFA_ERR_NO_DEVICE = -5,   /* no CUDA device */
-  WFA_ERR_OOM = -6          /* device memory exhausted */
+  WFA_ERR_OOM = -6,         /* device memory exhausted */
+  WFA_ERR_BUSY = -7         /* a resident stream's request ring is full: poll, then submit again */
 };
 
 /* ---- penalties ---------------------------------------------------------- */
@@ -301,7 +302,8 @@ typedef struct {
   int32_t short_workers;        /* short lane workers (default 2) */
   int32_t biwfa_workers;        /* BiWFA lane workers (default 2) */
   int32_t short_max_len;        /* n + m of the short lane (default 1024) */
-  int32_t reserved;
+  int32_t resident;             /* 1: the short lane is a resident stream (wfa_stream_*; n + m of the
+                                   short lane at most 2048) */
 } wfa_server_config_t;
 
 typedef struct wfa_server wfa_server_t;
@@ -339,6 +341,51 @@ WFA_API int64_t wfa_server_pending(wfa_server_t* s);
 /* Finishes the queued requests, stops the workers and frees the server. */
 WFA_API int wfa_server_stop(wfa_server_t* s);
 
+/* ---- resident stream: a persistent kernel fed request by request ----------
+ * No counterpart in the reference.  One kernel stays on the GPU and aligns
+ * single requests (end-to-end, high memory, n + m up to max_len_sum <= 2048,
+ * ASCII bytes) as they are submitted: the host appends each request to a
+ * ring in mapped pinned memory (capacity requests) and publishes it; one warp
+ * of the kernel watches the ring's tail and every other lane group claims
+ * the next request, aligns it with the batch kernels' per-pair aligner and
+ * writes its result and CIGAR straight into mapped memory.  The kernel's
+ * waits are bounded: it returns after about a second without requests (or
+ * at wfa_stream_stop) and is launched again by the next submit or poll.  A
+ * request that outgrows the kernel's scratch is aligned again through
+ * wfa_batch_align.  Results are those of wfa_align_end2end with the same
+ * metric, penalties and scope, whatever else is in flight.  The kernel holds
+ * blocks_per_sm blocks on every SM (0: as many as fit) for as long as it
+ * runs: work of other handles on the device shares what is left. */
+typedef struct wfa_stream wfa_stream_t;
+WFA_API wfa_stream_t* wfa_stream_start(wfa_metric_t metric, const wfa_penalties_t* penalties, int32_t device,
+                                       int32_t score_only, int32_t max_len_sum, int32_t capacity,
+                                       int32_t blocks_per_sm, int* err);
+/* Queues one pair (copied into the ring); returns its id (ids count up from
+ * 0), WFA_ERR_BUSY when capacity requests are outstanding, or an error. */
+WFA_API int64_t wfa_stream_submit(wfa_stream_t* s, const uint8_t* pattern, int32_t pattern_length,
+                                  const uint8_t* text, int32_t text_length);
+/* Queues `count` pairs (offsets into seq, as in wfa_batch_t with ASCII
+ * bytes) as separate requests with consecutive ids; returns the first id.
+ * All or none: WFA_ERR_BUSY if they do not all fit. */
+WFA_API int64_t wfa_stream_submit_many(wfa_stream_t* s, const uint8_t* seq, const int64_t* p_off,
+                                       const int32_t* p_len, const int64_t* t_off, const int32_t* t_len,
+                                       int64_t count);
+/* Moves up to `max` finished requests into `out` (CIGAR ops densely into
+ * `cigars`, at most cigar_cap bytes; mode 0), waiting up to timeout_ms for
+ * the first; latency_ns runs from submit to the poll that found the result.
+ * Returns the count (0 on timeout) or an error code. */
+WFA_API int32_t wfa_stream_poll(wfa_stream_t* s, wfa_served_t* out, int32_t max, uint8_t* cigars,
+                                int64_t cigar_cap, int32_t timeout_ms);
+/* Requests submitted and not yet polled. */
+WFA_API int64_t wfa_stream_pending(wfa_stream_t* s);
+/* Up to n of: kernel launches, launches that ended idle, lane groups that
+ * gave up polling, requests re-aligned through wfa_batch_align, blocks, lanes
+ * per request. */
+WFA_API int wfa_stream_stats(wfa_stream_t* s, int64_t* out, int32_t n);
+/* Aligns what was submitted, ends the kernel and frees the stream (results
+ * not yet polled are dropped). */
+WFA_API int wfa_stream_stop(wfa_stream_t* s);
+
 /* Number of the library's own kernel launches issued so far by this handle. */
 WFA_API int64_t wfa_kernel_launches(const wfa_aligner_t* h);
 
@@ -357,6 +404,13 @@ WFA_API int64_t wfa_last_rerun_pairs(const wfa_aligner_t* h);
  * n + m = 2048 always take whole warps.  Results never depend on it.  No
  * counterpart in the reference (it aligns one pair per call on the CPU). */
 WFA_API int wfa_set_lanes_per_pair(wfa_aligner_t* h, int32_t lanes);
+/* Lanes per pair of the BiWFA kernel: 32 (a warp aligns one pair), 128, 256
+ * or 512 (a team of 4, 8 or 16 warps of one block aligns one pair; their
+ * collectives meet at a named barrier), or 0 (the default) to choose by the
+ * launch's longest pair (n + m above 3000: 256; above 1000: 128; else 32).  Teams run the kernels without a heuristic; with a
+ * heuristic the BiWFA kernel always takes a warp per pair.  Results never
+ * depend on it.  No counterpart in the reference. */
+WFA_API int wfa_set_biwfa_lanes(wfa_aligner_t* h, int32_t lanes);
 /* Lanes per pair the handle's last batch ran with (first round). */
 WFA_API int32_t wfa_last_lanes_per_pair(const wfa_aligner_t* h);
 /* Device memory (bytes) one pair in flight used in the handle's last

@@ -164,19 +164,22 @@ static bool bi_pair(const AlignParams& P, int64_t i) {
   constexpr int NC = CLS == kAffine2pClass ? 5 : CLS == kAffineClass ? 3 : 1;
   const size_t ring = (size_t)P.scope * NC;
   std::vector<WfD> d1(ring), d2(ring), d3(ring);
-  std::vector<int32_t> v1(ring * P.wmax, 0x5A5A5A5A), v2(ring * P.wmax, 0x5A5A5A5A);
+  const size_t ring_fr = ring + (size_t)bi_idc_rows(NC, P.e1, P.e2);
+  std::vector<int32_t> v1(ring_fr * P.wmax, 0x5A5A5A5A), v2(ring_fr * P.wmax, 0x5A5A5A5A);
   std::vector<int32_t> v3(ring * P.wmax_base, 0x5A5A5A5A);
   std::vector<int4> hist((size_t)P.hist_scores, int4{0, -1, 0, 0});
   std::vector<int32_t> harena((size_t)P.hist_words, 0x5A5A5A5A);
   const int n = P.p_len[i], m = P.t_len[i];
   std::vector<uint32_t> rev((size_t)(n + m) / 4 + 16, 0);
   std::vector<uint8_t> tmp((size_t)2 * (n + m) + 16, 0);
+  std::vector<BiFrame> frames(kBiMaxDepth);
   BiWorkspace bw;
   bw.fwd = Workspace{d1.data(), v1.data(), nullptr, nullptr};
   bw.rev = Workspace{d2.data(), v2.data(), nullptr, nullptr};
   bw.base = Workspace{d3.data(), v3.data(), hist.data(), harena.data()};
   bw.rev_seq = reinterpret_cast<uint8_t*>(rev.data());
   bw.cig_tmp = tmp.data();
+  bw.frames = frames.data();
   auto go = [&]() -> bool {
     if (P.format == WFA_SEQ_PACKED2) {
       const uint32_t* w = reinterpret_cast<const uint32_t*>(P.seq);
@@ -226,11 +229,12 @@ extern "C" int64_t wfa_emu_biwfa(int metric, const int32_t* pen6, int compute_al
                                  const int64_t* p_off, const int32_t* p_len, const int64_t* t_off,
                                  const int32_t* t_len, int64_t num_pairs, const int64_t* cigar_off,
                                  uint8_t* cigars, wfa_result_t* results, int32_t wmax,
-                                 int32_t hist_scores, int64_t hist_words) {
+                                 int32_t hist_scores, int64_t hist_words, int32_t bi_idc) {
   AlignParams P;
   std::memset(&P, 0, sizeof P);
   wfa_penalties_t u = {pen6[0], pen6[1], pen6[2], pen6[3], pen6[4], pen6[5]};
   if (set_penalties(metric, &u, P) != WFA_OK) return -1;
+  P.bi_idc = bi_idc;
   P.hkind = hkind;
   if (hp3) { P.hp0 = hp3[0]; P.hp1 = hp3[1]; P.hp2 = hp3[2]; }
   P.compute_alignment = compute_alignment;

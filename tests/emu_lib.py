@@ -15,7 +15,8 @@ LANES = int(os.environ.get("WFA_EMU_LANES", "1"))
 def lib(lanes=None):
     lanes = LANES if lanes is None else lanes
     if lanes not in _L:
-        name = {32: "libwfa_emu32.so", 8: "libwfa_emu8.so"}.get(lanes, "libwfa_emu.so")
+        name = {32: "libwfa_emu32.so", 8: "libwfa_emu8.so",
+                128: "libwfa_emu128.so"}.get(lanes, "libwfa_emu.so")
         path = os.path.join(HERE, "emu", "_build", name)
         if os.system(f"make -s -C {os.path.join(HERE, 'emu')}") != 0 or not os.path.exists(path):
             raise RuntimeError("cannot build the emulation library")
@@ -89,8 +90,10 @@ def run(metric, pen, pairs, compute_alignment=True, span=0, extension=0, free=No
 
 def run_biwfa(metric, pen, pairs, compute_alignment=True, heuristic=0, hparams=(0, 0, 0),
               max_steps=2**31 - 1, packed=False, wmax=4096, hist_scores=1 << 16, hist_words=1 << 22,
-              lanes=None):
-    """BiWFA through the emulated device driver: (results, cigar strings)."""
+              lanes=None, idc=0):
+    """BiWFA through the emulated device driver: (results, cigar strings).
+    idc: the growth phase's I/D rings, 0 by length, 1 kept until the overlap
+    scans (every search restarts), 2 off."""
     n = len(pairs)
     if packed:
         words, p_off, t_off, p_len, t_len = [], [], [], [], []
@@ -127,7 +130,8 @@ def run_biwfa(metric, pen, pairs, compute_alignment=True, heuristic=0, hparams=(
     r = L.wfa_emu_biwfa(metric, _p(pen6), int(compute_alignment), heuristic, _p(hp3),
                         ctypes.c_int32(max_steps), 1 if packed else 0, _p(seq), _p(p_off), _p(p_len),
                         _p(t_off), _p(t_len), ctypes.c_int64(n), _p(c_off), _p(cig), _p(res),
-                        ctypes.c_int32(wmax), ctypes.c_int32(hist_scores), ctypes.c_int64(hist_words))
+                        ctypes.c_int32(wmax), ctypes.c_int32(hist_scores), ctypes.c_int64(hist_words),
+                        ctypes.c_int32(idc))
     assert r >= 0
     cigars = []
     for i in range(n):

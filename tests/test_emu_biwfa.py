@@ -32,9 +32,9 @@ def long_pairs(seed, count, lo, hi, rate):
     return out
 
 
-def compare(metric, pen, pairs, compute=True, hk=0, hp=(0, 0, 0), packed=False, lanes=None):
+def compare(metric, pen, pairs, compute=True, hk=0, hp=(0, 0, 0), packed=False, lanes=None, idc=0):
     res, cig = emu_lib.run_biwfa(metric, pen, pairs, compute_alignment=compute, heuristic=hk,
-                                 hparams=hp, packed=packed, lanes=lanes)
+                                 hparams=hp, packed=packed, lanes=lanes, idc=idc)
     for i, (p, t) in enumerate(pairs):
         a = O.OracleAligner(metric, pen)
         if hk:
@@ -51,6 +51,30 @@ def test_biwfa(metric, pen, packed):
     pairs = lcg_pairs(301 + metric, 10, 220) + long_pairs(303 + metric, 3, 250, 700, 0.1)
     compare(metric, pen, pairs, packed=packed)
     compare(metric, pen, pairs[:8] + pairs[-2:], compute=False, packed=packed)
+
+
+@pytest.mark.parametrize("idc", [0, 1, 2])
+@pytest.mark.parametrize("metric,pen", [(3, [0, 4, 6, 2]), (4, [0, 4, 6, 2, 24, 1])])
+def test_biwfa_growth_idc_rings(metric, pen, idc):
+    """Breakpoint searches of more than 2,048 antidiagonals keep their I/D
+    rows in small rings until near the overlap scans (0); kept until the
+    scans, every such search restarts with all rows kept (1); off (2).  The
+    results are the same."""
+    pairs = long_pairs(341 + metric, 3, 1100, 2400, 0.1)
+    assert max(len(p) + len(t) for p, t in pairs) > 2100
+    compare(metric, pen, pairs, packed=True, idc=idc)
+    compare(metric, pen, pairs[:1], compute=False, idc=idc)
+
+
+@pytest.mark.parametrize("metric,pen", [(1, None), (3, [0, 4, 6, 2]), (4, [0, 4, 6, 2, 24, 1])])
+def test_biwfa_team_lanes(metric, pen):
+    """The driver with 128 lanes as host threads that meet at barriers (a
+    team of four warps): every collective must be reached by all of its
+    lanes in the same order.  One pair that recurses (a breakpoint, base
+    cases) and one short pair."""
+    pairs = lcg_pairs(331 + metric, 1, 120) + long_pairs(333 + metric, 1, 420, 520, 0.1)
+    compare(metric, pen, pairs, packed=True, lanes=128)
+    compare(metric, pen, pairs[-1:], compute=False, lanes=128)
 
 
 @pytest.mark.parametrize("h,hp", [("banded-static", (-10, 10, 0)), ("banded-adaptive", (-8, 8, 1)),

@@ -21,9 +21,11 @@ def pkg():
     return load()
 
 
-def compare(pkg, metric, pen, pairs, compute=True, hk=0, hp=(0, 0, 0), packed=False):
+def compare(pkg, metric, pen, pairs, compute=True, hk=0, hp=(0, 0, 0), packed=False, lanes=0):
     a = pkg.WavefrontAligner(metric, pen)
     a.set_alignment_scope(compute)
+    if lanes:
+        a.set_biwfa_lanes(lanes)
     if hk:
         a.set_heuristic(hk, *hp)
     if packed:
@@ -46,12 +48,14 @@ def compare(pkg, metric, pen, pairs, compute=True, hk=0, hp=(0, 0, 0), packed=Fa
         assert (int(r["score"]), int(r["status"]), got) == (s, o.status(), ops), (metric, i, len(p))
 
 
+@pytest.mark.parametrize("lanes", [32, 128, 256, 512])
 @pytest.mark.parametrize("metric,pen", PENS)
-def test_biwfa_batch(pkg, metric, pen):
+def test_biwfa_batch(pkg, metric, pen, lanes):
+    """A warp per pair, and teams of 4, 8 and 16 warps."""
     pairs = lcg_pairs(401 + metric, 30, 250) + long_pairs(403 + metric, 8, 300, 1500, 0.1)
-    compare(pkg, metric, pen, pairs)
-    compare(pkg, metric, pen, pairs, packed=True)
-    compare(pkg, metric, pen, pairs, compute=False)
+    compare(pkg, metric, pen, pairs, lanes=lanes)
+    compare(pkg, metric, pen, pairs, packed=True, lanes=lanes)
+    compare(pkg, metric, pen, pairs, compute=False, lanes=lanes)
 
 
 @pytest.mark.parametrize("h,hp", [("banded-static", (-10, 10, 0)), ("banded-adaptive", (-8, 8, 1)),
@@ -88,13 +92,15 @@ def test_biwfa_plain_and_golden_cli(pkg, golden):
         assert lines == case["expected"], case["name"]
 
 
-def _batch_vs_oracle(pkg, metric, pen, ps):
+def _batch_vs_oracle(pkg, metric, pen, ps, lanes=0):
     """A packed host-buffer BiWFA batch against the oracle's align_biwfa on
     every pair: score, status and CIGAR (hashes of the op bytes)."""
     import os
     from wfa_b200 import synth
     a = pkg.WavefrontAligner(metric, pen)
     a.set_alignment_scope(True)
+    if lanes:
+        a.set_biwfa_lanes(lanes)
     words, pwo, two = synth.pack2bits(ps)
     res, cig = a.align_batch(np.concatenate([words, np.zeros(4, np.uint32)]), pwo, ps.p_len, two,
                              ps.t_len, packed=True, span=2)
@@ -108,7 +114,8 @@ def _batch_vs_oracle(pkg, metric, pen, ps):
     assert np.array_equal(gh, hs)
 
 
-def test_biwfa_longread_sizes(pkg):
+@pytest.mark.parametrize("lanes", [32, 256])
+def test_biwfa_longread_sizes(pkg, lanes):
     """Pairs of the uneven long-read batch at its long end: 16 pairs of
     8.5-20 kbp at 5-15 % edits (60 % indels), gap-affine 2-piece -- deep
     breakpoint recursions and the recovery threshold."""
@@ -116,7 +123,7 @@ def test_biwfa_longread_sizes(pkg):
     pool = synth.config3(400, synth.SEED_BASE + 3)
     ps = pool.subset(np.where(pool.p_len >= 8000)[0][:16])
     assert len(ps) == 16 and ps.p_len.max() > 15000
-    _batch_vs_oracle(pkg, 4, [0, 4, 6, 2, 24, 1], ps)
+    _batch_vs_oracle(pkg, 4, [0, 4, 6, 2, 24, 1], ps, lanes)
 
 
 def test_biwfa_serving_long_lane(pkg):

@@ -7,4 +7,4 @@ Python mirror.  Import it by path (the directory name is not an identifier),
 e.g. with importlib; see tests/_pkg.py.
 """
 from .aligner import (COMPLETED, EDIT, GAP_AFFINE, GAP_AFFINE_2P, GAP_LINEAR, INDEL,  # noqa: F401
-                      RESULT_DTYPE, Cigar, Server, WavefrontAligner, cigar_rle, lib)
+                      RESULT_DTYPE, Cigar, Server, Stream, WavefrontAligner, cigar_rle, lib)

@@ -29,7 +29,7 @@ HEURISTICS = {"none": 0, "wfa-adaptive": 1, "xdrop": 2, "zdrop": 3, "banded-stat
 SEQ_ASCII, SEQ_PACKED2 = 0, 1
 SPAN_END2END, SPAN_ENDSFREE = 0, 1
 ERRORS = {-1: "invalid penalties", -2: "invalid argument", -3: "unsupported configuration",
-          -4: "CUDA error", -5: "no CUDA device", -6: "out of device memory"}
+          -4: "CUDA error", -5: "no CUDA device", -6: "out of device memory", -7: "stream ring full"}
 
 RESULT_DTYPE = np.dtype([(f, np.int32) for f in (
     "score", "status", "cigar_begin", "cigar_length", "cigar_score", "end_v", "end_h",
@@ -56,7 +56,7 @@ class ServerConfig(ctypes.Structure):
                 ("max_batch_pairs", ctypes.c_int32), ("max_batch_bytes", ctypes.c_int64),
                 ("biwfa_above_bytes", ctypes.c_int64), ("short_workers", ctypes.c_int32),
                 ("biwfa_workers", ctypes.c_int32), ("short_max_len", ctypes.c_int32),
-                ("reserved", ctypes.c_int32)]
+                ("resident", ctypes.c_int32)]
 
 
 class Served(ctypes.Structure):
@@ -111,10 +111,19 @@ def lib():
         "wfa_server_last_error": (ctypes.c_char_p, [vp]),
         "wfa_server_pending": (i64, [vp]),
         "wfa_server_stop": (ctypes.c_int, [vp]),
+        "wfa_stream_start": (vp, [ctypes.c_int, ctypes.POINTER(Penalties), i32, i32, i32, i32, i32,
+                                  ctypes.POINTER(ctypes.c_int)]),
+        "wfa_stream_submit": (i64, [vp, ctypes.c_char_p, i32, ctypes.c_char_p, i32]),
+        "wfa_stream_submit_many": (i64, [vp, vp, vp, vp, vp, vp, i64]),
+        "wfa_stream_poll": (i32, [vp, ctypes.POINTER(Served), i32, vp, i64, i32]),
+        "wfa_stream_pending": (i64, [vp]),
+        "wfa_stream_stats": (ctypes.c_int, [vp, ctypes.POINTER(i64), i32]),
+        "wfa_stream_stop": (ctypes.c_int, [vp]),
         "wfa_kernel_launches": (i64, [vp]),
         "wfa_last_rerun_pairs": (i64, [vp]),
         "wfa_set_lanes_per_pair": (ctypes.c_int, [vp, i32]),
         "wfa_last_lanes_per_pair": (i32, [vp]),
+        "wfa_set_biwfa_lanes": (ctypes.c_int, [vp, i32]),
         "wfa_last_slice_bytes": (i64, [vp]),
         "wfa_autotune_report": (i32, [ctypes.c_char_p, i32]),
         "wfa_last_kernel_ms": (ctypes.c_double, [vp]),
@@ -278,6 +287,11 @@ class WavefrontAligner:
         heuristic, or 0 for the autotuned choice (the default)."""
         return self._check(self._L.wfa_set_lanes_per_pair(self._h, lanes))
 
+    def set_biwfa_lanes(self, lanes):
+        """32 lanes (a warp) or 128, 256, 512 (a team of warps) per pair for
+        BiWFA batches without a heuristic; 0 chooses by the longest pair."""
+        return self._check(self._L.wfa_set_biwfa_lanes(self._h, lanes))
+
     def last_lanes_per_pair(self):
         return self._L.wfa_last_lanes_per_pair(self._h)
 
@@ -381,11 +395,11 @@ class Server:
 
     def __init__(self, metric, penalties=None, device=0, score_only=False, workers=2,
                  max_batch_pairs=65536, max_batch_bytes=4 << 30, biwfa_above_bytes=256 << 20,
-                 short_workers=2, biwfa_workers=2, short_max_len=1024):
+                 short_workers=2, biwfa_workers=2, short_max_len=1024, resident=False):
         self._L = lib()
         cfg = ServerConfig(metric, _pen(metric, penalties), device, int(score_only), workers,
                            max_batch_pairs, max_batch_bytes, biwfa_above_bytes, short_workers,
-                           biwfa_workers, short_max_len, 0)
+                           biwfa_workers, short_max_len, int(resident))
         err = ctypes.c_int(0)
         self._s = self._L.wfa_server_start(ctypes.byref(cfg), ctypes.byref(err))
         if not self._s:
@@ -426,6 +440,100 @@ class Server:
         if self._s:
             self._L.wfa_server_stop(self._s)
             self._s = None
+
+    def __del__(self):
+        try:
+            self.stop()
+        except Exception:
+            pass
+
+
+STREAM_DTYPE = np.dtype([("id", np.int64), ("score", np.int32), ("status", np.int32),
+                         ("cigar_length", np.int32), ("cigar_score", np.int32), ("end_v", np.int32),
+                         ("end_h", np.int32), ("mode", np.int32), ("pad", np.int32),
+                         ("cigar_offset", np.int64), ("latency_ns", np.int64)])
+assert STREAM_DTYPE.itemsize == ctypes.sizeof(Served)
+
+
+class Stream:
+    """A resident serving kernel fed request by request (wfa_stream_* of the
+    C ABI): end-to-end alignments of pairs with n + m <= max_len_sum, each
+    submitted on its own (or many at once, still separate requests) while
+    the kernel runs; results are those of WavefrontAligner.align_end2end."""
+
+    def __init__(self, metric, penalties=None, device=0, score_only=False, max_len_sum=512,
+                 capacity=1 << 16, blocks_per_sm=0):
+        self._L = lib()
+        err = ctypes.c_int(0)
+        pen = _pen(metric, penalties)
+        self._s = self._L.wfa_stream_start(metric, ctypes.byref(pen), device, int(score_only),
+                                           max_len_sum, capacity, blocks_per_sm, ctypes.byref(err))
+        if not self._s:
+            raise RuntimeError(f"wfa_stream_start: {ERRORS.get(err.value, err.value)}")
+        self._max = 1 << 16
+        self._recs = np.zeros(self._max, STREAM_DTYPE)
+        self._cig = np.zeros(self._max * (2 * max_len_sum + 1), np.uint8)
+
+    def submit(self, pattern, text):
+        """One request; its id, or -7 (WFA_ERR_BUSY) when the ring is full."""
+        r = self._L.wfa_stream_submit(self._s, pattern, len(pattern), text, len(text))
+        if r < 0 and r != -7:
+            raise RuntimeError(f"wfa_stream_submit: {ERRORS.get(r, r)}")
+        return r
+
+    def submit_many(self, seq, p_off, p_len, t_off, t_len):
+        """Requests for pairs at byte offsets of seq (uint8); the first id
+        (ids are consecutive), or -7 (WFA_ERR_BUSY) if they do not all fit."""
+        seq = np.ascontiguousarray(seq, np.uint8)
+        arrs = [np.ascontiguousarray(a, t) for a, t in ((p_off, np.int64), (p_len, np.int32),
+                                                          (t_off, np.int64), (t_len, np.int32))]
+        r = self._L.wfa_stream_submit_many(self._s, seq.ctypes.data, *[a.ctypes.data for a in arrs],
+                                           len(arrs[1]))
+        if r < 0 and r != -7:
+            raise RuntimeError(f"wfa_stream_submit_many: {ERRORS.get(r, r)}")
+        return r
+
+    def poll_arrays(self, timeout_ms=100, max_records=1 << 16):
+        """Finished requests as a structured array (STREAM_DTYPE) and the
+        CIGAR byte buffer its cigar_offset fields index (valid until the next
+        poll)."""
+        c = self._L.wfa_stream_poll(self._s, self._recs.ctypes.data_as(ctypes.POINTER(Served)),
+                                    min(max_records, self._max), self._cig.ctypes.data,
+                                    len(self._cig), timeout_ms)
+        if c < 0:
+            raise RuntimeError(f"wfa_stream_poll: {ERRORS.get(c, c)}")
+        return self._recs[:c].copy(), self._cig
+
+    def poll(self, timeout_ms=100, max_records=4096):
+        """Finished requests: list of dicts (id, score, status, cigar bytes,
+        cigar_score, end_v, end_h, latency_ns)."""
+        recs, cig = self.poll_arrays(timeout_ms, max_records)
+        out = []
+        for r in recs:
+            o, n = int(r["cigar_offset"]), int(r["cigar_length"])
+            out.append({"id": int(r["id"]), "score": int(r["score"]), "status": int(r["status"]),
+                        "cigar": cig[o:o + n].tobytes() if o >= 0 else b"",
+                        "cigar_score": int(r["cigar_score"]), "end_v": int(r["end_v"]),
+                        "end_h": int(r["end_h"]), "latency_ns": int(r["latency_ns"])})
+        return out
+
+    def pending(self):
+        return self._L.wfa_stream_pending(self._s)
+
+    def stats(self):
+        """Kernel launches, launches that ended idle, lane groups that gave up
+        polling, requests re-aligned through the batch path, blocks, lanes."""
+        v = (ctypes.c_int64 * 6)()
+        self._L.wfa_stream_stats(self._s, v, 6)
+        keys = ("launches", "idle_exits", "gave_up", "fallbacks", "blocks", "lanes")
+        return dict(zip(keys, list(v)))
+
+    def stop(self):
+        if self._s:
+            rc = self._L.wfa_stream_stop(self._s)
+            self._s = None
+            if rc != 0:
+                raise RuntimeError(f"wfa_stream_stop: {ERRORS.get(rc, rc)}")
 
     def __del__(self):
         try:

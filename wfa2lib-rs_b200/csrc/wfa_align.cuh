@@ -141,26 +141,100 @@ struct Warp {
 // A group of LW lanes that aligns one pair: LW = 32 is the whole warp; 4, 8
 // or 16 put 8, 4 or 2 pairs in a warp (short pairs, whose wavefronts are a
 // few diagonals wide).  The groups of a warp run the same code on different
-// pairs; every collective names only the group's own lanes.  In the
-// emulation builds the emulated warp is the group.
+// pairs; every collective names only the group's own lanes.  LW = 64, 128,
+// 256 or 512 is a team of LW / 32 whole warps, the whole block (long pairs,
+// whose wavefronts are thousands of diagonals wide): its collectives meet at
+// named barrier 1 (barrier 0 is __syncthreads) and combine the warps'
+// partial results in shared memory.
+// A barrier also orders the team's shared- and global-memory accesses, as
+// __syncwarp does a warp's.  In the emulation builds the emulated warp is
+// the group.
 #if defined(WFA_CUDA_WARP)
 template <int LW>
 struct Lanes {
-  static_assert(LW == 4 || LW == 8 || LW == 16 || LW == 32, "lane group width");
+  static_assert(LW == 4 || LW == 8 || LW == 16 || LW == 32 || LW == 64 || LW == 128 || LW == 256 ||
+                    LW == 512,
+                "lane group width");
+  static constexpr bool TEAM = LW > 32;
+  static constexpr int NW = TEAM ? LW / 32 : 1;  // warps of a team
   static WFA_D unsigned mask() {
-    return LW == 32 ? 0xffffffffu : ((1u << LW) - 1u) << ((threadIdx.x & 31) & ~(LW - 1));
+    return LW >= 32 ? 0xffffffffu : ((1u << LW) - 1u) << ((threadIdx.x & 31) & ~(LW - 1));
   }
   static WFA_D int lane() { return threadIdx.x & (LW - 1); }
-  static WFA_D int min(int v) { return __reduce_min_sync(mask(), v); }
-  static WFA_D int max(int v) { return __reduce_max_sync(mask(), v); }
-  static WFA_D unsigned any(bool p) { return __ballot_sync(mask(), p) & mask(); }
-  static WFA_D void sync() { __syncwarp(mask()); }
+  static WFA_D void sync() {
+    if constexpr (TEAM)
+      asm volatile("bar.sync 1, %0;" ::"n"(LW) : "memory");
+    else
+      __syncwarp(mask());
+  }
+  // One partial per warp of the block: up to 16 warps (512 threads).
+  static WFA_D int* partials() {
+    __shared__ int part[16];
+    return part;
+  }
+  static WFA_D int team_first_warp() { return (int)(threadIdx.x >> 5) & ~(NW - 1); }
+  // The warps' partials of a team, combined after a barrier; a second
+  // barrier keeps the next collective from overwriting them early.
+  static WFA_D int min(int v) {
+    const int w = __reduce_min_sync(mask(), v);
+    if constexpr (!TEAM) {
+      return w;
+    } else {
+      int* part = partials();
+      if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = w;
+      sync();
+      const int b = team_first_warp();
+      int r = part[b];
+#pragma unroll
+      for (int i = 1; i < NW; ++i) r = ::min(r, part[b + i]);
+      sync();
+      return r;
+    }
+  }
+  static WFA_D int max(int v) {
+    const int w = __reduce_max_sync(mask(), v);
+    if constexpr (!TEAM) {
+      return w;
+    } else {
+      int* part = partials();
+      if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = w;
+      sync();
+      const int b = team_first_warp();
+      int r = part[b];
+#pragma unroll
+      for (int i = 1; i < NW; ++i) r = ::max(r, part[b + i]);
+      sync();
+      return r;
+    }
+  }
+  static WFA_D unsigned any(bool p) {
+    if constexpr (!TEAM) return __ballot_sync(mask(), p) & mask();
+    else return (unsigned)max(p ? 1 : 0);
+  }
   // Lanes of the group below this one with p set; *total: the group's lanes
   // with p set.
   static WFA_D int rank(bool p, int* total) {
     const unsigned b = __ballot_sync(mask(), p) & mask();
-    *total = __popc(b);
-    return __popc(b & ((1u << (threadIdx.x & 31)) - 1u));
+    const int below = __popc(b & ((1u << (threadIdx.x & 31)) - 1u));
+    if constexpr (!TEAM) {
+      *total = __popc(b);
+      return below;
+    } else {
+      int* part = partials();
+      if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = __popc(b);
+      sync();
+      const int f = team_first_warp(), me = (int)(threadIdx.x >> 5);
+      int tot = 0, before = 0;
+#pragma unroll
+      for (int i = 0; i < NW; ++i) {
+        const int c = part[f + i];
+        before += f + i < me ? c : 0;
+        tot += c;
+      }
+      sync();
+      *total = tot;
+      return before + below;
+    }
   }
   static WFA_D uint32_t atomic_or(uint32_t* a, uint32_t v) { return atomicOr(a, v); }
 };
@@ -350,6 +424,11 @@ struct PairAligner {
   int16_t dm = 0, d1 = 0, d2 = 0;  // depths: M, I1/D1, I2/D2
   int16_t nm = 0, n1 = 0, n2 = 0;  // next slots: M, piece 1, piece 2
   bool modular;  // score-only: no M history
+  // BiWFA growth phase (breakpoint searches before their overlap scans):
+  // nothing reads an I/D row more than e scores old, so the I/D rows go to
+  // a ring of e + 1 rows per component after the scope x NC rows
+  // (bi_idc_rows), which keeps a search's footprint near M's alone.
+  bool idc = false;
   int32_t cap;   // num_wavefronts score cap (high memory)
   int32_t p0, pf, t0, tf;
   bool endsfree;
@@ -458,6 +537,11 @@ struct PairAligner {
         idx = dm + 2 * d1 + (c == CD2 ? d2 : 0) + n2;
         if (c == CD2) n2 = n2 + 1 == d2 ? 0 : n2 + 1;
       }
+    } else if (idc && c != CM) {
+      const int r1 = P.e1 + 1, r2 = P.e2 + 1;
+      const int depth = (c == CI1 || c == CD1) ? r1 : r2;
+      const int first = c == CI1 ? 0 : c == CD1 ? r1 : c == CI2 ? 2 * r1 : 2 * r1 + r2;
+      idx = (int64_t)scope * NC + first + s % depth;
     } else {
       idx = (int64_t)sidx(s) * NC + c;
     }

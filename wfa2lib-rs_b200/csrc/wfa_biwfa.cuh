@@ -20,26 +20,44 @@ constexpr int32_t kBiFallbackMinScore = 250;
 constexpr int32_t kBiFallbackMinLength = 100;
 constexpr int32_t kBiRecoveryMinScore = 500;
 
-enum BiKind { BI_OK = 0, BI_END_REACHED, BI_UNREACHABLE, BI_MAXSTEPS, BI_UNATTAINABLE, BI_RETRY };
+// BI_RESTART: a breakpoint search reached its overlap scans before the I/D
+// rows they read were kept (the growth phase's I/D ring ended too late); the
+// search runs again with every row kept.
+enum BiKind { BI_OK = 0, BI_END_REACHED, BI_UNREACHABLE, BI_MAXSTEPS, BI_UNATTAINABLE, BI_RETRY, BI_RESTART };
 
 struct BiBreakpoint {  // BiAlignBreakpoint, src/bialign.rs:22-57
   int32_t score, sf, sr, kf, kr, of, orv, comp;
 };
 
-// Per-warp BiWFA workspace.
+// A pending sub-problem of the recursion: pattern [pb, pe), text [tb, te),
+// begin and end components, the score left to it.
+struct BiFrame {
+  int32_t pb, pe, tb, te, cb, ce, remaining;
+};
+// Deepest recursion kept (a pair whose stack would grow past it re-runs).
+constexpr int kBiMaxDepth = 64;
+
+// Per-pair BiWFA workspace (one lane group's).
 struct BiWorkspace {
   Workspace fwd, rev, base;  // ring descriptors + cells; base also history
   uint8_t* rev_seq;          // reversed pattern then reversed text
   uint8_t* cig_tmp;          // base-case CIGAR, written backwards
+  BiFrame* frames;           // the recursion's stack, kBiMaxDepth frames
 };
 
 // Diagonals per lane per pass in the BiWFA aligners (see PairAligner).
-constexpr int kBiUnroll = 4;
+// A warp takes 4 (its wavefronts are many times its width); a team 2 (its
+// width is already a large part of a wavefront, and wider unrolled passes
+// add code -- instruction-fetch stalls -- and registers).
+template <int LW>
+constexpr int bi_unroll() { return LW > 32 ? 2 : 4; }
 
-// GEN = false: no heuristic (the lean aligner instantiation).
-template <int CLS, class S, bool GEN>
+// GEN = false: no heuristic (the lean aligner instantiation).  LW: the lanes
+// of the group aligning the pair (a warp, or a team of warps).
+template <int CLS, class S, bool GEN, int LW = WFA_WARP>
 struct BiDriver {
-  using A = PairAligner<CLS, S, GEN, kBiUnroll>;
+  using A = PairAligner<CLS, S, GEN, bi_unroll<LW>(), LW>;
+  using G = Lanes<LW>;
   static constexpr int NC = A::NC;
   static constexpr bool AFF = A::AFF;
   static constexpr bool TWO = A::TWO;
@@ -50,6 +68,7 @@ struct BiDriver {
   // during the breakpoint searches, which keeps their registers free).
   Workspace base_ws;
   uint8_t* base_cg;
+  BiFrame* stack;
   S pat, txt, rpat, rtxt;  // whole-pair views: forward and reversed
   int32_t n, m, lane;
   uint8_t* cg;  // output CIGAR (forward appends)
@@ -70,6 +89,7 @@ struct BiDriver {
     // short pair's rows sit close together in the warp's slice.
     a.wmax = imin(modular ? P.wmax : P.wmax_base, n + m + 3);
     a.modular = modular;
+    a.idc = false;
     a.endsfree = false;
     a.p0 = a.pf = a.t0 = a.tf = 0;
     a.hist_nc = modular ? 1 : NC;
@@ -98,17 +118,17 @@ struct BiDriver {
   WFA_D void append_run(uint8_t op, int64_t len) {
     if (len <= 0) return;
     if (cg_len + len > cg_cap) { retry = true; return; }
-    for (int64_t i = lane; i < len; i += WFA_WARP) cg[cg_len + i] = op;
+    for (int64_t i = lane; i < len; i += LW) cg[cg_len + i] = op;
     cg_len += len;
   }
   WFA_D void append_base(const A& base) {  // base.cigar [cg_begin, cg_end) forward
     int64_t len = base.cg_end - base.cg_begin;
     if (len <= 0) return;
     if (cg_len + len > cg_cap) { retry = true; return; }
-    Warp::sync();
-    for (int64_t i = lane; i < len; i += WFA_WARP) cg[cg_len + i] = base.cg[base.cg_begin + i];
+    G::sync();
+    for (int64_t i = lane; i < len; i += LW) cg[cg_len + i] = base.cg[base.cg_begin + i];
     cg_len += len;
-    Warp::sync();
+    G::sync();
   }
 
   // bialign_overlap (src/bialign.rs:362-508) and the breakpoint scans
@@ -124,7 +144,7 @@ struct BiDriver {
     if (hi1i < lo0 || hi0 < lo1i) return;
     int mlo = imax(lo0, lo1i), mhi = imin(hi0, hi1i);
     int found = INT_MAX;
-    for (int k0 = mlo + lane; k0 <= mhi; k0 += WFA_WARP) {
+    for (int k0 = mlo + lane; k0 <= mhi; k0 += LW) {
       int k1 = (tlen - plen) - k0;
       int o0 = rd(w0, k0), o1 = rd(w1, k1);
       if (o0 + o1 < tlen) continue;
@@ -135,7 +155,7 @@ struct BiDriver {
       found = k0;
       break;
     }
-    found = Warp::min(found);
+    found = G::min(found);
     if (found == INT_MAX) return;
     int k0 = found, k1 = (tlen - plen) - k0;
     int o0 = rd(w0, k0), o1 = rd(w1, k1);
@@ -177,14 +197,25 @@ struct BiDriver {
     }
   }
 
-  // bialign_find_breakpoint, src/aligner.rs:2958-3124
+  // bialign_find_breakpoint, src/aligner.rs:2958-3124.  full: keep every
+  // score's I/D rows from the start.  Otherwise a long search (more than
+  // kBiIdcMinAd antidiagonals) stores them in the aligners' I/D rings
+  // (PairAligner::idc) while the antidiagonals left to cover exceed a margin:
+  // twice the growth expected over `scope` steps (a running mean) plus twice
+  // the largest recent single-step growth.  The overlap scans need the last
+  // `scope` scores' rows of both aligners; a search that reaches them with
+  // fewer kept returns BI_RESTART.
+  static constexpr int kBiIdcMinAd = 2048;
   WFA_D int find_breakpoint(int pb, int pe, int tb, int te, int cb, int ce, BiBreakpoint& bp,
-                            int32_t& end_score) {
+                            int32_t& end_score, bool full) {
     const int plen = pe - pb, tlen = te - tb;
     set_seqs(fwd, false, pb, pe, tb, te);
     set_seqs(rev, true, pb, pe, tb, te);
     fwd.comp_end = ce;
     rev.comp_end = cb;
+    const int max_ad = plen + tlen - 1;
+    const bool grow_idc = !GEN && AFF && !full && P.bi_idc != 2 && (max_ad > kBiIdcMinAd || P.bi_idc == 1);
+    fwd.idc = rev.idc = grow_idc;
     fwd.init_alignment_component(cb);
     rev.init_alignment_component(ce);
     if (fwd.retry || rev.retry) return BI_RETRY;
@@ -194,12 +225,25 @@ struct BiDriver {
       return (int)BI_UNREACHABLE;
     };
     const int gap_opening = CLS == kAffineClass ? P.o1 : TWO ? imax(P.o1, P.o2) : 0;
-    const int max_ad = plen + tlen - 1;
     int sf = 0, sr = 0, fak = 0, rak = 0, ak = 0;
+    // First scores whose I/D rows are kept (0: all of them); growth of
+    // fak + rak per step pair: 8 x its running mean, its recent maximum.
+    int keep_f = 0, keep_r = 0, mean8 = 64, gmax = 0, last_sum = 0;
     bool last_fwd = false;
     if (fwd.bi_extend(0, true, fak)) return quit(fwd);
     if (rev.bi_extend(0, true, rak)) return quit(rev);
     while (fak + rak < max_ad) {
+      if (fwd.idc && P.bi_idc == 0) {
+        const int g = fak + rak - last_sum;
+        last_sum = fak + rak;
+        mean8 += g - (mean8 >> 3);
+        gmax = imax(g, gmax - (gmax >> 5));
+        if (max_ad - (fak + rak) <= (P.scope * mean8) / 4 + 2 * gmax + 256) {
+          fwd.idc = rev.idc = false;
+          keep_f = sf + 1;
+          keep_r = sr + 1;
+        }
+      }
       ++sf;
       fwd.bi_compute(sf);
       if (fwd.retry) return BI_RETRY;
@@ -218,6 +262,9 @@ struct BiDriver {
       if (sf + sr >= P.max_steps) return BI_MAXSTEPS;
     }
     const int scope = P.scope;
+    if (grow_idc && (fwd.idc || keep_f > imax(0, sf - (scope - 1)) || keep_r > imax(0, sr - (scope - 1))))
+      return BI_RESTART;
+    fwd.idc = rev.idc = false;
     for (;;) {
       if (last_fwd) {
         int min_sr = sr > scope - 1 ? sr - (scope - 1) : 0;
@@ -239,6 +286,12 @@ struct BiDriver {
       last_fwd = true;
     }
     return BI_OK;
+  }
+  WFA_D int find_breakpoint(int pb, int pe, int tb, int te, int cb, int ce, BiBreakpoint& bp,
+                            int32_t& end_score) {
+    int st = find_breakpoint(pb, pe, tb, te, cb, ce, bp, end_score, false);
+    if (st == BI_RESTART) st = find_breakpoint(pb, pe, tb, te, cb, ce, bp, end_score, true);
+    return st;
   }
 
   // bialign_base, src/aligner.rs:3127-3202
@@ -292,20 +345,21 @@ struct BiDriver {
     return st;
   }
 
-  // bialign_recursive, src/aligner.rs:2809-2950, with an explicit stack.
-  struct Frame {
-    int32_t pb, pe, tb, te, cb, ce, remaining;
-  };
-  static constexpr int kMaxDepth = 64;
+  // bialign_recursive, src/aligner.rs:2809-2950, with an explicit stack in
+  // the group's workspace (shared memory in the kernel): lane 0 pushes, and
+  // a sync separates every push from the reads of the frames it writes.
+  WFA_D void push(int& top, const BiFrame& f) {
+    if (lane == 0) stack[top] = f;
+    ++top;
+  }
   WFA_D int recursive(int32_t& result) {
-    Frame stack[kMaxDepth];
     int top = 0;
-    stack[top++] = Frame{0, n, 0, m, CM, CM,
-                         imax(n, m) <= kBiFallbackMinLength ? 0 : INT_MAX};
+    push(top, BiFrame{0, n, 0, m, CM, CM, imax(n, m) <= kBiFallbackMinLength ? 0 : INT_MAX});
     bool first = true;
     int32_t top_result = 0;
     while (top > 0) {
-      Frame f = stack[--top];
+      G::sync();
+      const BiFrame f = stack[--top];
       const int plen = f.pe - f.pb, tlen = f.te - f.tb;
       int32_t r = 0;
       if (tlen == 0) {
@@ -350,19 +404,20 @@ struct BiDriver {
       if (st != BI_OK) return st;
       if (first) top_result = bp.score;
       first = false;
-      if (top + 2 > kMaxDepth) return BI_RETRY;
+      if (top + 2 > kBiMaxDepth) return BI_RETRY;
       const int bph = bp.of, bpv = bp.of - bp.kf;
       // Right half is processed after the left one (pushed first).
-      stack[top++] = Frame{f.pb + bpv, f.pe, f.tb + bph, f.te, bp.comp, f.ce, bp.sr};
-      stack[top++] = Frame{f.pb, f.pb + bpv, f.tb, f.tb + bph, f.cb, bp.comp, bp.sf};
+      G::sync();  // every lane has read the frame popped last
+      push(top, BiFrame{f.pb + bpv, f.pe, f.tb + bph, f.te, bp.comp, f.ce, bp.sr});
+      push(top, BiFrame{f.pb, f.pb + bpv, f.tb, f.tb + bph, f.cb, bp.comp, bp.sf});
     }
     result = top_result;
     return BI_OK;
   }
 };
 
-template <int CLS, class S, bool GEN>
-WFA_D S BiDriver<CLS, S, GEN>::sub(const S& x, int begin, int len) {
+template <int CLS, class S, bool GEN, int LW>
+WFA_D S BiDriver<CLS, S, GEN, LW>::sub(const S& x, int begin, int len) {
   S v = x;
   if constexpr (S::UNITS == 16) {
     v.off = x.off + begin;
@@ -375,11 +430,12 @@ WFA_D S BiDriver<CLS, S, GEN>::sub(const S& x, int begin, int len) {
 
 // align_biwfa (src/aligner.rs:2563-2644) or align_biwfa_score (:2650-2698)
 // of pair `pair`; writes its result.  Returns true to retry with more scratch.
-template <int CLS, class S, bool GEN>
+template <int CLS, class S, bool GEN, int LW = WFA_WARP>
 WFA_D bool biwfa_one(const AlignParams& P, const BiWorkspace& bw, int64_t pair, S pat, S txt,
                      S rpat, S rtxt) {
-  BiDriver<CLS, S, GEN> D(P);
-  D.lane = Warp::lane();
+  using D_t = BiDriver<CLS, S, GEN, LW>;
+  D_t D(P);
+  D.lane = Lanes<LW>::lane();
   D.n = P.p_len[pair];
   D.m = P.t_len[pair];
   D.pat = pat; D.txt = txt; D.rpat = rpat; D.rtxt = rtxt;
@@ -389,6 +445,7 @@ WFA_D bool biwfa_one(const AlignParams& P, const BiWorkspace& bw, int64_t pair, 
   D.setup(D.rev, bw.rev, true);
   D.base_ws = bw.base;
   D.base_cg = bw.cig_tmp;
+  D.stack = bw.frames;
   const int n = D.n, m = D.m;
   int32_t score = 0, status;
   D.cg = nullptr;
@@ -416,7 +473,7 @@ WFA_D bool biwfa_one(const AlignParams& P, const BiWorkspace& bw, int64_t pair, 
     if (st == BI_OK) {
       bool heur = P.hkind != WFA_HEURISTIC_NONE && D.cg_len > 0;
       if (n == 0 || m == 0 || heur) {
-        typename BiDriver<CLS, S, GEN>::A sc(P);
+        typename D_t::A sc(P);
         D.setup(sc, bw.base, false);
         sc.cg = D.cg;
         score = sc.cigar_wfa_score(0, D.cg_len, n, m);
@@ -432,7 +489,7 @@ WFA_D bool biwfa_one(const AlignParams& P, const BiWorkspace& bw, int64_t pair, 
       score = 0;
     }
   }
-  Warp::sync();
+  Lanes<LW>::sync();
   if (D.lane == 0) {
     wfa_result_t r;
     r.score = score;
@@ -451,9 +508,10 @@ WFA_D bool biwfa_one(const AlignParams& P, const BiWorkspace& bw, int64_t pair, 
 }
 
 // Reversed copies of a pair's sequences for the reverse aligner.
+template <int LW = WFA_WARP>
 WFA_D void reverse_into(const SeqPacked& s, uint32_t* out) {
   const int nw = (s.len + 15) >> 4;
-  for (int j = Warp::lane(); j < nw; j += WFA_WARP) {
+  for (int j = Lanes<LW>::lane(); j < nw; j += LW) {
     uint32_t x = s.fetch(s.len - 16 * (j + 1));
     // reverse the order of the sixteen 2-bit codes
     x = ((x >> 2) & 0x33333333u) | ((x & 0x33333333u) << 2);
@@ -463,8 +521,9 @@ WFA_D void reverse_into(const SeqPacked& s, uint32_t* out) {
     out[j] = x;
   }
 }
+template <int LW = WFA_WARP>
 WFA_D void reverse_into(const SeqAscii& s, uint8_t* out) {
-  for (int i = Warp::lane(); i < s.len; i += WFA_WARP) out[i] = s.p[s.len - 1 - i];
+  for (int i = Lanes<LW>::lane(); i < s.len; i += LW) out[i] = s.p[s.len - 1 - i];
 }
 
 }  // namespace wfab

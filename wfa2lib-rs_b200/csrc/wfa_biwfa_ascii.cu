@@ -1,8 +1,8 @@
-// wfa_biwfa_ascii.cu -- lean BiWFA kernels for ASCII sequences.
+// wfa_biwfa_ascii.cu -- lean BiWFA kernels, ASCII sequences, a warp per pair.
 #include "wfa_biwfa_kernels.cuh"
 
 namespace wfab {
 
-template cudaError_t launch_biwfa_enc<WFA_SEQ_ASCII, false>(const AlignParams&, int, int, size_t, cudaStream_t);
+WFA_BIWFA_INSTANCE(WFA_SEQ_ASCII, false, 32)
 
 }  // namespace wfab

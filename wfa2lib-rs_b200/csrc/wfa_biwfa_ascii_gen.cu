@@ -1,8 +1,8 @@
-// wfa_biwfa_ascii_gen.cu -- BiWFA kernels with heuristics, ASCII sequences.
+// wfa_biwfa_ascii_gen.cu -- BiWFA kernels with heuristic support, ASCII sequences, a warp per pair.
 #include "wfa_biwfa_kernels.cuh"
 
 namespace wfab {
 
-template cudaError_t launch_biwfa_enc<WFA_SEQ_ASCII, true>(const AlignParams&, int, int, size_t, cudaStream_t);
+WFA_BIWFA_INSTANCE(WFA_SEQ_ASCII, true, 32)
 
 }  // namespace wfab

@@ -1,8 +1,8 @@
-// wfa_biwfa_packed_gen.cu -- BiWFA kernels with heuristics, 2-bit packed sequences.
+// wfa_biwfa_packed_gen.cu -- BiWFA kernels with heuristic support, 2-bit packed sequences, a warp per pair.
 #include "wfa_biwfa_kernels.cuh"
 
 namespace wfab {
 
-template cudaError_t launch_biwfa_enc<WFA_SEQ_PACKED2, true>(const AlignParams&, int, int, size_t, cudaStream_t);
+WFA_BIWFA_INSTANCE(WFA_SEQ_PACKED2, true, 32)
 
 }  // namespace wfab

@@ -1,0 +1,8 @@
+// wfa_biwfa_packed_t128.cu -- lean BiWFA kernels, 2-bit packed sequences, teams of 4 warps per pair.
+#include "wfa_biwfa_kernels.cuh"
+
+namespace wfab {
+
+WFA_BIWFA_INSTANCE(WFA_SEQ_PACKED2, false, 128)
+
+}  // namespace wfab

@@ -11,6 +11,8 @@
 #include <cub/block/block_scan.cuh>
 
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <condition_variable>
 #include <cstdio>
 #include <cstring>
@@ -25,6 +27,7 @@
 #include "wfa_kernels.h"
 #include "wfa_noalloc.h"
 #include "wfa_params.h"
+#include "wfa_resident.h"
 
 using namespace wfab;
 
@@ -109,6 +112,7 @@ struct wfa_aligner {
   size_t occ_smem = 0;
   int occ_val = 1;
   int lanes_forced = 0;  // lanes per pair of the lean kernel (0: autotuned)
+  int bi_lanes_forced = 0;  // lanes per pair of the BiWFA kernel (0: by length)
   int last_lanes = 0;    // lanes per pair of the last batch's first round
   int launch_lanes = 0;  // lanes per pair of the last launch
   int64_t last_slice_bytes = 0;  // one lane group's scratch slice in the last launch
@@ -716,6 +720,11 @@ static int run_device_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t
   return WFA_OK;
 }
 
+// Lanes per pair of a BiWFA launch whose longest pair has n + m = len: a
+// team of 8 warps from a few kbp (measured fastest on 2.5-3 kbp pairs and
+// on the 1-20 kbp batch), 4 warps for kilobase pairs.
+static int biwfa_default_lanes(int32_t len) { return len > 3000 ? 256 : len > 1000 ? 128 : 32; }
+
 // BiWFA batch: the same round structure as run_device_batch with the BiWFA
 // kernel and its workspace layout.
 static int run_biwfa_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* d_results,
@@ -743,8 +752,13 @@ static int run_biwfa_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t*
   cfg.hist_scores = 1024 * nc;
   cfg.hist_words = (int64_t)nc * 600 * 600;
   const size_t budget = scratch_budget(h);
-  const size_t smem = (size_t)kWarpsPerBlock * 3 * P.scope * nc * kDescBytes;
+  const int lanes = bi_lanes_built(h->bi_lanes_forced ? h->bi_lanes_forced : biwfa_default_lanes(max_len_sum),
+                                   P.hkind != WFA_HEURISTIC_NONE);
+  const int gpb = bi_groups_per_block(lanes);
+  const size_t smem = bi_smem_bytes(lanes, P.scope, nc);
   if (smem > 200 * 1024) return fail(h, WFA_ERR_UNSUPPORTED, "wavefront ring too large");
+  h->last_lanes = lanes;
+  h->launch_lanes = lanes;
   int64_t todo = b->num_pairs;
   const int64_t* list = nullptr;
   h->last_kernel_ms = 0.0;
@@ -775,12 +789,15 @@ static int run_biwfa_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t*
   for (int round = 0; todo > 0; ++round) {
     if (round > 8) return fail(h, WFA_ERR_OOM, "alignment needs more scratch than available");
     const BiLayout L = bi_layout(P.scope, nc, cfg.wmax, wbase, cfg.hist_scores, cfg.hist_words,
-                                 max_len_sum);
-    int64_t max_warps = (int64_t)h->num_sms * 2 * kWarpsPerBlock;
-    int64_t warps = std::max<int64_t>(std::min<int64_t>(max_warps, todo), 1);
-    while (warps > 1 && (size_t)warps * L.words * 4 > budget) warps = warps * 3 / 4;
-    int blocks = (int)((warps + kWarpsPerBlock - 1) / kWarpsPerBlock);
-    CUDA_TRY(h, h->scratch.ensure((size_t)blocks * kWarpsPerBlock * L.words * 4), "scratch");
+                                 max_len_sum, bi_idc_rows(nc, P.e1, P.e2));
+    // One wave of resident blocks, no more groups than pairs, and the
+    // groups' slices within the scratch budget.
+    const int bpsm = std::max(1, occupancy_biwfa(P, cls, lanes, smem));
+    int64_t max_groups = (int64_t)h->num_sms * bpsm * gpb;
+    int64_t groups = std::max<int64_t>(std::min<int64_t>(max_groups, todo), 1);
+    while (groups > 1 && (size_t)groups * L.words * 4 > budget) groups = groups * 3 / 4;
+    int blocks = (int)((groups + gpb - 1) / gpb);
+    CUDA_TRY(h, h->scratch.ensure((size_t)blocks * gpb * L.words * 4), "scratch");
     P.scratch = h->scratch.as<int32_t>();
     P.warp_words = L.words;
     P.wmax = cfg.wmax;
@@ -792,7 +809,7 @@ static int run_biwfa_batch(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t*
     CUDA_TRY(h, cudaMemsetAsync(P.work_counter, 0, 16, st), "memset");
     CUDA_TRY(h, cudaEventRecord(h->ev0, st), "event");
     CUDA_TRY(h, cudaGetLastError(), "an earlier CUDA call of this thread");
-    CUDA_TRY(h, launch_biwfa(P, cls, blocks, smem, st), "BiWFA kernel launch");
+    CUDA_TRY(h, launch_biwfa(P, cls, lanes, blocks, smem, st), "BiWFA kernel launch");
     CUDA_TRY(h, cudaEventRecord(h->ev1, st), "event");
     h->launches++;
     int32_t retries = 0;
@@ -1276,6 +1293,11 @@ int64_t wfa_last_rerun_pairs(const wfa_aligner_t* h) { return h ? h->last_reruns
 int wfa_set_lanes_per_pair(wfa_aligner_t* h, int32_t lanes) {
   if (!h || !(lanes == 0 || lanes == 4 || lanes == 8 || lanes == 16 || lanes == 32)) return WFA_ERR_ARGUMENT;
   h->lanes_forced = lanes;
+  return WFA_OK;
+}
+int wfa_set_biwfa_lanes(wfa_aligner_t* h, int32_t lanes) {
+  if (!h || !(lanes == 0 || lanes == 32 || lanes == 128 || lanes == 256 || lanes == 512)) return WFA_ERR_ARGUMENT;
+  h->bi_lanes_forced = lanes;
   return WFA_OK;
 }
 int32_t wfa_last_lanes_per_pair(const wfa_aligner_t* h) { return h ? h->last_lanes : 0; }
@@ -1791,5 +1813,394 @@ int32_t wfa_cigar_rle(const uint8_t* ops, int32_t len, char* out, int32_t cap) {
 }
 
 const char* wfa_version(void) { return "wfa2lib-rs_b200 0.1 (sm_100a)"; }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Resident stream (wfa_stream_*): a persistent kernel (wfa_resident.cu) fed
+// from a request ring in mapped host memory.  Host side: the ring and its
+// slots' bookkeeping, the kernel's launches and relaunches, the results.
+// ---------------------------------------------------------------------------
+namespace {
+
+using StreamClock = std::chrono::steady_clock;
+
+template <class T>
+T* host_mapped(size_t count, T** dev) {
+  void* p = nullptr;
+  if (cudaHostAlloc(&p, std::max<size_t>(count * sizeof(T), 64), cudaHostAllocMapped) != cudaSuccess) return nullptr;
+  std::memset(p, 0, std::max<size_t>(count * sizeof(T), 64));
+  void* d = nullptr;
+  if (cudaHostGetDevicePointer(&d, p, 0) != cudaSuccess) {
+    cudaFreeHost(p);
+    return nullptr;
+  }
+  *dev = reinterpret_cast<T*>(d);
+  return reinterpret_cast<T*>(p);
+}
+
+// Polls of the doorbell (about 1.5 us each) without a new request before a
+// launch ends, and a lane group's polls (backing off to about 8 us) before it
+// gives up.
+constexpr int64_t kStreamIdlePolls = 700000;
+constexpr int64_t kStreamGroupPolls = 4000000;
+
+}  // namespace
+
+struct wfa_stream {
+  wfa_aligner_t* h = nullptr;   // the kernel's handle: its stream and scratch
+  wfa_aligner_t* fb = nullptr;  // requests that outgrow the kernel's scratch (made on first need)
+  int metric = 0;
+  wfa_penalties_t pen{};
+  int score_only = 0;
+  // Mapped host memory (host views; the device views are in R).
+  ResidentCtl* ctl = nullptr;
+  ResidentReq* reqs = nullptr;
+  uint8_t* arena = nullptr;
+  wfa_result_t* results = nullptr;
+  uint8_t* cigars = nullptr;
+  uint32_t* done = nullptr;
+  unsigned long long* xfer = nullptr;  // pinned word for the device counters
+  DevBuf dev;                          // head, dtail, dstop
+  ResidentArgs R{};
+  AlignParams P{};
+  int cls = 0, lanes = 32, blocks = 0;
+  size_t smem = 0;
+  int64_t cap = 0;
+  int32_t max_len_sum = 0;
+  std::mutex mu;
+  uint64_t tail = 0, oldest = 0;
+  std::vector<int64_t> t_submit;  // per slot (steady clock ns)
+  std::vector<uint8_t> taken;     // per slot: its result was returned
+  bool running = false;
+  cudaEvent_t ended = nullptr;
+  int64_t launches = 0, fallbacks = 0;
+  std::string err;
+};
+
+namespace {
+
+void stream_free(wfa_stream_t* s) {
+  if (s->ended) cudaEventDestroy(s->ended);
+  for (void* p : {(void*)s->ctl, (void*)s->reqs, (void*)s->arena, (void*)s->results, (void*)s->cigars,
+                  (void*)s->done, (void*)s->xfer})
+    if (p) cudaFreeHost(p);
+  s->dev.release();
+  if (s->h) wfa_aligner_destroy(s->h);
+  if (s->fb) wfa_aligner_destroy(s->fb);
+  delete s;
+}
+
+// Launches the kernel over what is published (caller holds mu).
+int stream_launch(wfa_stream_t* s) {
+  wfa_aligner_t* h = s->h;
+  *s->xfer = s->tail;
+  CUDA_TRY(h, cudaMemcpyAsync(s->R.dtail, s->xfer, 8, cudaMemcpyHostToDevice, h->stream), "stream tail");
+  CUDA_TRY(h, cudaMemsetAsync(s->R.dstop, 0, 4, h->stream), "stream stop flag");
+  CUDA_TRY(h, cudaGetLastError(), "an earlier CUDA call of this thread");
+  CUDA_TRY(h, launch_resident(s->P, s->R, s->cls, s->lanes, s->blocks, s->smem, h->stream),
+           "resident kernel launch");
+  CUDA_TRY(h, cudaEventRecord(s->ended, h->stream), "event");
+  s->running = true;
+  ++s->launches;
+  ++h->launches;
+  return WFA_OK;
+}
+
+// Notices the end of a launch; relaunches when requests were published that
+// no launch claimed (caller holds mu).
+int stream_tend(wfa_stream_t* s) {
+  if (!s->err.empty()) return WFA_ERR_CUDA;
+  wfa_aligner_t* h = s->h;
+  if (s->running) {
+    const cudaError_t q = cudaEventQuery(s->ended);
+    if (q == cudaErrorNotReady) return WFA_OK;
+    if (q != cudaSuccess) {
+      s->err = std::string("resident kernel: ") + cudaGetErrorString(q);
+      s->running = false;
+      return WFA_ERR_CUDA;
+    }
+    s->running = false;
+  }
+  if (s->tail == 0) return WFA_OK;
+  CUDA_TRY(h, cudaMemcpyAsync(s->xfer, s->R.head, 8, cudaMemcpyDeviceToHost, h->stream), "stream head");
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream), "stream head");
+  if (*s->xfer < s->tail) return stream_launch(s);
+  return WFA_OK;
+}
+
+void publish(wfa_stream_t* s) {
+  std::atomic_thread_fence(std::memory_order_release);
+  *reinterpret_cast<volatile unsigned long long*>(&s->ctl->tail) = s->tail;
+}
+
+int64_t stream_put(wfa_stream_t* s, const uint8_t* p, int32_t n, const uint8_t* t, int32_t m,
+                   int64_t now) {
+  const int64_t i = (int64_t)(s->tail % (uint64_t)s->cap);
+  s->reqs[i] = ResidentReq{n, m};
+  uint8_t* a = s->arena + i * s->R.seq_stride;
+  if (n) std::memcpy(a, p, (size_t)n);
+  if (m) std::memcpy(a + n, t, (size_t)m);
+  s->t_submit[(size_t)i] = now;
+  s->taken[(size_t)i] = 0;
+  return (int64_t)s->tail++;
+}
+
+int64_t now_ns() {
+  return std::chrono::duration_cast<std::chrono::nanoseconds>(StreamClock::now().time_since_epoch()).count();
+}
+
+// The result of slot i through the host-buffer batch path (a request whose
+// alignment outgrew the kernel's scratch).
+int stream_fallback(wfa_stream_t* s, int64_t i, wfa_result_t* r, std::vector<uint8_t>* cig) {
+  if (!s->fb) {
+    int e = WFA_OK;
+    s->fb = wfa_aligner_create((wfa_metric_t)s->metric, &s->pen, s->h->device, &e);
+    if (!s->fb) return e;
+    wfa_set_alignment_scope(s->fb, s->score_only ? WFA_SCOPE_SCORE : WFA_SCOPE_ALIGNMENT);
+  }
+  const ResidentReq q = s->reqs[i];
+  const int64_t po = 0, to = q.n;
+  const int32_t pl = q.n, tl = q.m;
+  wfa_batch_t b{};
+  b.format = WFA_SEQ_ASCII;
+  b.span = WFA_SPAN_END2END;
+  b.num_pairs = 1;
+  b.seq = s->arena + i * s->R.seq_stride;
+  b.seq_bytes = (int64_t)q.n + q.m;
+  b.p_off = &po;
+  b.p_len = &pl;
+  b.t_off = &to;
+  b.t_len = &tl;
+  cig->assign(2 * ((size_t)q.n + q.m) + 16, 0);
+  ++s->fallbacks;
+  return wfa_batch_align(s->fb, &b, r, s->score_only ? nullptr : cig->data());
+}
+
+}  // namespace
+
+extern "C" {
+
+wfa_stream_t* wfa_stream_start(wfa_metric_t metric, const wfa_penalties_t* penalties, int32_t device,
+                               int32_t score_only, int32_t max_len_sum, int32_t capacity,
+                               int32_t blocks_per_sm, int* err) {
+  auto bad = [&](int e) -> wfa_stream_t* {
+    if (err) *err = e;
+    return nullptr;
+  };
+  if (max_len_sum < 1 || max_len_sum > kLongPair || capacity < 1 || blocks_per_sm < 0)
+    return bad(WFA_ERR_ARGUMENT);
+  int e = WFA_OK;
+  wfa_aligner_t* h = wfa_aligner_create(metric, penalties, device, &e);
+  if (!h) return bad(e);
+  wfa_stream_t* s = new wfa_stream();
+  s->h = h;
+  s->metric = metric;
+  if (penalties) s->pen = *penalties;
+  s->score_only = score_only ? 1 : 0;
+  s->cap = capacity;
+  s->max_len_sum = max_len_sum;
+  wfa_set_alignment_scope(h, score_only ? WFA_SCOPE_SCORE : WFA_SCOPE_ALIGNMENT);
+  // Launch shape: the first round of a host batch of such pairs.
+  wfa_batch_t b{};
+  b.format = WFA_SEQ_ASCII;
+  b.span = WFA_SPAN_END2END;
+  fill_params(h, &b, s->P);
+  s->cls = metric_class(s->P.metric);
+  const int nc = metric_components(s->P.metric);
+  s->lanes = max_len_sum <= 512 ? 8 : 32;
+  Round r = first_round(s->P, nc, max_len_sum, s->lanes, true, max_len_sum);
+  int64_t group_words = 0;
+  SmemLayout L = round_layout(s->P, r, nc, &group_words);
+  if (L.total > 200 * 1024 && s->lanes == 8) {
+    s->lanes = 32;
+    r = first_round(s->P, nc, max_len_sum, s->lanes, true, max_len_sum);
+    L = round_layout(s->P, r, nc, &group_words);
+  }
+  if (L.total > 200 * 1024) {
+    stream_free(s);
+    return bad(WFA_ERR_UNSUPPORTED);
+  }
+  s->smem = L.total;
+  const int64_t seq_stride = ((int64_t)max_len_sum + 16 + 15) & ~(int64_t)15;
+  const int64_t cig_stride = (2 * (int64_t)max_len_sum + 1 + 15) & ~(int64_t)15;
+  // After the ring and history: the request's bytes and its CIGAR.
+  group_words = ((group_words + (seq_stride + cig_stride) / 4) + 63) & ~(int64_t)63;
+  int occ = occupancy_resident(s->cls, s->lanes, s->smem);
+  if (blocks_per_sm > 0) occ = std::min(occ, (int)blocks_per_sm);
+  s->blocks = h->num_sms * std::max(1, occ);
+  const int gpb = kWarpsPerBlock * 32 / s->lanes;
+  bool ok = h->scratch.ensure((size_t)s->blocks * gpb * group_words * 4) == cudaSuccess &&
+            s->dev.ensure(64) == cudaSuccess;
+  s->dev.st = h->stream;
+  ok = ok && cudaMemsetAsync(s->dev.p, 0, 64, h->stream) == cudaSuccess &&
+       cudaStreamSynchronize(h->stream) == cudaSuccess && cudaEventCreate(&s->ended) == cudaSuccess;
+  ResidentArgs& R = s->R;
+  ResidentCtl* ctl_d = nullptr;
+  ResidentReq* reqs_d = nullptr;
+  uint8_t *arena_d = nullptr, *cig_d = nullptr;
+  wfa_result_t* res_d = nullptr;
+  uint32_t* done_d = nullptr;
+  unsigned long long* xfer_d = nullptr;
+  ok = ok && (s->ctl = host_mapped<ResidentCtl>(1, &ctl_d)) && (s->reqs = host_mapped<ResidentReq>((size_t)s->cap, &reqs_d)) &&
+       (s->arena = host_mapped<uint8_t>((size_t)(s->cap * seq_stride), &arena_d)) &&
+       (s->results = host_mapped<wfa_result_t>((size_t)s->cap, &res_d)) &&
+       (s->cigars = host_mapped<uint8_t>((size_t)(s->cap * cig_stride), &cig_d)) &&
+       (s->done = host_mapped<uint32_t>((size_t)s->cap, &done_d)) &&
+       (s->xfer = host_mapped<unsigned long long>(1, &xfer_d));
+  if (!ok) {
+    cudaGetLastError();
+    stream_free(s);
+    return bad(WFA_ERR_OOM);
+  }
+  s->P.scratch = h->scratch.as<int32_t>();
+  s->P.warp_words = group_words;
+  R.ctl = ctl_d;
+  R.reqs = reqs_d;
+  R.arena = arena_d;
+  R.results = res_d;
+  R.cigars = cig_d;
+  R.done = done_d;
+  R.cap = s->cap;
+  R.seq_stride = seq_stride;
+  R.cig_stride = cig_stride;
+  unsigned long long* d = s->dev.as<unsigned long long>();
+  R.head = d;
+  R.dtail = d + 1;
+  R.dstop = reinterpret_cast<int32_t*>(d + 2);
+  R.idle_polls = kStreamIdlePolls;
+  R.group_polls = kStreamGroupPolls;
+  s->t_submit.assign((size_t)s->cap, 0);
+  s->taken.assign((size_t)s->cap, 0);
+  if (err) *err = WFA_OK;
+  return s;
+}
+
+int64_t wfa_stream_submit(wfa_stream_t* s, const uint8_t* pattern, int32_t n, const uint8_t* text, int32_t m) {
+  if (!s || n < 0 || m < 0 || (n > 0 && !pattern) || (m > 0 && !text) || (int64_t)n + m > s->max_len_sum)
+    return WFA_ERR_ARGUMENT;
+  const int64_t now = now_ns();
+  std::lock_guard<std::mutex> lock(s->mu);
+  if (!s->err.empty()) return WFA_ERR_CUDA;
+  if ((int64_t)(s->tail - s->oldest) >= s->cap) return WFA_ERR_BUSY;
+  const int64_t id = stream_put(s, pattern, n, text, m, now);
+  publish(s);
+  const int rc = stream_tend(s);
+  return rc == WFA_OK ? id : rc;
+}
+
+int64_t wfa_stream_submit_many(wfa_stream_t* s, const uint8_t* seq, const int64_t* p_off, const int32_t* p_len,
+                               const int64_t* t_off, const int32_t* t_len, int64_t count) {
+  if (!s || count < 0 || (count > 0 && (!seq || !p_off || !p_len || !t_off || !t_len))) return WFA_ERR_ARGUMENT;
+  for (int64_t j = 0; j < count; ++j)
+    if (p_len[j] < 0 || t_len[j] < 0 || (int64_t)p_len[j] + t_len[j] > s->max_len_sum) return WFA_ERR_ARGUMENT;
+  const int64_t now = now_ns();
+  std::lock_guard<std::mutex> lock(s->mu);
+  if (!s->err.empty()) return WFA_ERR_CUDA;
+  if ((int64_t)(s->tail - s->oldest) + count > s->cap) return WFA_ERR_BUSY;
+  const int64_t first = (int64_t)s->tail;
+  for (int64_t j = 0; j < count; ++j) stream_put(s, seq + p_off[j], p_len[j], seq + t_off[j], t_len[j], now);
+  publish(s);
+  const int rc = stream_tend(s);
+  return rc == WFA_OK ? first : rc;
+}
+
+int32_t wfa_stream_poll(wfa_stream_t* s, wfa_served_t* out, int32_t max, uint8_t* cigars, int64_t cigar_cap,
+                        int32_t timeout_ms) {
+  if (!s || !out || max <= 0) return WFA_ERR_ARGUMENT;
+  const auto deadline = StreamClock::now() + std::chrono::milliseconds(std::max(0, timeout_ms));
+  std::vector<uint8_t> fcig;
+  for (;;) {
+    {
+      std::lock_guard<std::mutex> lock(s->mu);
+      if (!s->err.empty()) return WFA_ERR_CUDA;
+      int32_t c = 0;
+      int64_t used = 0;
+      for (uint64_t q = s->oldest; q < s->tail && c < max; ++q) {
+        const int64_t i = (int64_t)(q % (uint64_t)s->cap);
+        if (s->taken[(size_t)i]) continue;
+        const uint32_t mark = *reinterpret_cast<volatile uint32_t*>(s->done + i);
+        if (mark != (uint32_t)(q / (uint64_t)s->cap) + 1u) continue;
+        std::atomic_thread_fence(std::memory_order_acquire);
+        const int64_t t_done = now_ns();
+        wfa_result_t r = s->results[i];
+        const uint8_t* ops = s->cigars + i * s->R.cig_stride;
+        if (r.status == kStatusRetry) {
+          const int rc = stream_fallback(s, i, &r, &fcig);
+          if (rc != WFA_OK) {
+            r.status = rc;
+            r.score = 0;
+            r.cigar_length = 0;
+          }
+          ops = fcig.data() + r.cigar_begin;
+        }
+        const int64_t len = s->score_only ? 0 : r.cigar_length;
+        wfa_served_t& o = out[c];
+        std::memset(&o, 0, sizeof o);
+        o.cigar_offset = -1;
+        if (len > 0) {
+          if (!cigars || used + len > cigar_cap) {
+            if (c == 0) return WFA_ERR_ARGUMENT;  // the next CIGAR does not fit the buffer
+            break;
+          }
+          std::memcpy(cigars + used, ops, (size_t)len);
+          o.cigar_offset = used;
+          used += len;
+        }
+        o.id = (int64_t)q;
+        o.score = r.score;
+        o.status = r.status;
+        o.cigar_length = (int32_t)len;
+        o.cigar_score = r.cigar_score;
+        o.end_v = r.end_v;
+        o.end_h = r.end_h;
+        o.mode = 0;
+        o.latency_ns = t_done - s->t_submit[(size_t)i];
+        s->taken[(size_t)i] = 1;
+        ++c;
+      }
+      while (s->oldest < s->tail && s->taken[(size_t)(s->oldest % (uint64_t)s->cap)]) {
+        s->taken[(size_t)(s->oldest % (uint64_t)s->cap)] = 0;
+        ++s->oldest;
+      }
+      if (c > 0) return c;
+      const int rc = stream_tend(s);
+      if (rc != WFA_OK) return rc;
+    }
+    if (StreamClock::now() >= deadline) return 0;
+    std::this_thread::sleep_for(std::chrono::microseconds(10));
+  }
+}
+
+int64_t wfa_stream_pending(wfa_stream_t* s) {
+  if (!s) return WFA_ERR_ARGUMENT;
+  std::lock_guard<std::mutex> lock(s->mu);
+  return (int64_t)(s->tail - s->oldest);
+}
+
+int wfa_stream_stats(wfa_stream_t* s, int64_t* out, int32_t n) {
+  if (!s || !out || n < 0) return WFA_ERR_ARGUMENT;
+  std::lock_guard<std::mutex> lock(s->mu);
+  const int64_t v[6] = {s->launches, (int64_t)s->ctl->idle_exits, (int64_t)s->ctl->gave_up, s->fallbacks,
+                        s->blocks, s->lanes};
+  for (int32_t j = 0; j < n && j < 6; ++j) out[j] = v[j];
+  return WFA_OK;
+}
+
+int wfa_stream_stop(wfa_stream_t* s) {
+  if (!s) return WFA_ERR_ARGUMENT;
+  int rc = WFA_OK;
+  {
+    // With stop set, a running launch (or one started here for requests no
+    // launch claimed) aligns what was published and returns.
+    std::lock_guard<std::mutex> lock(s->mu);
+    *reinterpret_cast<volatile int32_t*>(&s->ctl->stop) = 1;
+    std::atomic_thread_fence(std::memory_order_seq_cst);
+    rc = stream_tend(s);
+  }
+  if (cudaStreamSynchronize(s->h->stream) != cudaSuccess) rc = WFA_ERR_CUDA;
+  stream_free(s);
+  return rc;
+}
 
 }  // extern "C"

@@ -46,6 +46,10 @@ struct AlignParams {
   // Compat: 0 C (reproduce C's known bugs), 1 Corrected (src/aligner.rs:53-94).
   int32_t compat;
   int32_t max_steps;
+  // BiWFA growth-phase I/D rings (BiDriver::find_breakpoint): 0 as chosen
+  // by the search's length; 1 (tests) kept until the overlap scans, so that
+  // every search restarts; 2 off.
+  int32_t bi_idc;
   // Input.
   int32_t format;  // wfa_seq_format_t
   const uint8_t* seq;
@@ -125,6 +129,14 @@ __host__ __device__
 #endif
 inline int compact_desc_depth(const AlignParams& P, int cls) {
   return ((P.scope - 1) >> score_shift(score_step(P, cls))) + 1;
+}
+#if defined(__CUDACC__)
+__host__ __device__
+#endif
+inline int bi_idc_rows(int nc, int e1, int e2) {
+  // BiWFA's growth phase keeps its I/D rows in a ring of their own after the
+  // scope x NC rows: e + 1 rows for each of I and D of a piece.
+  return nc >= 3 ? 2 * (e1 + 1) + (nc == 5 ? 2 * (e2 + 1) : 0) : 0;
 }
 #if defined(__CUDACC__)
 __host__ __device__

@@ -9,6 +9,7 @@ namespace wfab {
 constexpr int kWarpsPerBlock = 4;
 constexpr int kMinBlocksPerSM = 6;  // register budget: 65536 / (6 * 128) = 85 per thread
 constexpr int kDescBytes = 32;      // sizeof(WfD)
+constexpr int kBiFrameBytes = 64 * 7 * 4;  // kBiMaxDepth BiFrames (the BiWFA recursion's stack)
 
 // Per-block dynamic shared memory of the unidirectional kernel: descriptor
 // rings, staged sequences and (optionally) ring cells, each as one slice per
@@ -68,8 +69,10 @@ inline int64_t slice_bt_words(const AlignParams& P) {
   return (2 * (int64_t)P.bt_cap + 2 * (int64_t)P.bt_init_cap + marks + 3) & ~(int64_t)3;
 }
 
-// BiWFA per-warp scratch slice (int32 word offsets).  seq_len_sum is the
-// longest n + m of the launch (sizes the reversed sequences and the base CIGAR).
+// BiWFA per-group scratch slice (int32 word offsets).  seq_len_sum is the
+// longest n + m of the launch (sizes the reversed sequences and the base
+// CIGAR); idc_rows: the forward and reverse rings' extra rows
+// (bi_idc_rows).
 // The forward and reverse rings are wmax cells wide; the base-case ring only
 // wmax_base: a base case ends by score 500 (plus one scope), and a wavefront
 // at score s spans at most 2s + 1 diagonals.
@@ -80,9 +83,9 @@ struct BiLayout {
 __host__ __device__
 #endif
 inline BiLayout bi_layout(int scope, int nc, int wmax, int wmax_base, int hist_scores,
-                          int64_t hist_words, int seq_len_sum) {
+                          int64_t hist_words, int seq_len_sum, int idc_rows) {
   BiLayout L;
-  const int64_t ring = ((int64_t)scope * nc * wmax + 3) & ~(int64_t)3;
+  const int64_t ring = (((int64_t)scope * nc + idc_rows) * wmax + 3) & ~(int64_t)3;
   const int64_t ring_b = ((int64_t)scope * nc * wmax_base + 3) & ~(int64_t)3;
   L.ring_f = 0;
   L.ring_r = L.ring_f + ring;
@@ -111,7 +114,20 @@ cudaError_t launch_order_scatter(const uint16_t* keys, int64_t n, const int32_t*
                                  int64_t* list, int num_sms, cudaStream_t st);
 
 bool needs_general(const AlignParams& P);
-cudaError_t launch_biwfa(const AlignParams& P, int cls, int blocks, size_t smem, cudaStream_t st);
+// BiWFA: lanes per pair 32 (a warp) or 128, 256, 512 (a team of warps; the
+// lean kernels only -- the kernels with heuristic support take 32 whatever
+// is asked); blocks of bi_block_threads(lanes) threads, bi_groups_per_block
+// pairs at a time, bi_smem_bytes of dynamic shared memory.
+constexpr int bi_block_threads(int lanes) { return lanes > 128 ? lanes : 128; }
+inline int bi_lanes_built(int lanes, bool gen) {
+  return gen ? 32 : (lanes == 128 || lanes == 256 || lanes == 512) ? lanes : 32;
+}
+inline int bi_groups_per_block(int lanes) { return bi_block_threads(lanes) / lanes; }
+inline size_t bi_smem_bytes(int lanes, int scope, int nc) {
+  return (size_t)bi_groups_per_block(lanes) * (3 * (size_t)scope * nc * kDescBytes + kBiFrameBytes);
+}
+cudaError_t launch_biwfa(const AlignParams& P, int cls, int lanes, int blocks, size_t smem, cudaStream_t st);
+int occupancy_biwfa(const AlignParams& P, int cls, int lanes, size_t smem);
 // Lanes per pair: 4, 8, 16 or 32 (32 / lanes pairs per warp).
 cudaError_t launch_unialign(const AlignParams& P, int metric_class, int lanes, int blocks, size_t smem,
                             cudaStream_t st);

@@ -10,6 +10,11 @@
 // files the results for pollers.  Several batches are on the GPU at once,
 // short requests never queue behind long batches, and a request that
 // arrives while batches run joins the next batch a worker of its lane forms.
+//
+// With `resident` set, the short lane is a resident stream instead
+// (wfa_stream_*: a persistent kernel that takes requests as they come): a
+// collector thread moves its results to the finished list, and a short
+// request that finds the stream's ring full takes the batch lane.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -17,6 +22,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -64,10 +70,57 @@ struct wfa_server {
   int64_t next_id = 0;
   int64_t outstanding = 0;  // submitted and not yet polled
   std::string last_error;   // of the last failed batch
+  // Resident short lane: the stream, its requests (stream id -> server id,
+  // submit time), the collector thread.
+  wfa_stream_t* stream = nullptr;
+  std::map<int64_t, std::pair<int64_t, Clock::time_point>> in_stream;
+  std::thread collector;
 
   void run_batch(wfa_aligner_t* h, std::vector<Request>& reqs, int span);
   void worker(int w);
+  void collect();
 };
+
+void wfa_server::collect() {
+  std::vector<wfa_served_t> recs(4096);
+  std::vector<uint8_t> cig((size_t)4096 * (2 * (size_t)cfg.short_max_len + 1));
+  for (;;) {
+    const int32_t c = wfa_stream_poll(stream, recs.data(), (int32_t)recs.size(), cig.data(),
+                                      (int64_t)cig.size(), 2);
+    const Clock::time_point t1 = Clock::now();
+    std::lock_guard<std::mutex> lock(mu);
+    if (c < 0) {
+      // The stream failed: its outstanding requests carry the error code.
+      last_error = "resident stream failed";
+      for (auto& kv : in_stream) {
+        Finished f;
+        std::memset(&f.rec, 0, sizeof f.rec);
+        f.rec.id = kv.second.first;
+        f.rec.status = c;
+        f.rec.cigar_offset = -1;
+        done.push_back(std::move(f));
+      }
+      in_stream.clear();
+      cv_done.notify_all();
+      return;
+    }
+    for (int32_t j = 0; j < c; ++j) {
+      const wfa_served_t& r = recs[(size_t)j];
+      auto it = in_stream.find(r.id);
+      if (it == in_stream.end()) continue;
+      Finished f;
+      f.rec = r;
+      f.rec.id = it->second.first;
+      f.rec.cigar_offset = -1;
+      f.rec.latency_ns = std::chrono::duration_cast<std::chrono::nanoseconds>(t1 - it->second.second).count();
+      if (r.cigar_length > 0) f.cigar.assign(cig.begin() + r.cigar_offset, cig.begin() + r.cigar_offset + r.cigar_length);
+      in_stream.erase(it);
+      done.push_back(std::move(f));
+    }
+    if (c > 0) cv_done.notify_all();
+    if (stopping && in_stream.empty()) return;
+  }
+}
 
 void wfa_server::run_batch(wfa_aligner_t* h, std::vector<Request>& reqs, int span) {
   if (reqs.empty()) return;
@@ -196,6 +249,20 @@ wfa_server_t* wfa_server_start(const wfa_server_config_t* config, int* err) {
     wfa_set_alignment_scope(h, s->cfg.score_only ? WFA_SCOPE_SCORE : WFA_SCOPE_ALIGNMENT);
     s->handles.push_back(h);
   }
+  if (s->cfg.resident) {
+    // The resident short lane holds one block per SM, so that the batch
+    // lanes' kernels find room beside it.
+    int e = WFA_OK;
+    s->stream = wfa_stream_start((wfa_metric_t)s->cfg.metric, &s->cfg.penalties, s->cfg.device, s->cfg.score_only,
+                                 std::min(s->cfg.short_max_len, 2048), 1 << 16, 1, &e);
+    if (!s->stream) {
+      for (wfa_aligner_t* x : s->handles) wfa_aligner_destroy(x);
+      delete s;
+      if (err) *err = e;
+      return nullptr;
+    }
+    s->collector = std::thread(&wfa_server::collect, s);
+  }
   for (size_t w = 0; w < s->lane_of.size(); ++w) s->threads.emplace_back(&wfa_server::worker, s, (int)w);
   if (err) *err = WFA_OK;
   return s;
@@ -222,6 +289,14 @@ int64_t wfa_server_submit(wfa_server_t* s, const uint8_t* pattern, int32_t n, co
     if (s->stopping) return WFA_ERR_ARGUMENT;
     id = r.id = s->next_id++;
     ++s->outstanding;
+    if (lane == 0 && s->stream) {
+      const int64_t sid = wfa_stream_submit(s->stream, pattern, n, text, m);
+      if (sid >= 0) {
+        s->in_stream[sid] = std::make_pair(id, r.t0);
+        return id;
+      }
+      // ring full (or the stream failed): the batch lane takes it
+    }
     s->queue[lane].push_back(std::move(r));
   }
   s->cv_work[lane].notify_one();
@@ -275,6 +350,10 @@ int wfa_server_stop(wfa_server_t* s) {
   }
   for (auto& cv : s->cv_work) cv.notify_all();
   for (std::thread& t : s->threads) t.join();
+  if (s->stream) {
+    s->collector.join();
+    wfa_stream_stop(s->stream);
+  }
   for (wfa_aligner_t* h : s->handles) wfa_aligner_destroy(h);
   delete s;
   return WFA_OK;
