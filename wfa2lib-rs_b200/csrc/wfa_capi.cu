@@ -2024,15 +2024,16 @@ wfa_stream_t* wfa_stream_start(wfa_metric_t metric, const wfa_penalties_t* penal
   s->smem = L.total;
   const int64_t seq_stride = ((int64_t)max_len_sum + 16 + 15) & ~(int64_t)15;
   const int64_t cig_stride = (2 * (int64_t)max_len_sum + 1 + 15) & ~(int64_t)15;
-  // After the ring and history: the request's bytes and its CIGAR.
-  group_words = ((group_words + (seq_stride + cig_stride) / 4) + 63) & ~(int64_t)63;
+  // After the ring and history (aligned to 16 bytes): the request's bytes
+  // and its CIGAR.
+  group_words = ((group_words + 4 + (seq_stride + cig_stride) / 4) + 63) & ~(int64_t)63;
   int occ = occupancy_resident(s->cls, s->lanes, s->smem);
   if (blocks_per_sm > 0) occ = std::min(occ, (int)blocks_per_sm);
   s->blocks = h->num_sms * std::max(1, occ);
   const int gpb = kWarpsPerBlock * 32 / s->lanes;
+  s->dev.st = h->stream;
   bool ok = h->scratch.ensure((size_t)s->blocks * gpb * group_words * 4) == cudaSuccess &&
             s->dev.ensure(64) == cudaSuccess;
-  s->dev.st = h->stream;
   ok = ok && cudaMemsetAsync(s->dev.p, 0, 64, h->stream) == cudaSuccess &&
        cudaStreamSynchronize(h->stream) == cudaSuccess && cudaEventCreate(&s->ended) == cudaSuccess;
   ResidentArgs& R = s->R;

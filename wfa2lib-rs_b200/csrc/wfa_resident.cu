@@ -42,6 +42,7 @@ WFA_D void doorbell(const ResidentArgs& R) {
     const unsigned long long t = ld_volatile(&R.ctl->tail);
     if (t != seen) {
       seen = t;
+      __threadfence_system();  // the requests below t are read after this
       *reinterpret_cast<volatile unsigned long long*>(R.dtail) = t;
       idle = 0;
     }
@@ -122,20 +123,26 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) resident_kernel(const 
   ws.bt = nullptr;
   ws.btinit = nullptr;
   ws.btmark = nullptr;
-  // After the ring and history: the request's bytes and its CIGAR.
-  uint8_t* stage = reinterpret_cast<uint8_t*>(ws.harena + ((P.hist_words + 3) & ~(int64_t)3));
+  // After the ring and history (16-byte aligned): the request's bytes and
+  // its CIGAR.
+  uint8_t* stage = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(ws.harena + P.hist_words) + 15) & ~(uintptr_t)15);
   uint8_t* cg_stage = stage + R.seq_stride;
   for (;;) {
     const int64_t slot = claim<LW>(R, lane);
     if (slot < 0) break;
     const int64_t i = slot % R.cap;
-    const ResidentReq q = R.reqs[i];
-    const int n = q.n, m = q.m;
+    // The slot was written by the host after any earlier read of its cache
+    // lines (a neighbouring slot's descriptor, the slot's previous request):
+    // read it with loads that fetch again (ld.cv) rather than from a cache.
+    __threadfence_system();
+    const int2 q = __ldcv(reinterpret_cast<const int2*>(R.reqs) + i);
+    const int n = q.x, m = q.y;
     // Stage the request's bytes (pattern then text) in device memory: the
     // aligner reads them many times.
-    const uint32_t* src = reinterpret_cast<const uint32_t*>(R.arena + i * R.seq_stride);
-    uint32_t* dst = reinterpret_cast<uint32_t*>(stage);
-    for (int w = lane; w < (n + m + 3) / 4; w += LW) dst[w] = src[w];
+    const int4* src = reinterpret_cast<const int4*>(R.arena + i * R.seq_stride);
+    int4* dst = reinterpret_cast<int4*>(stage);
+    for (int w = lane; w < (n + m + 15) / 16; w += LW) dst[w] = __ldcv(src + w);
     G::sync();
     SeqAscii sp{stage, n};
     SeqAscii st{stage + n, m};

@@ -19,9 +19,9 @@ struct ResidentCtl {
   int32_t pad;
 };
 
-// One request slot: lengths; its bytes (pattern then text) are at
-// arena + slot * seq_stride.
-struct ResidentReq {
+// One request slot: lengths (read by the kernel as one int2); its bytes
+// (pattern then text) are at arena + slot * seq_stride.
+struct alignas(8) ResidentReq {
   int32_t n, m;
 };
 
