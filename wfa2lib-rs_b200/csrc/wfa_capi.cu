@@ -1860,7 +1860,7 @@ struct wfa_stream {
   wfa_result_t* results = nullptr;
   uint8_t* cigars = nullptr;
   uint32_t* done = nullptr;
-  unsigned long long* xfer = nullptr;  // pinned word for the device counters
+  unsigned long long* xfer = nullptr;  // pinned words for the device counters
   DevBuf dev;                          // head, dtail, dstop
   ResidentArgs R{};
   AlignParams P{};
@@ -1870,6 +1870,7 @@ struct wfa_stream {
   int32_t max_len_sum = 0;
   std::mutex mu;
   uint64_t tail = 0, oldest = 0;
+  uint64_t served = 0;  // requests below this were served by ended launches
   std::vector<int64_t> t_submit;  // per slot (steady clock ns)
   std::vector<uint8_t> taken;     // per slot: its result was returned
   bool running = false;
@@ -1891,11 +1892,14 @@ void stream_free(wfa_stream_t* s) {
   delete s;
 }
 
-// Launches the kernel over what is published (caller holds mu).
+// Launches the kernel over what is published (caller holds mu): tickets
+// start at the first request no launch served (`served`), the mirrored tail
+// at what is published.
 int stream_launch(wfa_stream_t* s) {
   wfa_aligner_t* h = s->h;
-  *s->xfer = s->tail;
-  CUDA_TRY(h, cudaMemcpyAsync(s->R.dtail, s->xfer, 8, cudaMemcpyHostToDevice, h->stream), "stream tail");
+  s->xfer[0] = s->served;
+  s->xfer[1] = s->tail;
+  CUDA_TRY(h, cudaMemcpyAsync(s->R.head, s->xfer, 16, cudaMemcpyHostToDevice, h->stream), "stream counters");
   CUDA_TRY(h, cudaMemsetAsync(s->R.dstop, 0, 4, h->stream), "stream stop flag");
   CUDA_TRY(h, cudaGetLastError(), "an earlier CUDA call of this thread");
   CUDA_TRY(h, launch_resident(s->P, s->R, s->cls, s->lanes, s->blocks, s->smem, h->stream),
@@ -1922,10 +1926,18 @@ int stream_tend(wfa_stream_t* s) {
     }
     s->running = false;
   }
-  if (s->tail == 0) return WFA_OK;
-  CUDA_TRY(h, cudaMemcpyAsync(s->xfer, s->R.head, 8, cudaMemcpyDeviceToHost, h->stream), "stream head");
-  CUDA_TRY(h, cudaStreamSynchronize(h->stream), "stream head");
-  if (*s->xfer < s->tail) return stream_launch(s);
+  if (s->tail == s->served) return WFA_OK;
+  if (s->launches > 0) {
+    // The launch that ended served every request below the tail it saw last.
+    CUDA_TRY(h, cudaMemcpyAsync(s->xfer, s->R.dtail, 8, cudaMemcpyDeviceToHost, h->stream), "stream tail");
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream), "stream tail");
+    if (s->ctl->gave_up > 0) {
+      s->err = "resident kernel: a lane group gave up waiting for its request";
+      return WFA_ERR_CUDA;
+    }
+    s->served = s->xfer[0];
+  }
+  if (s->served < s->tail) return stream_launch(s);
   return WFA_OK;
 }
 
@@ -2048,7 +2060,7 @@ wfa_stream_t* wfa_stream_start(wfa_metric_t metric, const wfa_penalties_t* penal
        (s->results = host_mapped<wfa_result_t>((size_t)s->cap, &res_d)) &&
        (s->cigars = host_mapped<uint8_t>((size_t)(s->cap * cig_stride), &cig_d)) &&
        (s->done = host_mapped<uint32_t>((size_t)s->cap, &done_d)) &&
-       (s->xfer = host_mapped<unsigned long long>(1, &xfer_d));
+       (s->xfer = host_mapped<unsigned long long>(2, &xfer_d));
   if (!ok) {
     cudaGetLastError();
     stream_free(s);

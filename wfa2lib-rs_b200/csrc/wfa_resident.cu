@@ -5,8 +5,9 @@
 // a descriptor (lengths) and the pair's bytes per slot -- and publishes the
 // count in `tail`.  One warp of the kernel (warp 0 of block 0, the doorbell)
 // polls `tail` across the bus and mirrors it into device memory; every other
-// lane group claims the next request from a device counter (compare-and-swap
-// below the mirrored tail), stages its bytes, aligns it end to end with the
+// lane group takes a ticket from a device counter and serves that request
+// once the mirrored tail passes it: it stages the bytes, aligns them end to
+// end with the
 // same per-pair aligner as the batch kernels, and writes the result record
 // and CIGAR into mapped memory followed by the slot's completion mark.  So
 // requests join while the kernel runs, and nothing is copied per request by
@@ -47,6 +48,10 @@ WFA_D void doorbell(const ResidentArgs& R) {
       idle = 0;
     }
     if (ld_volatile(&R.ctl->stop)) {
+      // The host published its last requests before setting stop.
+      const unsigned long long t2 = ld_volatile(&R.ctl->tail);
+      __threadfence_system();
+      *reinterpret_cast<volatile unsigned long long*>(R.dtail) = t2;
       __threadfence();
       *reinterpret_cast<volatile int32_t*>(R.dstop) = 1;
       return;
@@ -61,27 +66,27 @@ WFA_D void doorbell(const ResidentArgs& R) {
   }
 }
 
-// The next request slot for a lane group (lane 0 claims it), or -1 when the
-// stream stopped or went idle and everything published was claimed, or when
-// the group polled R.group_polls times without either.
+// The next request for a lane group: lane 0 takes a ticket (one atomic add
+// on the device counter) and waits until the doorbell has seen that many
+// requests published; -1 when the stream stopped or went idle below the
+// ticket (every ticket below the final tail is served before its group
+// returns, so a relaunch starts at that tail), or when the group polled
+// R.group_polls times (counted in gave_up; the host then fails the stream).
 template <int LW>
 WFA_D int64_t claim(const ResidentArgs& R, int lane) {
   long long slot = -1;
   if (lane == 0) {
+    const unsigned long long ticket = atomicAdd(R.head, 1ull);
     int64_t polls = 0;
     unsigned ns = 64;
     for (;;) {
-      const unsigned long long h = ld_volatile(R.head), t = ld_volatile(R.dtail);
-      if (h < t) {
-        if (atomicCAS(R.head, h, h + 1) == h) {
-          slot = (long long)h;
-          break;
-        }
-        continue;  // another group took it: retry at once
+      if (ticket < ld_volatile(R.dtail)) {
+        slot = (long long)ticket;
+        break;
       }
       if (ld_volatile(R.dstop)) {
         // The doorbell stored the final tail before stop: one more look.
-        if (ld_volatile(R.head) < ld_volatile(R.dtail)) continue;
+        if (ticket < ld_volatile(R.dtail)) continue;
         break;
       }
       if (++polls > R.group_polls) {
@@ -89,7 +94,7 @@ WFA_D int64_t claim(const ResidentArgs& R, int lane) {
         break;
       }
       __nanosleep(ns);
-      ns = ns < 8192 ? ns * 2 : ns;
+      ns = ns < 4096 ? ns * 2 : ns;
     }
   }
   return (int64_t)__shfl_sync(Lanes<LW>::mask(), slot, 0, LW);

@@ -33,7 +33,7 @@ struct ResidentArgs {
   uint8_t* cigars;            // mapped, cap x cig_stride bytes
   uint32_t* done;             // mapped, cap marks: (slot / cap) + 1 once slot's result is written
   int64_t cap, seq_stride, cig_stride;
-  unsigned long long* head;   // device: requests claimed
+  unsigned long long* head;   // device: tickets handed out
   unsigned long long* dtail;  // device: the doorbell's copy of ctl->tail
   int32_t* dstop;             // device: 1 stopped by the host, 2 idle
   int64_t idle_polls;         // doorbell polls without a new request before the kernel ends
