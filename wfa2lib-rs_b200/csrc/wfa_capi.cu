@@ -1355,22 +1355,20 @@ int wfa_batch_align_device(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t*
   const bool order = orders_batch(h, b);
   OrderBufs ob{};
   if (order) {
-    // The longest pair and the cost keys in one pass over the batch.
+    // The longest pair, the cost keys and the ordered list in one pass (one
+    // cooperative launch), before the host waits; the list goes unused if the
+    // batch turns out to hold long pairs.
     if (int e = order_bufs(h, b->num_pairs, 1, &ob)) return e;
     CUDA_TRY(h, cudaMemsetAsync(ob.hist, 0, kOrderStride * 4, st), "memset");
-    CUDA_TRY(h, launch_order_count(static_cast<const uint8_t*>(b->seq), b->format == WFA_SEQ_PACKED2,
-                                   b->p_off, b->p_len, b->t_off, b->t_len, b->num_pairs, h->num_sms, d_max,
-                                   ob.keys, ob.hist, st), "cost keys");
+    int nl = 0;
+    CUDA_TRY(h, launch_order(static_cast<const uint8_t*>(b->seq), b->format == WFA_SEQ_PACKED2, b->p_off, b->p_len,
+                             b->t_off, b->t_len, b->num_pairs, h->num_sms, d_max, ob.keys, ob.hist,
+                             ob.hist + kOrderBins, ob.list, st, &nl),
+             "cost order");
+    h->launches += nl;
   } else {
     max_lengths<<<256, 256, 0, st>>>(b->p_len, b->t_len, b->num_pairs, d_max);
     CUDA_TRY(h, cudaGetLastError(), "max lengths");
-  }
-  h->launches++;
-  if (order) {
-    // The ordered list is made before the longest pair is known on the host
-    // (it goes unused if the batch turns out to hold long pairs).
-    CUDA_TRY(h, launch_order_scatter(ob.keys, b->num_pairs, ob.hist, ob.hist + kOrderBins, ob.list,
-                                     h->num_sms, st), "cost order");
     h->launches++;
   }
   int32_t mxs[2] = {0, 0};
@@ -1614,11 +1612,11 @@ int wfa_batch_align(wfa_aligner_t* h, const wfa_batch_t* b, wfa_result_t* result
     if (order && cn >= kSortMinPairs && length_bucket(I.max_len_sum) <= 2) {
       int32_t* hst = ob.hist + kOrderStride * ci;
       int32_t* dmx = hst + 2 * kOrderBins;  // the chunk's longest pair (known here already)
-      PIPE_TRY(launch_order_count(dseq, packed, dpo + a, dpl + a, dto + a, dtl + a, cn, h->num_sms, dmx,
-                                  ob.keys + a, hst, sc), "cost keys");
-      PIPE_TRY(launch_order_scatter(ob.keys + a, cn, hst, hst + kOrderBins, ob.list + a, h->num_sms, sc),
+      int nl = 0;
+      PIPE_TRY(launch_order(dseq, packed, dpo + a, dpl + a, dto + a, dtl + a, cn, h->num_sms, dmx, ob.keys + a,
+                            hst, hst + kOrderBins, ob.list + a, sc, &nl),
                "cost order");
-      h->launches += 2;
+      h->launches += nl;
       clist = ob.list + a;
     }
     PIPE_TRY(cudaEventRecord(h->evtime[2 * (size_t)ci], sc), "event");

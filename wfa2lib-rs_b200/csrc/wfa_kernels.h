@@ -112,6 +112,12 @@ cudaError_t launch_order_count(const uint8_t* seq, int packed, const int64_t* p_
                                int32_t* max_len_sum, uint16_t* keys, int32_t* hist, cudaStream_t st);
 cudaError_t launch_order_scatter(const uint16_t* keys, int64_t n, const int32_t* hist, int32_t* fill,
                                  int64_t* list, int num_sms, cudaStream_t st);
+// Both in one cooperative launch where the device supports it (else the two
+// launches); *launches: how many were made.
+cudaError_t launch_order(const uint8_t* seq, int packed, const int64_t* p_off, const int32_t* p_len,
+                         const int64_t* t_off, const int32_t* t_len, int64_t n, int num_sms, int32_t* max_len_sum,
+                         uint16_t* keys, int32_t* hist, int32_t* fill, int64_t* list, cudaStream_t st,
+                         int* launches);
 
 bool needs_general(const AlignParams& P);
 // BiWFA: lanes per pair 32 (a warp) or 128, 256, 512 (a team of warps; the

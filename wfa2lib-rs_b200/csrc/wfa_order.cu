@@ -11,6 +11,7 @@
 // distance follows the alignment score closely (correlation about 0.93).
 // The order only decides which pairs run together; results do not depend
 // on it.
+#include <cooperative_groups.h>
 #include <cub/block/block_scan.cuh>
 
 #include <algorithm>
@@ -34,12 +35,9 @@ constexpr int kProfileBases = 4096;  // bases of each sequence the estimate read
 // neighbour, updated with atomic adds whose results are not used (no update
 // waits for the previous one).
 constexpr uint32_t kBias = 0x4000;
-__global__ void __launch_bounds__(kCountBlock) order_count(const uint8_t* seq, int packed,
-                                                            const int64_t* p_off, const int32_t* p_len,
-                                                            const int64_t* t_off, const int32_t* t_len,
-                                                            int64_t n, int32_t* max_len_sum,
-                                                            uint16_t* keys, int32_t* hist) {
-  extern __shared__ __align__(16) uint8_t smem[];
+__device__ __forceinline__ void count_body(uint8_t* smem, const uint8_t* seq, int packed, const int64_t* p_off,
+                                           const int32_t* p_len, const int64_t* t_off, const int32_t* t_len,
+                                           int64_t n, int32_t* max_len_sum, uint16_t* keys, int32_t* hist) {
   uint32_t* prof = reinterpret_cast<uint32_t*>(smem);  // [128 word][kCountBlock]: 4-mers 2w, 2w+1
   int32_t* bins = reinterpret_cast<int32_t*>(smem + 128 * kCountBlock * 4);
   const int tid = threadIdx.x;
@@ -101,44 +99,81 @@ __global__ void __launch_bounds__(kCountBlock) order_count(const uint8_t* seq, i
     if (bins[b]) atomicAdd(&hist[b], bins[b]);
 }
 
+__global__ void __launch_bounds__(kCountBlock) order_count(const uint8_t* seq, int packed,
+                                                            const int64_t* p_off, const int32_t* p_len,
+                                                            const int64_t* t_off, const int32_t* t_len,
+                                                            int64_t n, int32_t* max_len_sum,
+                                                            uint16_t* keys, int32_t* hist) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  count_body(smem, seq, packed, p_off, p_len, t_off, t_len, n, max_len_sum, keys, hist);
+}
+
 constexpr int kScatterBlock = 256, kScatterItems = 8;
 constexpr int kScatterTile = kScatterBlock * kScatterItems;
 
 // list[] = the pair indices 0..n-1 in ascending bin order (falling cost).
-// Each block scans the histogram, then places a tile of pairs at a time:
-// ranks within the tile from shared-memory counters, one global reservation
-// per (tile, bin) in fill[].
-__global__ void __launch_bounds__(kScatterBlock) order_scatter(const uint16_t* keys, int64_t n,
-                                                               const int32_t* hist, int32_t* fill,
-                                                               int64_t* list) {
-  using Scan = cub::BlockScan<int32_t, kScatterBlock>;
-  __shared__ typename Scan::TempStorage scan_tmp;
-  __shared__ int32_t start[kOrderBins];  // exclusive scan of hist
-  __shared__ int32_t tcount[kOrderBins];  // this tile's pairs per bin, then their base
-  constexpr int kPer = kOrderBins / kScatterBlock;
+// Each block scans the histogram, then places a tile of BLOCK x ITEMS pairs
+// at a time: ranks within the tile from shared-memory counters, one global
+// reservation per (tile, bin) in fill[].
+template <int BLOCK, int ITEMS>
+struct ScatterSmem {
+  typename cub::BlockScan<int32_t, BLOCK>::TempStorage scan;
+  int32_t start[kOrderBins];   // exclusive scan of hist
+  int32_t tcount[kOrderBins];  // this tile's pairs per bin, then their base
+};
+template <int BLOCK, int ITEMS>
+__device__ __forceinline__ void scatter_body(ScatterSmem<BLOCK, ITEMS>& sm, const uint16_t* keys, int64_t n,
+                                             const int32_t* hist, int32_t* fill, int64_t* list) {
+  using Scan = cub::BlockScan<int32_t, BLOCK>;
+  constexpr int kPer = kOrderBins / BLOCK;
+  constexpr int kTile = BLOCK * ITEMS;
   int32_t v[kPer];
   for (int j = 0; j < kPer; ++j) v[j] = hist[threadIdx.x * kPer + j];
-  Scan(scan_tmp).ExclusiveSum(v, v);
-  for (int j = 0; j < kPer; ++j) start[threadIdx.x * kPer + j] = v[j];
-  for (int64_t t0 = (int64_t)blockIdx.x * kScatterTile; t0 < n; t0 += (int64_t)gridDim.x * kScatterTile) {
-    for (int b = threadIdx.x; b < kOrderBins; b += kScatterBlock) tcount[b] = 0;
+  Scan(sm.scan).ExclusiveSum(v, v);
+  for (int j = 0; j < kPer; ++j) sm.start[threadIdx.x * kPer + j] = v[j];
+  for (int64_t t0 = (int64_t)blockIdx.x * kTile; t0 < n; t0 += (int64_t)gridDim.x * kTile) {
+    for (int b = threadIdx.x; b < kOrderBins; b += BLOCK) sm.tcount[b] = 0;
     __syncthreads();
-    int32_t bin[kScatterItems], rank[kScatterItems];
-    for (int k = 0; k < kScatterItems; ++k) {
-      const int64_t i = t0 + (int64_t)k * kScatterBlock + threadIdx.x;
+    int32_t bin[ITEMS], rank[ITEMS];
+    for (int k = 0; k < ITEMS; ++k) {
+      const int64_t i = t0 + (int64_t)k * BLOCK + threadIdx.x;
       bin[k] = i < n ? kOrderBins - 1 - keys[i] : -1;
-      rank[k] = bin[k] >= 0 ? atomicAdd(&tcount[bin[k]], 1) : 0;
+      rank[k] = bin[k] >= 0 ? atomicAdd(&sm.tcount[bin[k]], 1) : 0;
     }
     __syncthreads();
-    for (int b = threadIdx.x; b < kOrderBins; b += kScatterBlock)
-      if (tcount[b]) tcount[b] = start[b] + atomicAdd(&fill[b], tcount[b]);
+    for (int b = threadIdx.x; b < kOrderBins; b += BLOCK)
+      if (sm.tcount[b]) sm.tcount[b] = sm.start[b] + atomicAdd(&fill[b], sm.tcount[b]);
     __syncthreads();
-    for (int k = 0; k < kScatterItems; ++k) {
-      const int64_t i = t0 + (int64_t)k * kScatterBlock + threadIdx.x;
-      if (bin[k] >= 0) list[tcount[bin[k]] + rank[k]] = i;
+    for (int k = 0; k < ITEMS; ++k) {
+      const int64_t i = t0 + (int64_t)k * BLOCK + threadIdx.x;
+      if (bin[k] >= 0) list[sm.tcount[bin[k]] + rank[k]] = i;
     }
     __syncthreads();
   }
+}
+
+__global__ void __launch_bounds__(kScatterBlock) order_scatter(const uint16_t* keys, int64_t n,
+                                                               const int32_t* hist, int32_t* fill,
+                                                               int64_t* list) {
+  __shared__ ScatterSmem<kScatterBlock, kScatterItems> sm;
+  scatter_body<kScatterBlock, kScatterItems>(sm, keys, n, hist, fill, list);
+}
+
+// Both steps in one cooperative launch: every block counts its share of the
+// pairs, the grid synchronises (the histogram is complete), then every block
+// places its tiles.  The count's shared memory is reused by the scatter.
+constexpr int kFusedItems = 16;
+using FusedSmem = ScatterSmem<kCountBlock, kFusedItems>;
+__global__ void __launch_bounds__(kCountBlock) order_pairs(const uint8_t* seq, int packed, const int64_t* p_off,
+                                                            const int32_t* p_len, const int64_t* t_off,
+                                                            const int32_t* t_len, int64_t n,
+                                                            int32_t* max_len_sum, uint16_t* keys,
+                                                            int32_t* hist, int32_t* fill, int64_t* list) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  count_body(smem, seq, packed, p_off, p_len, t_off, t_len, n, max_len_sum, keys, hist);
+  cooperative_groups::this_grid().sync();
+  __syncthreads();
+  scatter_body<kCountBlock, kFusedItems>(*reinterpret_cast<FusedSmem*>(smem), keys, n, hist, fill, list);
 }
 
 static cudaError_t allow_count_smem() {
@@ -150,7 +185,9 @@ static cudaError_t allow_count_smem() {
   return e;
 }
 
-size_t order_count_smem() { return (size_t)128 * kCountBlock * 4 + (size_t)kOrderBins * 4; }
+size_t order_count_smem() {
+  return std::max((size_t)128 * kCountBlock * 4 + (size_t)kOrderBins * 4, sizeof(FusedSmem));
+}
 
 cudaError_t launch_order_count(const uint8_t* seq, int packed, const int64_t* p_off, const int32_t* p_len,
                                const int64_t* t_off, const int32_t* t_len, int64_t n, int num_sms,
@@ -170,6 +207,48 @@ cudaError_t launch_order_scatter(const uint16_t* keys, int64_t n, const int32_t*
   const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)num_sms * 8));
   order_scatter<<<blocks, kScatterBlock, 0, st>>>(keys, n, hist, fill, list);
   return cudaGetLastError();
+}
+
+cudaError_t launch_order(const uint8_t* seq, int packed, const int64_t* p_off, const int32_t* p_len,
+                         const int64_t* t_off, const int32_t* t_len, int64_t n, int num_sms, int32_t* max_len_sum,
+                         uint16_t* keys, int32_t* hist, int32_t* fill, int64_t* list, cudaStream_t st,
+                         int* launches) {
+  cudaError_t e = allow_count_smem();
+  if (e != cudaSuccess) return e;
+  static int coop = -1, per_sm = 0;
+  if (coop < 0) {
+    int dev = 0, attr = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&attr, cudaDevAttrCooperativeLaunch, dev) == cudaSuccess && attr &&
+        cudaFuncSetAttribute(order_pairs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)order_count_smem()) ==
+            cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, order_pairs, kCountBlock, order_count_smem()) ==
+            cudaSuccess &&
+        per_sm > 0) {
+      coop = 1;
+    } else {
+      cudaGetLastError();
+      coop = 0;
+    }
+  }
+  const int64_t want = (n + kCountBlock - 1) / kCountBlock;
+  if (coop) {
+    // Every block of a cooperative launch is resident at once.
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)num_sms * std::min(per_sm, 3)));
+    void* args[] = {(void*)&seq, (void*)&packed, (void*)&p_off, (void*)&p_len, (void*)&t_off, (void*)&t_len,
+                    (void*)&n, (void*)&max_len_sum, (void*)&keys, (void*)&hist, (void*)&fill, (void*)&list};
+    e = cudaLaunchCooperativeKernel((const void*)order_pairs, dim3(blocks), dim3(kCountBlock), args,
+                                    order_count_smem(), st);
+    if (e == cudaSuccess) {
+      *launches = 1;
+      return cudaSuccess;
+    }
+    cudaGetLastError();
+  }
+  e = launch_order_count(seq, packed, p_off, p_len, t_off, t_len, n, num_sms, max_len_sum, keys, hist, st);
+  if (e != cudaSuccess) return e;
+  *launches = 2;
+  return launch_order_scatter(keys, n, hist, fill, list, num_sms, st);
 }
 
 }  // namespace wfab
