@@ -386,6 +386,13 @@ WFA_API int wfa_stream_stats(wfa_stream_t* s, int64_t* out, int32_t n);
  * not yet polled are dropped). */
 WFA_API int wfa_stream_stop(wfa_stream_t* s);
 
+/* Device-checks build only (libwfa_b200_checked.so, WFA_DEVICE_CHECKS): the
+ * number of failed index checks of the aligner's invariants in this
+ * handle's kernels so far (each failure skips the access or re-runs the
+ * pair); -1 from the product build, which compiles the checks out.  No
+ * counterpart in the reference (its debug builds assert). */
+WFA_API int64_t wfa_device_check_failures(wfa_aligner_t* h);
+
 /* Number of the library's own kernel launches issued so far by this handle. */
 WFA_API int64_t wfa_kernel_launches(const wfa_aligner_t* h);
 

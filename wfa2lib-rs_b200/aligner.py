@@ -15,7 +15,9 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "lib", "libwfa_b200.so")
+# WFA_B200_CHECKED=1 loads the device-checks build (tests only; make checked).
+LIB_PATH = os.path.join(_HERE, "lib", "libwfa_b200_checked.so" if os.environ.get("WFA_B200_CHECKED") == "1"
+                        else "libwfa_b200.so")
 
 # Enum values of include/wfa_b200.h (the reference's enum order).
 INDEL, EDIT, GAP_LINEAR, GAP_AFFINE, GAP_AFFINE_2P = range(5)
@@ -120,6 +122,7 @@ def lib():
         "wfa_stream_stats": (ctypes.c_int, [vp, ctypes.POINTER(i64), i32]),
         "wfa_stream_stop": (ctypes.c_int, [vp]),
         "wfa_kernel_launches": (i64, [vp]),
+        "wfa_device_check_failures": (i64, [vp]),
         "wfa_last_rerun_pairs": (i64, [vp]),
         "wfa_set_lanes_per_pair": (ctypes.c_int, [vp, i32]),
         "wfa_last_lanes_per_pair": (i32, [vp]),
@@ -291,6 +294,11 @@ class WavefrontAligner:
         """32 lanes (a warp) or 128, 256, 512 (a team of warps) per pair for
         BiWFA batches without a heuristic; 0 chooses by the longest pair."""
         return self._check(self._L.wfa_set_biwfa_lanes(self._h, lanes))
+
+    def device_check_failures(self):
+        """Failed index checks in this handle's kernels (device-checks build),
+        -1 with the product build."""
+        return self._L.wfa_device_check_failures(self._h)
 
     def last_lanes_per_pair(self):
         return self._L.wfa_last_lanes_per_pair(self._h)

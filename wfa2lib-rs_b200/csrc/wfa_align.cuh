@@ -57,6 +57,30 @@ struct uint2 { unsigned x, y; };
 
 namespace wfab {
 
+// Index checks of the aligner's invariants.  The emulation builds abort on a
+// failed check; the device-checks build (WFA_DEVICE_CHECKS) counts it in
+// P.check_count and takes the given way out (skip the access, or stop the
+// pair with a retry) so that no access goes out of bounds; the product build
+// compiles them out.
+#if !(defined(__CUDACC__) && !defined(WFA_EMU))
+#define WFA_CHECK(cond, on_fail) \
+  do {                          \
+    if (!(cond)) std::abort();  \
+  } while (0)
+#elif defined(WFA_DEVICE_CHECKS)
+#define WFA_CHECK(cond, on_fail)                          \
+  do {                                                    \
+    if (!(cond)) {                                        \
+      if (P.check_count) atomicAdd(P.check_count, 1);     \
+      on_fail;                                            \
+    }                                                     \
+  } while (0)
+#else
+#define WFA_CHECK(cond, on_fail) \
+  do {                          \
+  } while (0)
+#endif
+
 // ---------------------------------------------------------------------------
 // Warp primitives (one-lane stand-ins in the emulation build)
 // ---------------------------------------------------------------------------
@@ -494,9 +518,7 @@ struct PairAligner {
   WFA_D int sidx(int t) const {
     int i = cidx - ((cscore - t) >> gshift);
     i = i < 0 ? i + dscope : i;
-#if !(defined(__CUDACC__) && !defined(WFA_EMU))
-    if (i < 0 || i >= dscope) std::abort();  // emulation-only check
-#endif
+    WFA_CHECK(i >= 0 && i < dscope, i = 0);
     return i;
   }
   WFA_D void advance() {
@@ -545,9 +567,9 @@ struct PairAligner {
     } else {
       idx = (int64_t)sidx(s) * NC + c;
     }
-#if !(defined(__CUDACC__) && !defined(WFA_EMU))
-    if (compact && idx >= P.ring_slots) std::abort();  // emulation-only check
-#endif
+    WFA_CHECK(!compact || idx < P.ring_slots, { retry = true; return nullptr; });
+    WFA_CHECK(compact || idx < (int64_t)scope * NC + (modular ? bi_idc_rows(NC, P.e1, P.e2) : 0),
+              { retry = true; return nullptr; });
     if (w <= wmax) {
       int32_t* base = ws.ringv + idx * wmax;
       if (PB && pgb && c == CM) { mbase = base; mL = L; mH = H; }
@@ -1520,9 +1542,7 @@ struct PairAligner {
     if (!wf_present(d) || d.lo > d.hi) return;
     int32_t* b = ws.dom + (int64_t)c * dom_len + (d.lo - hist_lo);
     const int cnt = d.hi - d.lo + 1;
-#if !(defined(__CUDACC__) && !defined(WFA_EMU))
-    if (d.lo < hist_lo || d.hi - hist_lo >= dom_len) std::abort();  // emulation-only check
-#endif
+    WFA_CHECK(d.lo >= hist_lo && d.hi - hist_lo < dom_len, return);
     int first = cnt, last = -1;
     for (int i = lane; i < cnt; i += LW)
       if (d.vals[d.lo + i - d.a] > b[i]) { first = imin(first, i); last = imax(last, i); }
@@ -1549,9 +1569,7 @@ struct PairAligner {
     WfD d = slot(CM, s);
     if (wf_is_null(d) || d.lo > d.hi) return;
     int32_t* b = ws.dom + (d.lo - hist_lo);
-#if !(defined(__CUDACC__) && !defined(WFA_EMU))
-    if (d.lo < hist_lo || d.hi - hist_lo >= dom_len) std::abort();  // emulation-only check
-#endif
+    WFA_CHECK(d.lo >= hist_lo && d.hi - hist_lo < dom_len, return);
     for (int k = d.lo + lane; k <= d.hi; k += LW) b[k - d.lo] = imax(b[k - d.lo], d.vals[k - d.a]);
     G::sync();
   }

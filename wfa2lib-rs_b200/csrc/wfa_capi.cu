@@ -103,6 +103,7 @@ struct wfa_aligner {
   DevBuf seq, poff, plen, toff, tlen, coff, results, cigars, dense, scratch, counters, pairlist;
   DevBuf chunkinfo;               // per-chunk counters and dense CIGAR ranges
   DevBuf order;                   // cost ordering: keys, histograms, pair lists
+  DevBuf checks;                  // device-checks build: failed index checks
   int64_t* hinfo = nullptr;       // pinned host copy of the chunk info
   size_t hinfo_cap = 0;
   int64_t launches = 0;
@@ -391,6 +392,11 @@ static void fill_params(const wfa_aligner_t* h, const wfa_batch_t* b, AlignParam
   P.p0 = h->p0; P.pf = h->pf; P.t0 = h->t0; P.tf = h->tf;
   P.hkind = h->hkind; P.hp0 = h->hp0; P.hp1 = h->hp1; P.hp2 = h->hp2;
   P.compute_alignment = h->scope == WFA_SCOPE_ALIGNMENT;
+#ifdef WFA_DEVICE_CHECKS
+  P.check_count = h->checks.as<int32_t>();
+#else
+  P.check_count = nullptr;
+#endif
   // Med/low with an alignment: the piggyback backtrace (BiWFA ignores the mode).
   P.piggyback = P.compute_alignment && h->memory_mode != WFA_MEMORY_HIGH && b->span != WFA_SPAN_BIWFA
                     ? (h->memory_mode == WFA_MEMORY_LOW ? 2 : 1)
@@ -1028,8 +1034,15 @@ wfa_aligner_t* wfa_aligner_create(wfa_metric_t metric, const wfa_penalties_t* pe
   }
   for (DevBuf* b : {&h->seq, &h->poff, &h->plen, &h->toff, &h->tlen, &h->coff, &h->results,
                     &h->cigars, &h->dense, &h->scratch, &h->counters, &h->pairlist, &h->chunkinfo,
-                    &h->order})
+                    &h->order, &h->checks})
     b->st = h->stream;
+#ifdef WFA_DEVICE_CHECKS
+  if (h->checks.ensure(16) != cudaSuccess || cudaMemset(h->checks.p, 0, 16) != cudaSuccess) {
+    wfa_aligner_destroy(h);
+    if (err) *err = WFA_ERR_CUDA;
+    return nullptr;
+  }
+#endif
   if (event_pool(h, 32) != cudaSuccess) {
     wfa_aligner_destroy(h);
     if (err) *err = WFA_ERR_CUDA;
@@ -1054,7 +1067,7 @@ void wfa_aligner_destroy(wfa_aligner_t* h) {
     if (x) cudaStreamSynchronize(x);
   for (DevBuf* b : {&h->seq, &h->poff, &h->plen, &h->toff, &h->tlen, &h->coff, &h->results,
                     &h->cigars, &h->dense, &h->scratch, &h->counters, &h->pairlist, &h->chunkinfo,
-                    &h->order})
+                    &h->order, &h->checks})
     b->release();
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->pinned) cudaFreeHost(h->pinned);
@@ -1289,6 +1302,19 @@ int wfa_alignment_end_pos(const wfa_aligner_t* h, int32_t* s, int32_t* k, int32_
 int wfa_last_error(const wfa_aligner_t* h) { return h ? h->last_err : WFA_ERR_ARGUMENT; }
 const char* wfa_last_error_string(const wfa_aligner_t* h) { return h ? h->err_str.c_str() : "null handle"; }
 int64_t wfa_kernel_launches(const wfa_aligner_t* h) { return h ? h->launches : 0; }
+int64_t wfa_device_check_failures(wfa_aligner_t* h) {
+#ifdef WFA_DEVICE_CHECKS
+  if (!h) return WFA_ERR_ARGUMENT;
+  int32_t v = 0;
+  cudaSetDevice(h->device);
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess ||
+      cudaMemcpy(&v, h->checks.p, 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return WFA_ERR_CUDA;
+  return v;
+#else
+  return h ? -1 : WFA_ERR_ARGUMENT;
+#endif
+}
 int64_t wfa_last_rerun_pairs(const wfa_aligner_t* h) { return h ? h->last_reruns : 0; }
 int wfa_set_lanes_per_pair(wfa_aligner_t* h, int32_t lanes) {
   if (!h || !(lanes == 0 || lanes == 4 || lanes == 8 || lanes == 16 || lanes == 32)) return WFA_ERR_ARGUMENT;

@@ -85,6 +85,8 @@ struct AlignParams {
   int64_t dom_words;   // Corrected-mode dominance array per warp (cells; 0: none)
   unsigned long long* work_counter;
   int32_t* retry_count;
+  // Device-checks build (WFA_DEVICE_CHECKS): failed index checks counted here.
+  int32_t* check_count;
 };
 
 // Score step of the unidirectional aligner: scores that are not multiples
