@@ -186,10 +186,15 @@ struct Lanes {
   }
   static WFA_D int lane() { return threadIdx.x & (LW - 1); }
   static WFA_D void sync() {
-    if constexpr (TEAM)
-      asm volatile("bar.sync 1, %0;" ::"n"(LW) : "memory");
-    else
+    if constexpr (TEAM) {
+      // The warp's lanes may reach this point apart (after lane-dependent
+      // branches): reconverge them first, and use the barrier form that does
+      // not assume a converged warp (bar.sync is barrier.sync.aligned).
+      __syncwarp();
+      asm volatile("barrier.sync 1, %0;" ::"n"(LW) : "memory");
+    } else {
       __syncwarp(mask());
+    }
   }
   // One partial per warp of the block: up to 16 warps (512 threads).
   static WFA_D int* partials() {
