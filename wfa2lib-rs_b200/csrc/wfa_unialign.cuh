@@ -25,8 +25,13 @@ namespace wfab {
 // 128 (4 blocks) rather than spill.
 // The med/low instantiation carries three arrays per cell and the backtrace
 // buffer: 2 blocks per SM (up to 255 registers) rather than spill.
-template <int CLS, bool GEN, bool PB = false>
-constexpr int min_blocks() { return PB ? 2 : (GEN || CLS == kAffine2pClass) ? 4 : kMinBlocksPerSM; }
+// With 4 lanes per pair a block's 32 rings in shared memory already hold an
+// SM to 5 blocks, so that width gets the registers of 5 (96) instead of
+// spilling to fit a sixth block that could not be resident.
+template <int CLS, bool GEN, bool PB = false, int LW = 32>
+constexpr int min_blocks() {
+  return PB ? 2 : (GEN || CLS == kAffine2pClass) ? 4 : LW == 4 ? 5 : kMinBlocksPerSM;
+}
 
 // The sequences of pair `pair`, staged in the group's shared memory (2 x sw
 // words) when both fit, else read from device memory.
@@ -83,7 +88,7 @@ WFA_D void mark_retry(const AlignParams& P, int64_t pair, int lane) {
 }
 
 template <int CLS, int ENC, bool GEN, int LW, bool PB = false>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, (min_blocks<CLS, GEN, PB>()))
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, (min_blocks<CLS, GEN, PB, LW>()))
     unialign_kernel(const AlignParams P) {
   extern __shared__ __align__(16) uint8_t smem[];
   constexpr int kGroups = kWarpsPerBlock * 32 / LW;  // lane groups (pairs in flight) per block
