@@ -499,7 +499,7 @@ def run_serve(args):
     per_rate = args.pairs
     srv = pkg.Server(pkg.GAP_AFFINE, PEN, device=local, workers=args.workers,
                      short_workers=args.workers, biwfa_workers=args.workers,
-                     max_batch_bytes=16 << 30)
+                     max_batch_bytes=16 << 30, resident=args.resident)
     # Warm-up: a few requests of each kind.
     wps, _ = synth.config5(64, synth.SEED_BASE + 55)
     for i in range(len(wps)):
@@ -556,6 +556,7 @@ def run_serve(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)",
             "config": {"workload": SERVE, "requests_per_rate": per_rate,
                        "workers_per_lane": args.workers, "lanes": "short (n+m<=1024), long, BiWFA",
+                       "short_lane": "resident stream" if args.resident else "host-buffer batches",
                        "form": "wfa_server_* continuous batching, host request buffers"},
             "p50_ms": best["p50_ms"], "p99_ms": best["p99_ms"], "sweep": table}
     print(json.dumps(line), flush=True)
@@ -679,6 +680,8 @@ def main():
                     type=lambda s: tuple(int(x) for x in s.split(",")),
                     help="lo,hi: keep only pairs with pattern length in [lo, hi] (profiling)")
     ap.add_argument("--workers", type=int, default=2, help="serve: workers per lane")
+    ap.add_argument("--resident", action="store_true",
+                    help="serve: the short lane is a resident stream (wfa_stream_*)")
     ap.add_argument("--pairs", type=int, default=None)
     ap.add_argument("--plain-pairs", type=int, default=None)
     ap.add_argument("--cpu-sample", type=int, default=None)

@@ -303,7 +303,9 @@ typedef struct {
   int32_t biwfa_workers;        /* BiWFA lane workers (default 2) */
   int32_t short_max_len;        /* n + m of the short lane (default 1024) */
   int32_t resident;             /* 1: the short lane is a resident stream (wfa_stream_*; n + m of the
-                                   short lane at most 2048) */
+                                   short lane at most 2048).  Measured: the long and BiWFA lanes'
+                                   batches then wait until the resident kernel has ended (a second
+                                   after the last request); use it for short-read traffic. */
 } wfa_server_config_t;
 
 typedef struct wfa_server wfa_server_t;

@@ -1043,7 +1043,11 @@ wfa_aligner_t* wfa_aligner_create(wfa_metric_t metric, const wfa_penalties_t* pe
     return nullptr;
   }
 #endif
-  if (event_pool(h, 32) != cudaSuccess) {
+  // Events made now rather than by the first batches: creating an event
+  // waits for the work running on the device, which beside a resident
+  // stream's kernel (running until it has been idle for about a second)
+  // would hold a batch that long.
+  if (event_pool(h, 32) != cudaSuccess || timing_events(h, 16) != cudaSuccess) {
     wfa_aligner_destroy(h);
     if (err) *err = WFA_ERR_CUDA;
     return nullptr;
@@ -1839,6 +1843,51 @@ int32_t wfa_cigar_rle(const uint8_t* ops, int32_t len, char* out, int32_t cap) {
 const char* wfa_version(void) { return "wfa2lib-rs_b200 0.1 (sm_100a)"; }
 
 }  // extern "C"
+
+namespace wfab {
+cudaError_t preload_order_kernels();
+
+// Loads every kernel of the library on `device` now.  CUDA loads a kernel
+// at its first launch, and loading waits until the kernels already running
+// on the device have finished: beside a resident stream's kernel (which
+// runs until it has been idle for about a second) a batch lane's first
+// launch of each kernel would wait that long.  The occupancy queries need
+// each kernel loaded, so one query per instantiation loads them all.
+int preload_kernels(int device) {
+  if (cudaSetDevice(device) != cudaSuccess) return WFA_ERR_CUDA;
+  cudaFuncAttributes a;
+  for (const void* f : {(const void*)collect_retries, (const void*)compact_cigars, (const void*)scan_tiles<0, false>,
+                        (const void*)scan_tiles<0, true>, (const void*)scan_tiles<1, false>,
+                        (const void*)scan_tiles<1, true>, (const void*)scan_tile_offsets, (const void*)max_lengths,
+                        (const void*)collect_retries_capped})
+    if (cudaFuncGetAttributes(&a, f) != cudaSuccess) return WFA_ERR_CUDA;
+  if (preload_order_kernels() != cudaSuccess) return WFA_ERR_CUDA;
+  for (int metric : {(int)WFA_METRIC_EDIT, (int)WFA_METRIC_GAP_LINEAR, (int)WFA_METRIC_GAP_AFFINE,
+                     (int)WFA_METRIC_GAP_AFFINE_2P}) {
+    const int cls = metric_class(metric);
+    AlignParams P{};
+    P.metric = metric;
+    P.compute_alignment = 1;
+    for (int fmt : {(int)WFA_SEQ_ASCII, (int)WFA_SEQ_PACKED2}) {
+      P.format = fmt;
+      P.span = WFA_SPAN_END2END;
+      P.piggyback = 0;
+      P.hkind = WFA_HEURISTIC_NONE;
+      for (int lanes : {4, 8, 16, 32}) occupancy_blocks_per_sm(P, cls, lanes, 0);
+      for (int lanes : {32, 128, 256, 512}) occupancy_biwfa(P, cls, lanes, 0);
+      P.hkind = WFA_HEURISTIC_WFADAPTIVE;  // the kernels with heuristic support
+      occupancy_blocks_per_sm(P, cls, 32, 0);
+      occupancy_biwfa(P, cls, 32, 0);
+      P.hkind = WFA_HEURISTIC_NONE;
+      P.piggyback = 1;  // med/low
+      occupancy_blocks_per_sm(P, cls, 32, 0);
+    }
+    for (int lanes : {8, 32}) occupancy_resident(cls, lanes, 0);
+  }
+  cudaGetLastError();
+  return WFA_OK;
+}
+}  // namespace wfab
 
 // ---------------------------------------------------------------------------
 // Resident stream (wfa_stream_*): a persistent kernel (wfa_resident.cu) fed

@@ -209,6 +209,17 @@ cudaError_t launch_order_scatter(const uint16_t* keys, int64_t n, const int32_t*
   return cudaGetLastError();
 }
 
+// Loads the ordering kernels (CUDA loads a kernel at its first launch
+// otherwise; see preload_kernels in wfa_capi.cu).
+cudaError_t preload_order_kernels() {
+  cudaFuncAttributes a;
+  for (const void* f : {(const void*)order_count, (const void*)order_scatter, (const void*)order_pairs}) {
+    cudaError_t e = cudaFuncGetAttributes(&a, f);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 cudaError_t launch_order(const uint8_t* seq, int packed, const int64_t* p_off, const int32_t* p_len,
                          const int64_t* t_off, const int32_t* t_len, int64_t n, int num_sms, int32_t* max_len_sum,
                          uint16_t* keys, int32_t* hist, int32_t* fill, int64_t* list, cudaStream_t st,

@@ -209,9 +209,20 @@ static cudaError_t launch_res_t(const AlignParams& P, const ResidentArgs& R, int
                                 cudaStream_t st) {
   auto k = resident_kernel<CLS, LW>;
   static size_t configured = 0;
+  static bool carveout = false;
   static std::mutex mu;
   {
     std::lock_guard<std::mutex> lock(mu);
+    // The SMs that host the resident kernel keep its shared-memory
+    // configuration while it runs: ask for the largest, so that other
+    // kernels' blocks (larger shared-memory needs) fit beside it instead of
+    // waiting for it to end.
+    if (!carveout) {
+      cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                           (int)cudaSharedmemCarveoutMaxShared);
+      if (e != cudaSuccess) return e;
+      carveout = true;
+    }
     if (smem > configured) {
       cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       if (e != cudaSuccess) return e;

@@ -30,6 +30,10 @@
 
 #include "../../include/wfa_b200.h"
 
+namespace wfab {
+int preload_kernels(int device);  // wfa_capi.cu
+}
+
 namespace {
 
 using Clock = std::chrono::steady_clock;
@@ -251,8 +255,15 @@ wfa_server_t* wfa_server_start(const wfa_server_config_t* config, int* err) {
   }
   if (s->cfg.resident) {
     // The resident short lane holds one block per SM, so that the batch
-    // lanes' kernels find room beside it.
-    int e = WFA_OK;
+    // lanes' kernels find room beside it; every kernel is loaded before it
+    // starts (a first launch beside it would wait for it to end).
+    int e = wfab::preload_kernels(s->cfg.device);
+    if (e != WFA_OK) {
+      for (wfa_aligner_t* x : s->handles) wfa_aligner_destroy(x);
+      delete s;
+      if (err) *err = e;
+      return nullptr;
+    }
     s->stream = wfa_stream_start((wfa_metric_t)s->cfg.metric, &s->cfg.penalties, s->cfg.device, s->cfg.score_only,
                                  std::min(s->cfg.short_max_len, 2048), 1 << 16, 1, &e);
     if (!s->stream) {
