@@ -131,6 +131,13 @@ template <int ENC, bool GEN, int LW>
 int occupancy_biwfa_lw(int cls, size_t smem) {
   int nb = 0;
   cudaError_t e;
+  // Loads the kernel if it is not yet (see occ_t in wfa_unialign.cuh).
+  cudaFuncAttributes fa;
+  const void* fk = cls == kEditClass     ? (const void*)biwfa_kernel<kEditClass, ENC, GEN, LW>
+                   : cls == kLinearClass ? (const void*)biwfa_kernel<kLinearClass, ENC, GEN, LW>
+                   : cls == kAffineClass ? (const void*)biwfa_kernel<kAffineClass, ENC, GEN, LW>
+                                         : (const void*)biwfa_kernel<kAffine2pClass, ENC, GEN, LW>;
+  if (cudaFuncGetAttributes(&fa, fk) != cudaSuccess) cudaGetLastError();
   switch (cls) {
     case kEditClass:
       e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, biwfa_kernel<kEditClass, ENC, GEN, LW>,

@@ -1851,8 +1851,9 @@ cudaError_t preload_order_kernels();
 // at its first launch, and loading waits until the kernels already running
 // on the device have finished: beside a resident stream's kernel (which
 // runs until it has been idle for about a second) a batch lane's first
-// launch of each kernel would wait that long.  The occupancy queries need
-// each kernel loaded, so one query per instantiation loads them all.
+// launch of each kernel would wait that long.  The occupancy queries load
+// their kernel (cudaFuncGetAttributes), so one query per instantiation
+// loads them all.
 int preload_kernels(int device) {
   if (cudaSetDevice(device) != cudaSuccess) return WFA_ERR_CUDA;
   cudaFuncAttributes a;

@@ -236,6 +236,8 @@ static cudaError_t launch_res_t(const AlignParams& P, const ResidentArgs& R, int
 template <int CLS, int LW>
 static int occ_res_t(size_t smem) {
   int nb = 0;
+  cudaFuncAttributes fa;  // loads the kernel if it is not yet
+  if (cudaFuncGetAttributes(&fa, resident_kernel<CLS, LW>) != cudaSuccess) cudaGetLastError();
   if (cudaFuncSetAttribute(resident_kernel<CLS, LW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
           cudaSuccess ||
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, resident_kernel<CLS, LW>, kWarpsPerBlock * 32, smem) !=

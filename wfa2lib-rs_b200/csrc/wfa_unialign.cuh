@@ -162,6 +162,10 @@ template <int CLS, int ENC, bool GEN, int LW, bool PB = false>
 static int occ_t(size_t smem) {
   int nb = 0;
   auto k = unialign_kernel<CLS, ENC, GEN, LW, PB>;
+  // Loads the kernel if it is not yet (the server loads every kernel this
+  // way before its resident lane starts).
+  cudaFuncAttributes fa;
+  if (cudaFuncGetAttributes(&fa, k) != cudaSuccess) cudaGetLastError();
   if (allow_smem<CLS, ENC, GEN, LW, PB>(smem) != cudaSuccess ||
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, kWarpsPerBlock * 32, smem) != cudaSuccess) {
     cudaGetLastError();
